@@ -1,0 +1,192 @@
+"""ctypes mirror of the QPhiX C API (qphix_int.h, qphix_f3.h, qphix_d3.h).
+
+One class, ``QphixLib``, drives any shared library that exports the
+reference's ``QPHIX_*`` symbols: the product library ``libqphix_b200.so``
+and, in the tests, the reference host code built as ``oracle/_ref``.  The
+structures below restate ``QPHIX_layout_t``, ``QPHIX_info_t``,
+``QPHIX_invert_arg_t`` and ``QPHIX_resid_arg_t`` (qphix_int.h:30-85) field by
+field; the call sequence is MILC's (init -> create_L -> create_V ->
+invert/dslash -> extract_V -> destroy).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+QPHIX_SUCCESS, QPHIX_FAIL, QPHIX_MEM_ERROR = 0, 1, 2
+QPHIX_EVEN, QPHIX_ODD, QPHIX_EVENODD = 0x02, 0x01, 0x03
+PARITY = {"even": QPHIX_EVEN, "odd": QPHIX_ODD, "evenodd": QPHIX_EVENODD}
+
+NODE_NUMBER_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_int))
+NODE_INDEX_FN = C.CFUNCTYPE(C.c_size_t, C.POINTER(C.c_int))
+
+
+class Layout(C.Structure):
+    _fields_ = [
+        ("node_number", NODE_NUMBER_FN),
+        ("node_index", NODE_INDEX_FN),
+        ("latdim", C.c_int),
+        ("latsize", C.POINTER(C.c_int)),
+        ("machdim", C.c_int),
+        ("machsize", C.POINTER(C.c_int)),
+        ("this_node", C.c_int),
+        ("sites_on_node", C.c_size_t),
+        ("even_sites_on_node", C.c_size_t),
+        ("mpi_comm", C.c_void_p),
+    ]
+
+
+class Info(C.Structure):
+    _fields_ = [("final_sec", C.c_double), ("final_flop", C.c_double),
+                ("status", C.c_int), ("count1", C.c_int), ("count2", C.c_int)]
+
+
+class InvertArg(C.Structure):
+    _fields_ = [("parity", C.c_int), ("max", C.c_int), ("restart", C.c_int),
+                ("nrestart", C.c_int), ("evenodd", C.c_int)]
+
+
+class ResidArg(C.Structure):
+    _fields_ = [("resid", C.c_double), ("final_rsq", C.c_double),
+                ("relresid", C.c_double), ("final_rel", C.c_double),
+                ("size_r", C.c_double), ("size_relr", C.c_double),
+                ("final_iter", C.c_int), ("final_restart", C.c_int)]
+
+
+def _node_number(coords):
+    return 0
+
+
+def _node_index(coords):
+    return 0
+
+
+_NODE_NUMBER = NODE_NUMBER_FN(_node_number)
+_NODE_INDEX = NODE_INDEX_FN(_node_index)
+
+
+def make_layout(dims):
+    """Single-node layout for lattice ``dims`` = [Nx, Ny, Nz, Nt]."""
+    lat = (C.c_int * 4)(*dims)
+    mach = (C.c_int * 4)(1, 1, 1, 1)
+    V = int(np.prod(dims))
+    lay = Layout(_NODE_NUMBER, _NODE_INDEX, 4, lat, 4, mach, 0, V, V // 2, None)
+    lay._keep = (lat, mach)
+    return lay
+
+
+class QphixLib:
+    """Calls into one QPHIX_* library; ``prec`` is 'F' (float) or 'D' (double)."""
+
+    def __init__(self, path, mode=C.RTLD_LOCAL):
+        self.path = str(path)
+        self.lib = C.CDLL(self.path, mode=mode)
+        L = self.lib
+        L.QPHIX_init.restype = C.c_int
+        L.QPHIX_init.argtypes = [C.POINTER(Layout)]
+        L.QPHIX_finalize.restype = C.c_int
+        for P, real in (("F", C.c_float), ("D", C.c_double)):
+            rp = C.POINTER(real)
+            f = getattr(L, f"QPHIX_{P}3_create_V_from_raw")
+            f.restype, f.argtypes = C.c_void_p, [rp, C.c_int]
+            f = getattr(L, f"QPHIX_{P}3_extract_V_to_raw")
+            f.restype, f.argtypes = None, [rp, C.c_void_p, C.c_int]
+            f = getattr(L, f"QPHIX_{P}3_destroy_V")
+            f.restype, f.argtypes = None, [C.c_void_p]
+            f = getattr(L, f"QPHIX_{P}3_asqtad_create_L_from_raw")
+            f.restype, f.argtypes = C.c_void_p, [rp, rp, rp, rp, C.c_int]
+            f = getattr(L, f"QPHIX_{P}3_asqtad_extract_L_to_raw")
+            f.restype, f.argtypes = None, [rp, rp, C.c_void_p, C.c_int]
+            f = getattr(L, f"QPHIX_{P}3_asqtad_destroy_L")
+            f.restype, f.argtypes = None, [C.c_void_p]
+            f = getattr(L, f"QPHIX_{P}3_asqtad_dslash")
+            f.restype, f.argtypes = None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+            f = getattr(L, f"QPHIX_{P}3_asqtad_invert")
+            f.restype = C.c_int
+            f.argtypes = [C.POINTER(Info), C.c_void_p, C.POINTER(InvertArg),
+                          C.POINTER(ResidArg), real, C.c_void_p, C.c_void_p]
+            f = getattr(L, f"QPHIX_{P}3_asqtad_invert_multi")
+            f.restype = C.c_int
+            f.argtypes = [C.POINTER(Info), C.c_void_p, C.POINTER(InvertArg),
+                          C.POINTER(C.POINTER(ResidArg)), rp, C.c_int,
+                          C.POINTER(C.c_void_p), C.c_void_p]
+
+    # -- helpers -----------------------------------------------------------
+    @staticmethod
+    def _real(prec):
+        return (C.c_float, np.float32) if prec == "F" else (C.c_double, np.float64)
+
+    def _fn(self, prec, name):
+        return getattr(self.lib, f"QPHIX_{prec}3_{name}")
+
+    # -- API ---------------------------------------------------------------
+    def init(self, dims):
+        self._layout = make_layout(dims)
+        self.dims = tuple(dims)
+        return self.lib.QPHIX_init(C.byref(self._layout))
+
+    def finalize(self):
+        return self.lib.QPHIX_finalize()
+
+    def create_V(self, prec, raw, evenodd="evenodd"):
+        ct, nt = self._real(prec)
+        a = np.ascontiguousarray(raw, dtype=nt)
+        return self._fn(prec, "create_V_from_raw")(a.ctypes.data_as(C.POINTER(ct)), PARITY[evenodd])
+
+    def extract_V(self, prec, handle, evenodd="evenodd", out=None):
+        ct, nt = self._real(prec)
+        V = int(np.prod(self.dims))
+        if out is None:
+            out = np.zeros(V * 6, dtype=nt)
+        self._fn(prec, "extract_V_to_raw")(out.ctypes.data_as(C.POINTER(ct)), handle, PARITY[evenodd])
+        return out
+
+    def destroy_V(self, prec, handle):
+        self._fn(prec, "destroy_V")(handle)
+
+    def create_L(self, prec, links, evenodd="evenodd"):
+        ct, nt = self._real(prec)
+        arrs = [np.ascontiguousarray(links[k], dtype=nt) for k in ("fat", "lng", "fatback", "lngback")]
+        ptrs = [a.ctypes.data_as(C.POINTER(ct)) for a in arrs]
+        return self._fn(prec, "asqtad_create_L_from_raw")(*ptrs, PARITY[evenodd])
+
+    def extract_L(self, prec, handle, evenodd="evenodd"):
+        ct, nt = self._real(prec)
+        V = int(np.prod(self.dims))
+        fat = np.zeros(V * 72, dtype=nt)
+        lng = np.zeros(V * 72, dtype=nt)
+        self._fn(prec, "asqtad_extract_L_to_raw")(fat.ctypes.data_as(C.POINTER(ct)),
+                                                   lng.ctypes.data_as(C.POINTER(ct)),
+                                                   handle, PARITY[evenodd])
+        return fat, lng
+
+    def destroy_L(self, prec, handle):
+        self._fn(prec, "asqtad_destroy_L")(handle)
+
+    def dslash(self, prec, L, out, inp, parity):
+        self._fn(prec, "asqtad_dslash")(L, out, inp, PARITY[parity])
+
+    def invert(self, prec, L, out, inp, mass, parity="even", max_iter=1000, restart=1000,
+               nrestart=5, resid=1e-20, relresid=0.0):
+        info = Info()
+        inv = InvertArg(PARITY[parity], max_iter, restart, nrestart, QPHIX_EVENODD)
+        res = ResidArg(resid, 0, relresid, 0, 0, 0, 0, 0)
+        it = self._fn(prec, "asqtad_invert")(C.byref(info), L, C.byref(inv), C.byref(res),
+                                             mass, out, inp)
+        return it, info, res
+
+    def invert_multi(self, prec, L, outs, inp, masses, parity="even", max_iter=1000,
+                     restart=1000, nrestart=5, resid=1e-20, relresid=0.0):
+        ct, nt = self._real(prec)
+        n = len(masses)
+        info = Info()
+        inv = InvertArg(PARITY[parity], max_iter, restart, nrestart, QPHIX_EVENODD)
+        res = [ResidArg(resid, 0, relresid, 0, 0, 0, 0, 0) for _ in range(n)]
+        res_ptrs = (C.POINTER(ResidArg) * n)(*[C.pointer(r) for r in res])
+        m = np.ascontiguousarray(masses, dtype=nt)
+        outs_arr = (C.c_void_p * n)(*outs)
+        it = self._fn(prec, "asqtad_invert_multi")(C.byref(info), L, C.byref(inv), res_ptrs,
+                                                   m.ctypes.data_as(C.POINTER(ct)), n,
+                                                   outs_arr, inp)
+        return it, info, res
