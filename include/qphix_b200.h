@@ -1,0 +1,86 @@
+/*
+ * qphix_b200.h -- additions of libqphix_b200.so beyond the reference QPhiX
+ * C API.  None of these has a counterpart in the reference (which is CPU
+ * only); they control how the GPU runs the reference entry points and
+ * expose measurements.  All are optional: a MILC build that only includes
+ * qphix.h gets the reference behaviour (pure-precision solves).
+ */
+#ifndef _QPHIX_B200_H
+#define _QPHIX_B200_H
+
+#include <qphix_int.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Inner (sloppy) precision of QPHIX_D3_asqtad_invert / _invert_multi.
+ * DOUBLE: FP64 throughout with the reference control flow (default).
+ * SINGLE: FP32 inner CG with FP64 reliable updates; FP64 solution, FP64
+ *         reductions; converges on the FP64 true residual.
+ * HALF:   16-bit inner CG (per-site-normalised FP16 vectors, 16-bit fixed
+ *         point links, FP32 arithmetic) with FP64 reliable updates.
+ * The environment variable QPHIX_GPU_PRECISION=double|single|half sets the
+ * initial value at QPHIX_init. */
+typedef enum {
+  QPHIX_B200_PREC_HALF = 0,
+  QPHIX_B200_PREC_SINGLE = 1,
+  QPHIX_B200_PREC_DOUBLE = 2
+} QPHIX_B200_precision_t;
+
+QPHIX_status_t QPHIX_B200_set_inner_precision(QPHIX_B200_precision_t p);
+QPHIX_B200_precision_t QPHIX_B200_get_inner_precision(void);
+
+/* Reliable-update threshold of the mixed-precision solvers: the FP64 true
+ * residual is recomputed when the sloppy residual norm has dropped by this
+ * factor since the last update (default 0.1). */
+QPHIX_status_t QPHIX_B200_set_reliable_delta(double delta);
+
+/* Diagnostics of the most recent invert / invert_multi call. */
+typedef struct {
+  double solve_ms;        /* device time of the call (CUDA events) */
+  int iterations;         /* Krylov iterations (all precisions) */
+  int reliable_updates;   /* FP64 true-residual recomputations */
+  int dslash_launches;    /* plain Dslash launches that did work (timing on) */
+  double dslash_ms;       /* their summed device time */
+  int mdagm_launches;     /* fused Dslash + M^dag M epilogue launches (timing on) */
+  double mdagm_ms;        /* their summed device time */
+  double true_rsq;        /* final |b - M x|^2 / |b|^2 (largest over masses) */
+} QPHIX_B200_stats_t;
+
+QPHIX_status_t QPHIX_B200_get_last_stats(QPHIX_B200_stats_t *stats);
+
+/* Per-launch CUDA-event timing of the Dslash kernels inside solves
+ * (0 = off, the default). */
+QPHIX_status_t QPHIX_B200_set_kernel_timing(int on);
+
+/* Device timer on the library's CUDA stream: start, then stop returns the
+ * elapsed milliseconds between the two points of the stream. */
+QPHIX_status_t QPHIX_B200_timer_start(void);
+QPHIX_status_t QPHIX_B200_timer_stop(double *ms);
+
+/* `reps` back-to-back Dslash launches out[parity] = D in[opposite]
+ * timed with CUDA events; *ms_per_call = mean device time of one launch. */
+QPHIX_status_t QPHIX_B200_F3_dslash_timed(void *links, void *out, void *in,
+                                          QPHIX_evenodd_t parity, int reps,
+                                          double *ms_per_call);
+QPHIX_status_t QPHIX_B200_D3_dslash_timed(void *links, void *out, void *in,
+                                          QPHIX_evenodd_t parity, int reps,
+                                          double *ms_per_call);
+
+/* Host-side neighbour arithmetic used by the Dslash kernels (no GPU
+ * needed): block index, in the opposite parity, of neighbour k of site
+ * `site` of parity cb on lattice L[4] = {Nx,Ny,Nz,Nt}.  k follows the
+ * reference NeighTable order (qphix_misc.cpp:88-221). */
+long QPHIX_B200_neighbor_index(const int L[4], int cb, long site, int k);
+
+/* Message of the last failed call (empty string if none). */
+const char *QPHIX_B200_last_error(void);
+
+/* Library version, e.g. 100 for 1.0.0. */
+int QPHIX_B200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* _QPHIX_B200_H */

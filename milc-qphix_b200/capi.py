@@ -76,6 +76,16 @@ def make_layout(dims):
     return lay
 
 
+class Stats(C.Structure):
+    _fields_ = [("solve_ms", C.c_double), ("iterations", C.c_int),
+                ("reliable_updates", C.c_int), ("dslash_launches", C.c_int),
+                ("dslash_ms", C.c_double), ("mdagm_launches", C.c_int),
+                ("mdagm_ms", C.c_double), ("true_rsq", C.c_double)]
+
+
+PRECISION = {"half": 0, "single": 1, "double": 2}
+
+
 class QphixLib:
     """Calls into one QPHIX_* library; ``prec`` is 'F' (float) or 'D' (double)."""
 
@@ -111,6 +121,62 @@ class QphixLib:
             f.argtypes = [C.POINTER(Info), C.c_void_p, C.POINTER(InvertArg),
                           C.POINTER(C.POINTER(ResidArg)), rp, C.c_int,
                           C.POINTER(C.c_void_p), C.c_void_p]
+
+        # QPHIX_B200_* additions (absent from the reference library)
+        self.has_b200 = hasattr(L, "QPHIX_B200_version")
+        if self.has_b200:
+            L.QPHIX_B200_last_error.restype = C.c_char_p
+            L.QPHIX_B200_set_inner_precision.argtypes = [C.c_int]
+            L.QPHIX_B200_set_reliable_delta.argtypes = [C.c_double]
+            L.QPHIX_B200_get_last_stats.argtypes = [C.POINTER(Stats)]
+            L.QPHIX_B200_set_kernel_timing.argtypes = [C.c_int]
+            L.QPHIX_B200_timer_stop.argtypes = [C.POINTER(C.c_double)]
+            for P in ("F", "D"):
+                f = getattr(L, f"QPHIX_B200_{P}3_dslash_timed")
+                f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                              C.POINTER(C.c_double)]
+            L.QPHIX_B200_neighbor_index.restype = C.c_long
+            L.QPHIX_B200_neighbor_index.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_long, C.c_int]
+
+    # -- QPHIX_B200_* ------------------------------------------------------
+    def last_error(self):
+        if not self.has_b200:
+            return ""
+        return self.lib.QPHIX_B200_last_error().decode()
+
+    def set_inner_precision(self, name):
+        return self.lib.QPHIX_B200_set_inner_precision(PRECISION[name])
+
+    def set_reliable_delta(self, delta):
+        return self.lib.QPHIX_B200_set_reliable_delta(delta)
+
+    def last_stats(self):
+        s = Stats()
+        self.lib.QPHIX_B200_get_last_stats(C.byref(s))
+        return s
+
+    def set_kernel_timing(self, on):
+        return self.lib.QPHIX_B200_set_kernel_timing(1 if on else 0)
+
+    def timer_start(self):
+        return self.lib.QPHIX_B200_timer_start()
+
+    def timer_stop(self):
+        ms = C.c_double()
+        self.lib.QPHIX_B200_timer_stop(C.byref(ms))
+        return ms.value
+
+    def dslash_timed(self, prec, L, out, inp, parity, reps):
+        ms = C.c_double()
+        rc = getattr(self.lib, f"QPHIX_B200_{prec}3_dslash_timed")(L, out, inp, PARITY[parity], reps,
+                                                                   C.byref(ms))
+        if rc != 0:
+            raise RuntimeError("dslash_timed failed: " + self.last_error())
+        return ms.value
+
+    def neighbor_index(self, dims, cb, site, k):
+        Ld = (C.c_int * 4)(*dims)
+        return self.lib.QPHIX_B200_neighbor_index(Ld, cb, site, k)
 
     # -- helpers -----------------------------------------------------------
     @staticmethod

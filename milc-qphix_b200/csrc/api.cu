@@ -1,0 +1,639 @@
+// The C ABI: QPHIX_* entry points of qphix_int.h / qphix_f3.h / qphix_d3.h
+// and the QPHIX_B200_* additions of qphix_b200.h.
+//
+// Error behaviour: where the reference asserts and exits (MYASSERT,
+// ks_boundary.h:35, and assert() in the solvers) this library returns
+// QPHIX_FAIL (through the return value or info->status), or NULL from a
+// create call, and records a message for QPHIX_B200_last_error().  Nothing
+// exits, aborts or traps.
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "context.h"
+#include "device_common.cuh"
+
+using namespace qb;
+
+namespace {
+
+template <typename F>
+QPHIX_status_t guarded(F f)
+{
+    try {
+        f();
+        ctx().last_error.clear();
+        return QPHIX_SUCCESS;
+    } catch (const Error &e) {
+        ctx().last_error = e.what();
+        return e.status;
+    } catch (const std::exception &e) {
+        ctx().last_error = e.what();
+        return QPHIX_FAIL;
+    }
+}
+
+void require_init()
+{
+    if (!ctx().initialized) throw Error("QPhiX library used before QPHIX_init");
+}
+
+Prec env_precision(Prec dflt)
+{
+    const char *e = std::getenv("QPHIX_GPU_PRECISION");
+    if (!e) return dflt;
+    if (!strcmp(e, "double") || !strcmp(e, "fp64")) return Prec::Double;
+    if (!strcmp(e, "single") || !strcmp(e, "fp32") || !strcmp(e, "mixed")) return Prec::Single;
+    if (!strcmp(e, "half") || !strcmp(e, "fp16")) return Prec::Half;
+    return dflt;
+}
+
+// Lattice checks of QPHIX_init (qphix_misc.cpp:455-469, 494-497)
+void init_context(QPHIX_layout_t *layout)
+{
+    Context &c = ctx();
+    if (!layout || !layout->latsize) throw Error("QPHIX_init: layout or latsize is NULL");
+    if (layout->machdim != layout->latdim) throw Error("QPHIX_init: machine dimension must equal lattice dimension");
+    if (layout->latdim != 4) throw Error("QPHIX_init: only 4-dimensional lattices are supported");
+    int nranks = 1;
+    for (int i = 0; i < layout->machdim; ++i) nranks *= layout->machsize ? layout->machsize[i] : 1;
+    if (nranks != 1) throw Error("QPHIX_init: one lattice per GPU; machsize must be all ones");
+    const int *L = layout->latsize;
+    for (int i = 0; i < 4; ++i)
+        if (L[i] <= 0) throw Error("QPHIX_init: non-positive lattice extent");
+    if (L[0] % 2) throw Error("QPHIX_init: Nx must be even");
+    if ((L[0] / 2) % 2 != 0) throw Error("QPHIX_init: Nx/2 must be even");
+    if (L[1] % 4 || L[2] % 4 || L[3] % 4) throw Error("QPHIX_init: Ny, Nz and Nt must be multiples of 4");
+    const long long V = (long long)L[0] * L[1] * L[2] * L[3];
+    if (V / 2 > (1LL << 30)) throw Error("QPHIX_init: lattice too large for 32-bit site indices");
+    if (2LL * ((V / 2 + kBlock - 1) / kBlock) > 4LL * kMaxPartials)
+        throw Error("QPHIX_init: lattice too large for one GPU's reduction scratch");
+    if (layout->node_number) {
+        const int orig[4] = {0, 0, 0, 0};
+        (void)layout->node_number(orig);  // the reference calls it (qphix_misc.cpp:489)
+    }
+    if (c.initialized) {
+        if (c.dims[0] == L[0] && c.dims[1] == L[1] && c.dims[2] == L[2] && c.dims[3] == L[3]) return;
+        throw Error("QPHIX_init: already initialised with another lattice; call QPHIX_finalize first");
+    }
+    const char *dev = std::getenv("QPHIX_GPU_DEVICE");
+    c.device = dev ? std::atoi(dev) : 0;
+    QB_CUDA(cudaSetDevice(c.device));
+    QB_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    cudaMemPool_t pool;
+    QB_CUDA(cudaDeviceGetDefaultMemPool(&pool, c.device));
+    uint64_t thr = UINT64_MAX;
+    QB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    for (int i = 0; i < 4; ++i) c.dims[i] = L[i];
+    c.g = make_geom(L[0], L[1], L[2], L[3]);
+    QB_CUDA(cudaMalloc(&c.d_state, sizeof(SolverState)));
+    QB_CUDA(cudaMemset(c.d_state, 0, sizeof(SolverState)));
+    QB_CUDA(cudaMallocHost(&c.h_state, sizeof(SolverState)));
+    std::memset(c.h_state, 0, sizeof(SolverState));
+    QB_CUDA(cudaMalloc(&c.d_partials, sizeof(double) * 4 * kMaxPartials));
+    QB_CUDA(cudaMalloc(&c.d_scalars, sizeof(double) * 64));
+    QB_CUDA(cudaMallocHost(&c.h_scalars, sizeof(double) * 64));
+    for (int i = 0; i < 2; ++i) {
+        QB_CUDA(cudaEventCreate(&c.ev_solve[i]));
+        QB_CUDA(cudaEventCreate(&c.ev_user[i]));
+    }
+    c.inner = env_precision(Prec::Double);
+    c.initialized = true;
+}
+
+void finalize_context()
+{
+    Context &c = ctx();
+    if (!c.initialized) return;
+    cudaStreamSynchronize(c.stream);
+    cudaFree(c.d_state);
+    cudaFreeHost(c.h_state);
+    cudaFree(c.d_partials);
+    cudaFree(c.d_scalars);
+    cudaFreeHost(c.h_scalars);
+    for (int i = 0; i < 2; ++i) {
+        cudaEventDestroy(c.ev_solve[i]);
+        cudaEventDestroy(c.ev_user[i]);
+    }
+    for (auto e : c.ktimer.ev) cudaEventDestroy(e);
+    c.ktimer.ev.clear();
+    cudaStreamDestroy(c.stream);
+    c.stream = nullptr;
+    c.d_state = nullptr;
+    c.h_state = nullptr;
+    c.initialized = false;
+    for (int i = 0; i < 4; ++i) c.dims[i] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// precision-generic API bodies
+// ---------------------------------------------------------------------------
+template <typename Real> struct Api;
+template <> struct Api<float> {
+    using CV = QPHIX_F3_ColorVector;
+    using FL = QPHIX_F3_FermionLinksAsqtad;
+    static constexpr Prec prec = Prec::Single;
+};
+template <> struct Api<double> {
+    using CV = QPHIX_D3_ColorVector;
+    using FL = QPHIX_D3_FermionLinksAsqtad;
+    static constexpr Prec prec = Prec::Double;
+};
+
+template <typename Real>
+typename Api<Real>::CV *create_V(Real *src, QPHIX_evenodd_t evenodd)
+{
+    using CV = typename Api<Real>::CV;
+    CV *V = nullptr;
+    QPHIX_status_t s = guarded([&] {
+        require_init();
+        Context &c = ctx();
+        if (!src) throw Error("create_V_from_raw: NULL source");
+        if ((evenodd & QPHIX_EVENODD) == 0) throw Error("create_V_from_raw: bad evenodd");
+        V = new CV();
+        V->parity = evenodd;
+        const size_t nblk = (size_t)c.g.vh * 6;
+        void *stage = dev_alloc(nblk * sizeof(Real));
+        for (int cb = 0; cb < 2; ++cb) {
+            const int want = cb == 0 ? (evenodd & QPHIX_EVEN) : (evenodd & QPHIX_ODD);
+            if (!want) continue;
+            V->blk[cb] = alloc_vec(Api<Real>::prec);
+            QB_CUDA(cudaMemcpyAsync(stage, src + cb * nblk, nblk * sizeof(Real), cudaMemcpyHostToDevice, c.stream));
+            vec_from_raw(Api<Real>::prec, V->blk[cb], stage, sizeof(Real) == 8, c.launch());
+        }
+        dev_free(stage);
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+        QB_CUDA(cudaGetLastError());
+        V->even = V->blk[0].data;
+        V->odd = V->blk[1].data;
+    });
+    if (s != QPHIX_SUCCESS && V) {
+        for (auto &b : V->blk) free_vec(b);
+        delete V;
+        V = nullptr;
+    }
+    return V;
+}
+
+template <typename Real>
+void extract_V(Real *dest, typename Api<Real>::CV *V)
+{
+    guarded([&] {
+        require_init();
+        Context &c = ctx();
+        if (!dest || !V) throw Error("extract_V_to_raw: NULL argument");
+        const size_t nblk = (size_t)c.g.vh * 6;
+        void *stage = dev_alloc(nblk * sizeof(Real));
+        for (int cb = 0; cb < 2; ++cb) {
+            const int have = cb == 0 ? (V->parity & QPHIX_EVEN) : (V->parity & QPHIX_ODD);
+            if (!have) continue;
+            vec_to_raw(Api<Real>::prec, stage, sizeof(Real) == 8, V->blk[cb], c.launch());
+            QB_CUDA(cudaMemcpyAsync(dest + cb * nblk, stage, nblk * sizeof(Real), cudaMemcpyDeviceToHost, c.stream));
+        }
+        dev_free(stage);
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+        QB_CUDA(cudaGetLastError());
+    });
+}
+
+template <typename Real>
+void destroy_V(typename Api<Real>::CV *V)
+{
+    if (!V) return;
+    guarded([&] {
+        for (auto &b : V->blk) free_vec(b);
+        if (ctx().initialized) QB_CUDA(cudaStreamSynchronize(ctx().stream));
+    });
+    delete V;
+}
+
+template <typename FL>
+void free_link_handle(FL *L)
+{
+    free_links(L->links);
+    free_links(L->sloppy_half);
+    if constexpr (std::is_same<FL, QPHIX_D3_FermionLinksAsqtad>::value) free_links(L->sloppy_single);
+}
+
+template <typename Real>
+typename Api<Real>::FL *create_L(Real *fat, Real *lng, Real *fatback, Real *lngback, QPHIX_evenodd_t evenodd)
+{
+    using FL = typename Api<Real>::FL;
+    FL *H = nullptr;
+    QPHIX_status_t s = guarded([&] {
+        require_init();
+        Context &c = ctx();
+        if (!fat || !lng || !fatback || !lngback) throw Error("asqtad_create_L_from_raw: NULL link array");
+        H = new FL();
+        H->links = alloc_links(Api<Real>::prec);
+        const size_t nhalf = (size_t)c.g.vh * 72;
+        Real *stage = static_cast<Real *>(dev_alloc(2 * nhalf * sizeof(Real)));
+        Real *raw[4] = {fat, fatback, lng, lngback};  // slots 0..3
+        for (int slot = 0; slot < 4; ++slot) {
+            QB_CUDA(cudaMemsetAsync(stage, 0, 2 * nhalf * sizeof(Real), c.stream));
+            // only the parities asked for are read, as in qphix_f3.cpp:976-1063
+            if (evenodd & QPHIX_EVEN)
+                QB_CUDA(cudaMemcpyAsync(stage, raw[slot], nhalf * sizeof(Real), cudaMemcpyHostToDevice, c.stream));
+            if (evenodd & QPHIX_ODD)
+                QB_CUDA(cudaMemcpyAsync(stage + nhalf, raw[slot] + nhalf, nhalf * sizeof(Real),
+                                        cudaMemcpyHostToDevice, c.stream));
+            links_from_raw(Api<Real>::prec, H->links, stage, sizeof(Real) == 8, slot, c.launch());
+        }
+        dev_free(stage);
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+        QB_CUDA(cudaGetLastError());
+        const size_t famoff = (size_t)8 * 9 * c.g.vh * (sizeof(Real) * 2);
+        H->fateven = H->links.blk[0];
+        H->fatodd = H->links.blk[1];
+        H->lngeven = static_cast<char *>(H->links.blk[0]) + famoff;
+        H->lngodd = static_cast<char *>(H->links.blk[1]) + famoff;
+    });
+    if (s != QPHIX_SUCCESS && H) {
+        free_link_handle(H);
+        delete H;
+        H = nullptr;
+    }
+    return H;
+}
+
+template <typename Real>
+void extract_L(Real *fat, Real *lng, typename Api<Real>::FL *H, QPHIX_evenodd_t evenodd)
+{
+    guarded([&] {
+        require_init();
+        Context &c = ctx();
+        if (!fat || !lng || !H) throw Error("asqtad_extract_L_to_raw: NULL argument");
+        const size_t nhalf = (size_t)c.g.vh * 72;
+        Real *stage = static_cast<Real *>(dev_alloc(2 * nhalf * sizeof(Real)));
+        Real *dst[2] = {fat, lng};
+        const int slots[2] = {0, 2};  // forward links only (qphix_f3.cpp:1125-1143)
+        for (int f = 0; f < 2; ++f) {
+            links_to_raw(Api<Real>::prec, stage, sizeof(Real) == 8, H->links, slots[f], c.launch());
+            if (evenodd & QPHIX_EVEN)
+                QB_CUDA(cudaMemcpyAsync(dst[f], stage, nhalf * sizeof(Real), cudaMemcpyDeviceToHost, c.stream));
+            if (evenodd & QPHIX_ODD)
+                QB_CUDA(cudaMemcpyAsync(dst[f] + nhalf, stage + nhalf, nhalf * sizeof(Real), cudaMemcpyDeviceToHost,
+                                        c.stream));
+            QB_CUDA(cudaStreamSynchronize(c.stream));
+        }
+        dev_free(stage);
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+        QB_CUDA(cudaGetLastError());
+    });
+}
+
+template <typename Real>
+void destroy_L(typename Api<Real>::FL *H)
+{
+    if (!H) return;
+    guarded([&] {
+        free_link_handle(H);
+        if (ctx().initialized) QB_CUDA(cudaStreamSynchronize(ctx().stream));
+    });
+    delete H;
+}
+
+// QPHIX_*_asqtad_dslash (qphix_f3.cpp:1233-1245)
+template <typename Real>
+QPHIX_status_t asqtad_dslash(typename Api<Real>::FL *H, typename Api<Real>::CV *out, typename Api<Real>::CV *in,
+                             QPHIX_evenodd_t parity)
+{
+    return guarded([&] {
+        require_init();
+        Context &c = ctx();
+        if (!H || !out || !in) throw Error("asqtad_dslash: NULL argument");
+        if (parity != QPHIX_EVEN && parity != QPHIX_ODD) throw Error("asqtad_dslash: parity must be EVEN or ODD");
+        const int cb = parity == QPHIX_EVEN ? 0 : 1;
+        const int need_in = cb == 0 ? QPHIX_ODD : QPHIX_EVEN;
+        if (!(out->parity & parity) || !(in->parity & need_in))
+            throw Error("asqtad_dslash: vectors lack the parities the operator needs");
+        dslash(Api<Real>::prec, c.launch(), out->blk[cb], in->blk[1 - cb], H->links, cb);
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+        QB_CUDA(cudaGetLastError());
+    });
+}
+
+template <typename Real>
+int asqtad_invert(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_invert_arg_t *inv, QPHIX_resid_arg_t *res,
+                  Real mass, typename Api<Real>::CV *out, typename Api<Real>::CV *in)
+{
+    int iters = 0;
+    QPHIX_status_t s = guarded([&] {
+        require_init();
+        Context &c = ctx();
+        if (!info || !H || !inv || !res || !out || !in) throw Error("asqtad_invert: NULL argument");
+        // ks_d_congrad_fn.cpp:233
+        if (!(in->parity == out->parity && in->parity == inv->parity))
+            throw Error("asqtad_invert: in, out and inv_arg parities differ");
+        if (inv->max <= 0 || inv->nrestart < 0) throw Error("asqtad_invert: bad iteration limits");
+        c.stats = Stats();
+        SolveArgs a{info, inv, res, (double)mass, {out->blk[0], out->blk[1]}, {in->blk[0], in->blk[1]}};
+        QB_CUDA(cudaEventRecord(c.ev_solve[0], c.stream));
+        Prec inner = Api<Real>::prec;
+        if constexpr (std::is_same<Real, double>::value) inner = c.inner;
+        if (inner == Api<Real>::prec) {
+            iters = cg_reference(Api<Real>::prec, H->links, a);
+        } else {
+            const LinkSet &lss = [&]() -> const LinkSet & {
+                if constexpr (std::is_same<Real, double>::value) {
+                    if (inner == Prec::Single) {
+                        if (!H->sloppy_single.valid) {
+                            H->sloppy_single = alloc_links(Prec::Single);
+                            links_convert(Prec::Single, H->sloppy_single, Prec::Double, H->links, c.launch());
+                        }
+                        return H->sloppy_single;
+                    }
+                }
+                if (!H->sloppy_half.valid) {
+                    H->sloppy_half = alloc_links(Prec::Half);
+                    links_absmax(Api<Real>::prec, H->links, H->sloppy_half, c.launch(), c.d_partials);
+                    links_convert(Prec::Half, H->sloppy_half, Api<Real>::prec, H->links, c.launch());
+                }
+                return H->sloppy_half;
+            }();
+            if constexpr (std::is_same<Real, double>::value) iters = cg_mixed(inner, H->links, lss, a);
+            else throw Error("asqtad_invert: mixed precision is available through the D3 API");
+        }
+        QB_CUDA(cudaEventRecord(c.ev_solve[1], c.stream));
+        QB_CUDA(cudaEventSynchronize(c.ev_solve[1]));
+        float ms = 0;
+        QB_CUDA(cudaEventElapsedTime(&ms, c.ev_solve[0], c.ev_solve[1]));
+        c.stats.solve_ms = ms;
+        QB_CUDA(cudaGetLastError());
+    });
+    if (s != QPHIX_SUCCESS && info) info->status = s;
+    return iters;
+}
+
+template <typename Real>
+int asqtad_invert_multi(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_invert_arg_t *inv,
+                        QPHIX_resid_arg_t *res[], Real *mass, int n, typename Api<Real>::CV *out[],
+                        typename Api<Real>::CV *in)
+{
+    int iters = 0;
+    if (n == 0) return 0;  // ks_multicg_offset.cpp:218-225
+    QPHIX_status_t s = guarded([&] {
+        require_init();
+        Context &c = ctx();
+        if (!info || !H || !inv || !res || !mass || !out || !in || n < 0) throw Error("asqtad_invert_multi: bad argument");
+        if (!(in->parity == out[0]->parity && in->parity == inv->parity))  // :232
+            throw Error("asqtad_invert_multi: in, out[0] and inv_arg parities differ");
+        if (inv->max <= 0 || inv->nrestart < 0) throw Error("asqtad_invert_multi: bad iteration limits");
+        c.stats = Stats();
+        MultiArgs a;
+        a.info = info;
+        a.inv = inv;
+        a.res = res;
+        std::vector<double> m(mass, mass + n);
+        a.mass = m.data();
+        a.n = n;
+        for (int j = 0; j < n; ++j) {
+            if (!out[j] || !res[j]) throw Error("asqtad_invert_multi: NULL out or res entry");
+            a.out[0].push_back(out[j]->blk[0]);
+            a.out[1].push_back(out[j]->blk[1]);
+        }
+        a.in[0] = in->blk[0];
+        a.in[1] = in->blk[1];
+        QB_CUDA(cudaEventRecord(c.ev_solve[0], c.stream));
+        Prec inner = Api<Real>::prec;
+        if constexpr (std::is_same<Real, double>::value) inner = c.inner;
+        if (inner == Api<Real>::prec) {
+            iters = multishift_reference(Api<Real>::prec, H->links, a);
+        } else if constexpr (std::is_same<Real, double>::value) {
+            LinkSet *lss;
+            if (inner == Prec::Single) {
+                if (!H->sloppy_single.valid) {
+                    H->sloppy_single = alloc_links(Prec::Single);
+                    links_convert(Prec::Single, H->sloppy_single, Prec::Double, H->links, c.launch());
+                }
+                lss = &H->sloppy_single;
+            } else {
+                if (!H->sloppy_half.valid) {
+                    H->sloppy_half = alloc_links(Prec::Half);
+                    links_absmax(Prec::Double, H->links, H->sloppy_half, c.launch(), c.d_partials);
+                    links_convert(Prec::Half, H->sloppy_half, Prec::Double, H->links, c.launch());
+                }
+                lss = &H->sloppy_half;
+            }
+            iters = multishift_mixed(inner, H->links, *lss, a);
+        } else {
+            throw Error("asqtad_invert_multi: mixed precision is available through the D3 API");
+        }
+        QB_CUDA(cudaEventRecord(c.ev_solve[1], c.stream));
+        QB_CUDA(cudaEventSynchronize(c.ev_solve[1]));
+        float ms = 0;
+        QB_CUDA(cudaEventElapsedTime(&ms, c.ev_solve[0], c.ev_solve[1]));
+        c.stats.solve_ms = ms;
+        QB_CUDA(cudaGetLastError());
+    });
+    if (s != QPHIX_SUCCESS && info) info->status = s;
+    return iters;
+}
+
+template <typename Real>
+QPHIX_status_t dslash_timed(void *links, void *out, void *in, QPHIX_evenodd_t parity, int reps, double *ms)
+{
+    return guarded([&] {
+        require_init();
+        Context &c = ctx();
+        auto *H = static_cast<typename Api<Real>::FL *>(links);
+        auto *O = static_cast<typename Api<Real>::CV *>(out);
+        auto *I = static_cast<typename Api<Real>::CV *>(in);
+        if (!H || !O || !I || !ms || reps <= 0) throw Error("dslash_timed: bad argument");
+        if (parity != QPHIX_EVEN && parity != QPHIX_ODD) throw Error("dslash_timed: parity must be EVEN or ODD");
+        const int cb = parity == QPHIX_EVEN ? 0 : 1;
+        if (!O->blk[cb].data || !I->blk[1 - cb].data) throw Error("dslash_timed: vectors lack the needed parity");
+        QB_CUDA(cudaEventRecord(c.ev_user[0], c.stream));
+        for (int r = 0; r < reps; ++r)
+            dslash(Api<Real>::prec, c.launch(), O->blk[cb], I->blk[1 - cb], H->links, cb);
+        QB_CUDA(cudaEventRecord(c.ev_user[1], c.stream));
+        QB_CUDA(cudaEventSynchronize(c.ev_user[1]));
+        float t = 0;
+        QB_CUDA(cudaEventElapsedTime(&t, c.ev_user[0], c.ev_user[1]));
+        *ms = t / reps;
+        QB_CUDA(cudaGetLastError());
+    });
+}
+
+void not_on_path(QPHIX_info_t *info, const char *what)
+{
+    ctx().last_error = std::string(what) + ": the gauge force is not part of this library's solver path";
+    if (info) info->status = QPHIX_FAIL;
+}
+
+}  // namespace
+
+#pragma GCC visibility push(default)
+extern "C" {
+
+// ----------------------------------------------------------- init/finalize --
+QPHIX_status_t QPHIX_init_F(QPHIX_layout_t *layout) { return guarded([&] { init_context(layout); }); }
+QPHIX_status_t QPHIX_init_D(QPHIX_layout_t *layout) { return guarded([&] { init_context(layout); }); }
+QPHIX_status_t QPHIX_init(QPHIX_layout_t *layout)
+{
+    return (QPHIX_status_t)(QPHIX_init_F(layout) | QPHIX_init_D(layout));
+}
+QPHIX_status_t QPHIX_finalize_F() { return guarded([&] { finalize_context(); }); }
+QPHIX_status_t QPHIX_finalize_D() { return guarded([&] { finalize_context(); }); }
+QPHIX_status_t QPHIX_finalize() { return (QPHIX_status_t)(QPHIX_finalize_F() | QPHIX_finalize_D()); }
+
+// ------------------------------------------------------------------- F3 --
+QPHIX_F3_ColorVector *QPHIX_F3_create_V_from_raw(QPHIX_F_Real *src, QPHIX_evenodd_t evenodd) { return create_V<float>(src, evenodd); }
+void QPHIX_F3_extract_V_to_raw(QPHIX_F_Real *dest, QPHIX_F3_ColorVector *src, QPHIX_evenodd_t) { extract_V<float>(dest, src); }
+void QPHIX_F3_destroy_V(QPHIX_F3_ColorVector *V) { destroy_V<float>(V); }
+QPHIX_F3_FermionLinksAsqtad *QPHIX_F3_asqtad_create_L_from_raw(QPHIX_F_Real *fat, QPHIX_F_Real *lng, QPHIX_F_Real *fatback,
+                                                               QPHIX_F_Real *lngback, QPHIX_evenodd_t evenodd)
+{
+    return create_L<float>(fat, lng, fatback, lngback, evenodd);
+}
+void QPHIX_F3_asqtad_extract_L_to_raw(QPHIX_F_Real *fat, QPHIX_F_Real *lng, QPHIX_F3_FermionLinksAsqtad *src,
+                                      QPHIX_evenodd_t evenodd)
+{
+    extract_L<float>(fat, lng, src, evenodd);
+}
+void QPHIX_F3_asqtad_destroy_L(QPHIX_F3_FermionLinksAsqtad *L) { destroy_L<float>(L); }
+void QPHIX_F3_asqtad_dslash(QPHIX_F3_FermionLinksAsqtad *L, QPHIX_F3_ColorVector *out, QPHIX_F3_ColorVector *in,
+                            QPHIX_evenodd_t parity)
+{
+    asqtad_dslash<float>(L, out, in, parity);
+}
+int QPHIX_F3_asqtad_invert(QPHIX_info_t *info, QPHIX_F3_FermionLinksAsqtad *L, QPHIX_invert_arg_t *inv,
+                           QPHIX_resid_arg_t *res, QPHIX_F_Real mass, QPHIX_F3_ColorVector *out, QPHIX_F3_ColorVector *in)
+{
+    return asqtad_invert<float>(info, L, inv, res, mass, out, in);
+}
+int QPHIX_F3_asqtad_invert_multi(QPHIX_info_t *info, QPHIX_F3_FermionLinksAsqtad *L, QPHIX_invert_arg_t *inv,
+                                 QPHIX_resid_arg_t *res[], QPHIX_F_Real *mass, int n, QPHIX_F3_ColorVector *out[],
+                                 QPHIX_F3_ColorVector *in)
+{
+    return asqtad_invert_multi<float>(info, L, inv, res, mass, n, out, in);
+}
+QPHIX_F3_Force *QPHIX_F3_create_F_from_raw(QPHIX_F_Real *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_F3_create_F_from_raw"); return nullptr; }
+void QPHIX_F3_extract_F_to_raw(QPHIX_F_Real *, QPHIX_F3_Force *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_F3_extract_F_to_raw"); }
+void QPHIX_F3_destroy_F(QPHIX_F3_Force *) {}
+QPHIX_F3_GaugeField *QPHIX_F3_create_G_from_raw(QPHIX_F_Real *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_F3_create_G_from_raw"); return nullptr; }
+void QPHIX_F3_extract_G_to_raw(QPHIX_F_Real *, QPHIX_F3_GaugeField *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_F3_extract_G_to_raw"); }
+void QPHIX_F3_destroy_G(QPHIX_F3_GaugeField *) {}
+void QPHIX_F3_symanzik_1loop_gauge_force(QPHIX_info_t *info, QPHIX_F3_GaugeField *, QPHIX_F3_Force *,
+                                         QPHIX_gauge_coeffs_t *, QPHIX_F_Real)
+{
+    not_on_path(info, "QPHIX_F3_symanzik_1loop_gauge_force");
+}
+
+// ------------------------------------------------------------------- D3 --
+QPHIX_D3_ColorVector *QPHIX_D3_create_V_from_raw(QPHIX_D_Real *src, QPHIX_evenodd_t evenodd) { return create_V<double>(src, evenodd); }
+void QPHIX_D3_extract_V_to_raw(QPHIX_D_Real *dest, QPHIX_D3_ColorVector *src, QPHIX_evenodd_t) { extract_V<double>(dest, src); }
+void QPHIX_D3_destroy_V(QPHIX_D3_ColorVector *V) { destroy_V<double>(V); }
+QPHIX_D3_FermionLinksAsqtad *QPHIX_D3_asqtad_create_L_from_raw(QPHIX_D_Real *fat, QPHIX_D_Real *lng, QPHIX_D_Real *fatback,
+                                                               QPHIX_D_Real *lngback, QPHIX_evenodd_t evenodd)
+{
+    return create_L<double>(fat, lng, fatback, lngback, evenodd);
+}
+void QPHIX_D3_asqtad_extract_L_to_raw(QPHIX_D_Real *fat, QPHIX_D_Real *lng, QPHIX_D3_FermionLinksAsqtad *src,
+                                      QPHIX_evenodd_t evenodd)
+{
+    extract_L<double>(fat, lng, src, evenodd);
+}
+void QPHIX_D3_asqtad_destroy_L(QPHIX_D3_FermionLinksAsqtad *L) { destroy_L<double>(L); }
+void QPHIX_D3_asqtad_dslash(QPHIX_D3_FermionLinksAsqtad *L, QPHIX_D3_ColorVector *out, QPHIX_D3_ColorVector *in,
+                            QPHIX_evenodd_t parity)
+{
+    asqtad_dslash<double>(L, out, in, parity);
+}
+int QPHIX_D3_asqtad_invert(QPHIX_info_t *info, QPHIX_D3_FermionLinksAsqtad *L, QPHIX_invert_arg_t *inv,
+                           QPHIX_resid_arg_t *res, QPHIX_D_Real mass, QPHIX_D3_ColorVector *out, QPHIX_D3_ColorVector *in)
+{
+    return asqtad_invert<double>(info, L, inv, res, mass, out, in);
+}
+int QPHIX_D3_asqtad_invert_multi(QPHIX_info_t *info, QPHIX_D3_FermionLinksAsqtad *L, QPHIX_invert_arg_t *inv,
+                                 QPHIX_resid_arg_t *res[], QPHIX_D_Real *mass, int n, QPHIX_D3_ColorVector *out[],
+                                 QPHIX_D3_ColorVector *in)
+{
+    return asqtad_invert_multi<double>(info, L, inv, res, mass, n, out, in);
+}
+QPHIX_D3_Force *QPHIX_D3_create_F_from_raw(QPHIX_D_Real *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_D3_create_F_from_raw"); return nullptr; }
+void QPHIX_D3_extract_F_to_raw(QPHIX_D_Real *, QPHIX_D3_Force *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_D3_extract_F_to_raw"); }
+void QPHIX_D3_destroy_F(QPHIX_D3_Force *) {}
+QPHIX_D3_GaugeField *QPHIX_D3_create_G_from_raw(QPHIX_D_Real *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_D3_create_G_from_raw"); return nullptr; }
+void QPHIX_D3_extract_G_to_raw(QPHIX_D_Real *, QPHIX_D3_GaugeField *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_D3_extract_G_to_raw"); }
+void QPHIX_D3_destroy_G(QPHIX_D3_GaugeField *) {}
+void QPHIX_D3_symanzik_1loop_gauge_force(QPHIX_info_t *info, QPHIX_D3_GaugeField *, QPHIX_D3_Force *,
+                                         QPHIX_gauge_coeffs_t *, QPHIX_D_Real)
+{
+    not_on_path(info, "QPHIX_D3_symanzik_1loop_gauge_force");
+}
+
+// --------------------------------------------------------------- B200 API --
+QPHIX_status_t QPHIX_B200_set_inner_precision(QPHIX_B200_precision_t p)
+{
+    return guarded([&] {
+        if (p != QPHIX_B200_PREC_HALF && p != QPHIX_B200_PREC_SINGLE && p != QPHIX_B200_PREC_DOUBLE)
+            throw Error("set_inner_precision: unknown precision");
+        ctx().inner = static_cast<Prec>(p);
+    });
+}
+QPHIX_B200_precision_t QPHIX_B200_get_inner_precision(void) { return static_cast<QPHIX_B200_precision_t>(ctx().inner); }
+QPHIX_status_t QPHIX_B200_set_reliable_delta(double delta)
+{
+    return guarded([&] {
+        if (!(delta > 0 && delta < 1)) throw Error("set_reliable_delta: delta must lie in (0, 1)");
+        ctx().reliable_delta = delta;
+    });
+}
+QPHIX_status_t QPHIX_B200_get_last_stats(QPHIX_B200_stats_t *s)
+{
+    return guarded([&] {
+        if (!s) throw Error("get_last_stats: NULL");
+        const Stats &t = ctx().stats;
+        s->solve_ms = t.solve_ms;
+        s->iterations = t.iterations;
+        s->reliable_updates = t.reliable_updates;
+        s->dslash_launches = t.dslash_launches;
+        s->dslash_ms = t.dslash_ms;
+        s->mdagm_launches = t.mdagm_launches;
+        s->mdagm_ms = t.mdagm_ms;
+        s->true_rsq = t.true_rsq;
+    });
+}
+QPHIX_status_t QPHIX_B200_set_kernel_timing(int on) { return guarded([&] { ctx().kernel_timing = on ? 1 : 0; }); }
+QPHIX_status_t QPHIX_B200_timer_start(void)
+{
+    return guarded([&] {
+        require_init();
+        QB_CUDA(cudaEventRecord(ctx().ev_user[0], ctx().stream));
+    });
+}
+QPHIX_status_t QPHIX_B200_timer_stop(double *ms)
+{
+    return guarded([&] {
+        require_init();
+        if (!ms) throw Error("timer_stop: NULL");
+        Context &c = ctx();
+        QB_CUDA(cudaEventRecord(c.ev_user[1], c.stream));
+        QB_CUDA(cudaEventSynchronize(c.ev_user[1]));
+        float t = 0;
+        QB_CUDA(cudaEventElapsedTime(&t, c.ev_user[0], c.ev_user[1]));
+        *ms = t;
+    });
+}
+QPHIX_status_t QPHIX_B200_F3_dslash_timed(void *links, void *out, void *in, QPHIX_evenodd_t parity, int reps, double *ms)
+{
+    return dslash_timed<float>(links, out, in, parity, reps, ms);
+}
+QPHIX_status_t QPHIX_B200_D3_dslash_timed(void *links, void *out, void *in, QPHIX_evenodd_t parity, int reps, double *ms)
+{
+    return dslash_timed<double>(links, out, in, parity, reps, ms);
+}
+long QPHIX_B200_neighbor_index(const int L[4], int cb, long site, int k)
+{
+    if (!L || k < 0 || k > 15 || (cb & ~1)) return -1;
+    const Geom g = make_geom(L[0], L[1], L[2], L[3]);
+    if (site < 0 || site >= g.vh) return -1;
+    const SiteCoords s = decode(g, cb, (int)site);
+    return neighbor(g, s, k);
+}
+const char *QPHIX_B200_last_error(void) { return ctx().last_error.c_str(); }
+int QPHIX_B200_version(void) { return 100; }
+
+}  // extern "C"
+#pragma GCC visibility pop

@@ -1,0 +1,504 @@
+// Solver BLAS kernels (K3, K4, K5): one thread per site, all six reals of
+// the site in registers, FP64 reductions finished in the last block.
+//
+// Reference: the CG BLAS of ks_d_congrad_fn.cpp:62-188 (calc_source_norm,
+// calc_rsq, calc_rsq2, calc_pkp, axpy), the multi-shift BLAS of
+// ks_multicg_offset.cpp:69-184 (calc_rsq2, update_dest, update_pm) and
+// relative_residue (ks_blas_utils_c.cpp:110-149).  The reference accumulates
+// in its fptype; here every reduction accumulates in FP64 and the step sizes
+// are rounded to the solve precision exactly where the reference assigns
+// them to an fptype variable.
+#include "device_common.cuh"
+
+namespace qb {
+
+// ------------------------------------------------------------------ norms --
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+k_norm2(VecView<S> v, SolverState *st, double *partials, int which, double *out)
+{
+    using A = typename Acc<S>::type;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    double s[1] = {0.0};
+    if (j < v.vh) {
+        A a[6];
+        v.load_cg(j, a);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s[0] += (double)(a[i] * a[i]);
+    }
+    grid_reduce<1>(s, partials, &st->counter2, [&](const double *t) {
+        if (which == 0) st->source_norm = t[0];
+        else if (which == 1) st->rsq = t[0];
+        if (out) *out = t[0];
+    });
+}
+
+// per-site |r|^2/|x|^2 term of relative_residue (ks_blas_utils_c.cpp:110-134)
+template <typename A>
+__device__ __forceinline__ double relres_term(const A r[6], const A x[6])
+{
+    double num = 0, den = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        num += (double)(r[i] * r[i]);
+        den += (double)(x[i] * x[i]);
+    }
+    if (num == 0) return 0.0;
+    return den == 0 ? 1.0 : num / den;
+}
+
+// ---------------------------------------------------------- CG restart --
+// calc_rsq (ks_d_congrad_fn.cpp:82-99): ttt += (-m4) x; r = b + ttt; p = r;
+// rsq = |r|^2 (+ relative residue sum when requested)
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+k_cg_restart(VecView<S> ttt, VecView<S> x, VecView<S> b, VecView<S> r, VecView<S> pv, bool setp,
+             SolverState *st, double *partials, bool relres, double *out)
+{
+    using A = typename Acc<S>::type;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    double s[2] = {0.0, 0.0};
+    if (j < ttt.vh) {
+        A t[6], xv[6], bv[6], rv[6];
+        ttt.load_cg(j, t);
+        x.load_cg(j, xv);
+        b.load_cg(j, bv);
+        const A m = (A)(-st->msq_x4);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            t[i] = t[i] + m * xv[i];
+            rv[i] = bv[i] + t[i];
+        }
+        ttt.store(j, t);
+        r.store(j, rv);
+        if constexpr (std::is_same<S, __half>::value) r.load(j, rv);
+        if (setp) pv.store(j, rv);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
+        if (relres) s[1] = relres_term(rv, xv);
+    }
+    grid_reduce<2>(s, partials, &st->counter2, [&](const double *t) {
+        if (out) {
+            out[0] = t[0];
+        } else {
+            st->rsq = t[0];
+            st->relrsq = t[1];
+        }
+    });
+}
+
+// --------------------------------------------------------- CG iteration --
+// calc_rsq2 (ks_d_congrad_fn.cpp:131-147): x += a p; r += a ttt; rsq = |r|^2
+// followed by the scalar bookkeeping of :543-566 and the completion test at
+// the top of the loop (:360-363), evaluated on the device.
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+k_cg_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverState *st,
+            double *partials, int gate, bool relres, int V)
+{
+    using A = typename Acc<S>::type;
+    if (gated_off(st, gate)) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    double s[2] = {0.0, 0.0};
+    if (j < x.vh) {
+        A xv[6], p[6], rv[6], t[6];
+        x.load_cg(j, xv);
+        pv.load_cg(j, p);
+        r.load_cg(j, rv);
+        ttt.load_cg(j, t);
+        const A a = (A)st->a;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            xv[i] = xv[i] + a * p[i];
+            rv[i] = rv[i] + a * t[i];
+        }
+        x.store(j, xv);
+        r.store(j, rv);
+        if constexpr (std::is_same<S, __half>::value) {
+            r.load(j, rv);
+            x.load(j, xv);
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
+        if (relres) s[1] = relres_term(rv, xv);
+    }
+    grid_reduce<2>(s, partials, &st->counter, [&](const double *t) {
+        const int single = st->prec_single;
+        const double oldrsq = st->rsq;
+        const double rsq = t[0];
+        st->oldrsq = oldrsq;
+        st->rsq = rsq;
+        double relrsq = st->relrsq;
+        if (relres) relrsq = round_to(sqrt(2.0 * t[1] / (double)V), single);
+        st->relrsq = relrsq;
+        st->size_r = round_to(rsq, single) / st->source_norm;
+        st->size_relr = round_to(relrsq, single);
+        st->b = round_to(round_to(rsq, single) / oldrsq, single);
+        const bool conv = (st->rsqmin <= 0 || st->rsqmin > st->size_r) &&
+                          (st->relrsqmin <= 0 || st->relrsqmin > st->size_relr);
+        if ((st->iteration % st->niter == 0) || conv) st->stop_at = gate;
+    });
+}
+
+// axpy (ks_d_congrad_fn.cpp:178-188): p = r + b p
+template <typename S>
+__global__ void __launch_bounds__(kBlock) k_cg_axpy(VecView<S> r, VecView<S> pv, SolverState *st, int gate)
+{
+    using A = typename Acc<S>::type;
+    if (gated_off(st, gate)) return;
+    if (gate >= 0 && st->axpy_skip_at == gate) return;  // p update redone by the host (mixed RU)
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= r.vh) return;
+    A rv[6], p[6];
+    r.load_cg(j, rv);
+    pv.load_cg(j, p);
+    const A b = (A)st->b;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) p[i] = rv[i] + b * p[i];
+    pv.store(j, p);
+}
+
+// ------------------------------------------------------------ multi-shift --
+// calc_rsq2 (ks_multicg_offset.cpp:124-140) + the convergence test (:520)
+// + the alpha recurrences (:587-598), evaluated on the device.
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+k_ms_residual(VecView<S> r, VecView<S> ttt, SolverState *st, double *partials, int gate)
+{
+    using A = typename Acc<S>::type;
+    if (gated_off(st, gate)) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    double s[1] = {0.0};
+    if (j < r.vh) {
+        A rv[6], t[6];
+        r.load_cg(j, rv);
+        ttt.load_cg(j, t);
+        const A bl = (A)st->beta_i[st->j_low];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) rv[i] = rv[i] + bl * t[i];
+        r.store(j, rv);
+        if constexpr (std::is_same<S, __half>::value) r.load(j, rv);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
+    }
+    grid_reduce<1>(s, partials, &st->counter, [&](const double *t) {
+        const int single = st->prec_single;
+        const double oldrsq = st->rsq;
+        const double rsq = t[0];
+        st->oldrsq = oldrsq;
+        st->rsq = rsq;
+        if (rsq <= st->rsqstop) {
+            st->converged = 1;
+            st->stop_at = gate;
+            return;
+        }
+        const int jl = st->j_low;
+        st->alpha[jl] = round_to(rsq / oldrsq, single);
+        for (int k = 0; k < st->num_now; ++k) {
+            if (k == jl) continue;
+            const double zb = round_to(st->zeta_i[k] * st->beta_i[jl], single);
+            if (zb != 0.0)
+                st->alpha[k] = round_to(round_to(round_to(st->alpha[jl] * st->zeta_ip1[k], single) *
+                                                 st->beta_i[k], single) / zb, single);
+            else { st->alpha[k] = 0.0; st->finished[k] = 1; }
+        }
+        if (st->iteration >= st->max_cg) st->stop_at = gate;
+    });
+}
+
+// update_pm / update_dest (ks_multicg_offset.cpp:142-184) for every active
+// shift in one pass over the sites: r is read once, x_j and p_j once each.
+template <typename S, typename X>
+__global__ void __launch_bounds__(kBlock)
+k_ms_update(VecBlock *xs, VecBlock *ps, VecView<S> r, int n, SolverState *st, int gate)
+{
+    using A = typename Acc<S>::type;
+    using AX = typename Acc<X>::type;
+    if (gated_off(st, gate)) return;
+    __shared__ double sb[kMaxShifts], sz[kMaxShifts], sa[kMaxShifts];
+    const int nn = st->num_now;
+    const bool conv = st->converged;
+    for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+        sb[k] = st->beta_i[k];
+        sz[k] = st->zeta_ip1[k];
+        sa[k] = st->alpha[k];
+    }
+    __syncthreads();
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= r.vh) return;
+    A rv[6];
+    if (!conv) r.load_cg(j, rv);
+    for (int k = 0; k < nn; ++k) {
+        VecView<S> pk = view<S>(ps[k], r.vh);
+        VecView<X> xk = view<X>(xs[k], r.vh);
+        A p[6];
+        AX xv[6];
+        pk.load_cg(j, p);
+        xk.load_cg(j, xv);
+        const AX bk = (AX)sb[k];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) xv[i] = xv[i] + bk * (AX)p[i];
+        xk.store(j, xv);
+        if (!conv) {
+            const A ak = (A)sa[k];
+            const double zk = sz[k];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                const A tt = (A)((double)rv[i] * zk);
+                p[i] = tt + ak * p[i];
+            }
+            pk.store(j, p);
+        }
+    }
+}
+
+// ------------------------------------------------- mixed-precision inner CG --
+// x_s += a p; r_s += a ttt; rsq = |r_s|^2; b = rsq/oldrsq; request a
+// reliable update when |r_s|^2 < delta^2 |r_RU|^2 or the sloppy residual
+// passes the target.  The request cancels this iteration's p update, which the
+// host redoes with the true residual.
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+k_mx_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverState *st,
+            double *partials, int gate, double delta2)
+{
+    using A = typename Acc<S>::type;
+    if (gated_off(st, gate)) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    double s[1] = {0.0};
+    if (j < x.vh) {
+        A xv[6], p[6], rv[6], t[6];
+        x.load_cg(j, xv);
+        pv.load_cg(j, p);
+        r.load_cg(j, rv);
+        ttt.load_cg(j, t);
+        const A a = (A)st->a;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            xv[i] = xv[i] + a * p[i];
+            rv[i] = rv[i] + a * t[i];
+        }
+        x.store(j, xv);
+        r.store(j, rv);
+        if constexpr (std::is_same<S, __half>::value) r.load(j, rv);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
+    }
+    grid_reduce<1>(s, partials, &st->counter, [&](const double *t) {
+        const double oldrsq = st->rsq;
+        const double rsq = t[0];
+        st->oldrsq = oldrsq;
+        st->rsq = rsq;
+        st->b = rsq / oldrsq;
+        const bool ru = (rsq < delta2 * st->rsq_ru) || (rsq <= st->rsqstop) ||
+                        (st->iteration >= st->max_cg) || !(rsq == rsq);
+        if (ru) {
+            st->stop_at = gate;
+            st->axpy_skip_at = gate;  // this iteration's p update waits for the true residual
+        }
+    });
+}
+
+// -------------------------------------------------------------- elementwise --
+template <typename D, typename S>
+__global__ void __launch_bounds__(kBlock) k_copy(VecView<D> d, VecView<S> s)
+{
+    using AD = typename Acc<D>::type;
+    using AS = typename Acc<S>::type;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= d.vh) return;
+    AS a[6];
+    AD b[6];
+    s.load_cg(j, a);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) b[i] = (AD)a[i];
+    d.store(j, b);
+}
+
+template <typename Y, typename X>
+__global__ void __launch_bounds__(kBlock) k_add(VecView<Y> y, VecView<X> x)
+{
+    using AY = typename Acc<Y>::type;
+    using AX = typename Acc<X>::type;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= y.vh) return;
+    AX a[6];
+    AY b[6];
+    x.load_cg(j, a);
+    y.load_cg(j, b);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) b[i] = b[i] + (AY)a[i];
+    y.store(j, b);
+}
+
+// --------------------------------------------------------------- dispatch --
+#define QB_DISPATCH(p, F, ...)                               \
+    switch (p) {                                             \
+    case Prec::Double: F<double>(__VA_ARGS__); break;        \
+    case Prec::Single: F<float>(__VA_ARGS__); break;         \
+    case Prec::Half: F<__half>(__VA_ARGS__); break;          \
+    }
+
+template <typename S>
+static void norm2_impl(const Launch &L, VecBlock v, SolverState *st, double *partials, int which, double *out)
+{
+    k_norm2<S><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(view<S>(v, L.g->vh), st, partials, which, out);
+}
+
+void norm2_to_state(Prec p, const Launch &L, VecBlock v, SolverState *st, double *partials, int which)
+{
+    QB_DISPATCH(p, norm2_impl, L, v, st, partials, which, nullptr);
+}
+
+template <typename S>
+static void restart_impl(const Launch &L, VecBlock ttt, VecBlock x, VecBlock b, VecBlock r,
+                         VecBlock pv, bool setp, SolverState *st, double *partials, bool relres,
+                         double *out)
+{
+    const int vh = L.g->vh;
+    k_cg_restart<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(ttt, vh), view<S>(x, vh), view<S>(b, vh),
+                                                           view<S>(r, vh), view<S>(pv, vh), setp, st,
+                                                           partials, relres, out);
+}
+
+void cg_restart_residual(Prec p, const Launch &L, VecBlock ttt, VecBlock x, VecBlock b, VecBlock r,
+                         VecBlock pv, SolverState *st, double *partials, bool relres)
+{
+    QB_DISPATCH(p, restart_impl, L, ttt, x, b, r, pv, true, st, partials, relres, nullptr);
+}
+
+template <typename S>
+static void update_impl(const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlock ttt,
+                        SolverState *st, double *partials, int gate, bool relres)
+{
+    const int vh = L.g->vh;
+    k_cg_update<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(x, vh), view<S>(pv, vh), view<S>(r, vh),
+                                                          view<S>(ttt, vh), st, partials, gate, relres,
+                                                          2 * vh);
+}
+
+void cg_update(Prec p, const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlock ttt,
+               SolverState *st, double *partials, int gate, bool relres)
+{
+    QB_DISPATCH(p, update_impl, L, x, pv, r, ttt, st, partials, gate, relres);
+}
+
+template <typename S>
+static void axpy_impl(const Launch &L, VecBlock r, VecBlock pv, SolverState *st, int gate)
+{
+    const int vh = L.g->vh;
+    k_cg_axpy<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(r, vh), view<S>(pv, vh), st, gate);
+}
+
+void cg_axpy(Prec p, const Launch &L, VecBlock r, VecBlock pv, SolverState *st, int gate)
+{
+    QB_DISPATCH(p, axpy_impl, L, r, pv, st, gate);
+}
+
+template <typename S>
+static void msres_impl(const Launch &L, VecBlock r, VecBlock ttt, SolverState *st, double *partials, int gate)
+{
+    const int vh = L.g->vh;
+    k_ms_residual<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(r, vh), view<S>(ttt, vh), st, partials, gate);
+}
+
+void ms_residual(Prec p, const Launch &L, VecBlock r, VecBlock ttt, SolverState *st, double *partials, int gate)
+{
+    QB_DISPATCH(p, msres_impl, L, r, ttt, st, partials, gate);
+}
+
+void ms_update(Prec p, const Launch &L, Prec xprec, VecBlock *x, VecBlock *pv, VecBlock r, int n,
+               SolverState *st, int gate)
+{
+    const int vh = L.g->vh;
+    const int grid = grid_for(vh);
+    if (xprec == Prec::Double && p == Prec::Double)
+        k_ms_update<double, double><<<grid, kBlock, 0, L.stream>>>(x, pv, view<double>(r, vh), n, st, gate);
+    else if (xprec == Prec::Double && p == Prec::Single)
+        k_ms_update<float, double><<<grid, kBlock, 0, L.stream>>>(x, pv, view<float>(r, vh), n, st, gate);
+    else if (xprec == Prec::Double && p == Prec::Half)
+        k_ms_update<__half, double><<<grid, kBlock, 0, L.stream>>>(x, pv, view<__half>(r, vh), n, st, gate);
+    else if (xprec == Prec::Single && p == Prec::Single)
+        k_ms_update<float, float><<<grid, kBlock, 0, L.stream>>>(x, pv, view<float>(r, vh), n, st, gate);
+    else if (xprec == Prec::Single && p == Prec::Half)
+        k_ms_update<__half, float><<<grid, kBlock, 0, L.stream>>>(x, pv, view<__half>(r, vh), n, st, gate);
+}
+
+template <typename S>
+static void mx_impl(const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlock ttt, SolverState *st,
+                    double *partials, int gate, double delta2)
+{
+    const int vh = L.g->vh;
+    k_mx_update<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(x, vh), view<S>(pv, vh), view<S>(r, vh),
+                                                          view<S>(ttt, vh), st, partials, gate, delta2);
+}
+
+void mx_update(Prec p, const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlock ttt,
+               SolverState *st, double *partials, int gate, double delta2)
+{
+    QB_DISPATCH(p, mx_impl, L, x, pv, r, ttt, st, partials, gate, delta2);
+}
+
+template <typename D, typename S>
+static void copy2(const Launch &L, VecBlock d, VecBlock s)
+{
+    const int vh = L.g->vh;
+    k_copy<D, S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<D>(d, vh), view<S>(s, vh));
+}
+
+template <typename D>
+static void copy1(const Launch &L, VecBlock d, Prec sp, VecBlock s)
+{
+    switch (sp) {
+    case Prec::Double: copy2<D, double>(L, d, s); break;
+    case Prec::Single: copy2<D, float>(L, d, s); break;
+    case Prec::Half: copy2<D, __half>(L, d, s); break;
+    }
+}
+
+void vec_copy(Prec dst_p, VecBlock dst, Prec src_p, VecBlock src, const Launch &L)
+{
+    QB_DISPATCH(dst_p, copy1, L, dst, src_p, src);
+}
+
+void vec_zero(Prec p, VecBlock v, const Launch &L)
+{
+    const size_t n = (size_t)3 * L.g->vh * (p == Prec::Double ? 16 : (p == Prec::Single ? 8 : 4));
+    cudaMemsetAsync(v.data, 0, n, L.stream);
+    if (p == Prec::Half) cudaMemsetAsync(v.norm, 0, sizeof(float) * L.g->vh, L.stream);
+}
+
+template <typename Y, typename X>
+static void add2(const Launch &L, VecBlock y, VecBlock x)
+{
+    const int vh = L.g->vh;
+    k_add<Y, X><<<grid_for(vh), kBlock, 0, L.stream>>>(view<Y>(y, vh), view<X>(x, vh));
+}
+
+template <typename Y>
+static void add1(const Launch &L, VecBlock y, Prec xp, VecBlock x)
+{
+    switch (xp) {
+    case Prec::Double: add2<Y, double>(L, y, x); break;
+    case Prec::Single: add2<Y, float>(L, y, x); break;
+    case Prec::Half: add2<Y, __half>(L, y, x); break;
+    }
+}
+
+void vec_add(Prec yp, VecBlock y, Prec xp, VecBlock x, const Launch &L)
+{
+    QB_DISPATCH(yp, add1, L, y, xp, x);
+}
+
+void cg_true_residual(Prec p, const Launch &L, VecBlock ttt, VecBlock x, VecBlock b, VecBlock r,
+                      SolverState *st, double *partials, double *out)
+{
+    QB_DISPATCH(p, restart_impl, L, ttt, x, b, r, r, false, st, partials, false, out);
+}
+
+void norm2_dev(Prec p, const Launch &L, VecBlock v, SolverState *st, double *partials, double *out)
+{
+    QB_DISPATCH(p, norm2_impl, L, v, st, partials, 2, out);
+}
+
+}  // namespace qb

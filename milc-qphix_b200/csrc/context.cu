@@ -1,0 +1,92 @@
+// Context, device memory and state transfer helpers.
+#include "context.h"
+
+namespace qb {
+
+Context &ctx()
+{
+    static Context c;
+    return c;
+}
+
+double wall_seconds()
+{
+    using namespace std::chrono;
+    return duration<double>(system_clock::now().time_since_epoch()).count();
+}
+
+void *dev_alloc(size_t bytes)
+{
+    void *p = nullptr;
+    if (bytes == 0) return nullptr;
+    QB_CUDA(cudaMallocAsync(&p, bytes, ctx().stream));
+    return p;
+}
+
+void dev_free(void *p)
+{
+    if (p) cudaFreeAsync(p, ctx().stream);
+}
+
+static size_t cx_bytes(Prec p) { return p == Prec::Double ? 16 : (p == Prec::Single ? 8 : 4); }
+
+VecBlock alloc_vec(Prec p)
+{
+    Context &c = ctx();
+    VecBlock b;
+    const size_t n = (size_t)3 * c.g.vh;
+    b.data = dev_alloc(n * cx_bytes(p));
+    QB_CUDA(cudaMemsetAsync(b.data, 0, n * cx_bytes(p), c.stream));
+    if (p == Prec::Half) {
+        b.norm = static_cast<float *>(dev_alloc(sizeof(float) * c.g.vh));
+        QB_CUDA(cudaMemsetAsync(b.norm, 0, sizeof(float) * c.g.vh, c.stream));
+    }
+    return b;
+}
+
+void free_vec(VecBlock &b)
+{
+    dev_free(b.data);
+    dev_free(b.norm);
+    b.data = nullptr;
+    b.norm = nullptr;
+}
+
+LinkSet alloc_links(Prec p)
+{
+    Context &c = ctx();
+    LinkSet ls;
+    const size_t bytes = (size_t)kMats * 9 * c.g.vh * cx_bytes(p);
+    for (int cb = 0; cb < 2; ++cb) {
+        ls.blk[cb] = dev_alloc(bytes);
+        QB_CUDA(cudaMemsetAsync(ls.blk[cb], 0, bytes, c.stream));
+    }
+    ls.valid = true;
+    return ls;
+}
+
+void free_links(LinkSet &ls)
+{
+    for (int cb = 0; cb < 2; ++cb) {
+        dev_free(ls.blk[cb]);
+        ls.blk[cb] = nullptr;
+    }
+    ls.valid = false;
+}
+
+void upload_state()
+{
+    Context &c = ctx();
+    QB_CUDA(cudaMemcpyAsync(c.d_state, c.h_state, sizeof(SolverState), cudaMemcpyHostToDevice, c.stream));
+    // the pinned mirror is edited again right after; let the copy land first
+    QB_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+void download_state()
+{
+    Context &c = ctx();
+    QB_CUDA(cudaMemcpyAsync(c.h_state, c.d_state, sizeof(SolverState), cudaMemcpyDeviceToHost, c.stream));
+    QB_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+}  // namespace qb

@@ -1,0 +1,172 @@
+// Internal definitions of libqphix_b200: device field layouts, the global
+// context, handle structures and the kernel launcher interface.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <type_traits>
+
+#include "geometry.cuh"
+
+namespace qb {
+
+// ----------------------------------------------------------------------------
+// Field layouts in HBM (one parity block of Vh sites each)
+//
+// Colour vector  : 3 complex components, component-major, site-minor:
+//                  c2[c*Vh + j]  (double2 / float2).  A warp reading 32
+//                  consecutive sites issues one fully used 512 B / 256 B
+//                  transaction per component.
+// Half vector    : half2 h[c*Vh + j] holding v/norm[j], float norm[j] = max
+//                  |component| of the site (per-site scaling).
+// Link block     : the 16 matrices an output site needs, matrix-major then
+//                  complex element then site: m2[(mat*9 + e)*Vh + j],
+//                  e = 3*row + col, mat = 4*slot + dir with slot
+//                  0 fat forward F_dir(x), 1 fat backward B_dir(x),
+//                  2 Naik forward L_dir(x), 3 Naik backward LB_dir(x).
+//                  Every link is read once per Dslash as a contiguous,
+//                  coalesced stream; nothing about links is gathered.
+//                  The block for output parity cb is built from the raw
+//                  sites cb*Vh + j (qphix_f3.cpp:995-1018).
+// Half links     : short2 fixed point per complex, value = q * link_max/32767
+//                  with one range for the fat slots and one for the Naik
+//                  slots (Naik links are ~1/24 the size of fat links).
+// ----------------------------------------------------------------------------
+constexpr int kMats = 16;
+constexpr int kLinkReals = kMats * 18;  // reals per site in a link block
+
+template <typename R> struct Cx;
+template <> struct Cx<double> { using type = double2; };
+template <> struct Cx<float> { using type = float2; };
+template <typename R> using cx_t = typename Cx<R>::type;
+
+enum class Prec : int { Half = 0, Single = 1, Double = 2 };
+
+inline size_t prec_real_bytes(Prec p) { return p == Prec::Double ? 8 : (p == Prec::Single ? 4 : 2); }
+
+// One parity block of a colour vector in device memory.
+struct VecBlock {
+    void *data = nullptr;   // cx_t<R>[3*Vh]   (half: half2[3*Vh])
+    float *norm = nullptr;  // half only: float[Vh]
+};
+
+// Link blocks of both output parities.
+struct LinkSet {
+    void *blk[2] = {nullptr, nullptr};  // cx_t<R>[16*9*Vh] per parity (half: short2)
+    float link_max[2] = {0.f, 0.f};     // half only: fixed-point range of fat / Naik links
+    bool valid = false;
+};
+
+// ----------------------------------------------------------------------------
+// Device-resident scalars of a running solve.  All reductions accumulate in
+// FP64 and finish in the last block of the reducing kernel, in a fixed order
+// (bit-reproducible), so the host never waits inside an iteration.
+// ----------------------------------------------------------------------------
+constexpr int kMaxShifts = 150;  // MAXNDMASS, ks_d_congrad_fn.h:4
+
+struct SolverState {
+    // CG (ks_d_congrad_fn.cpp) and the multi-shift base system
+    double rsq, oldrsq, pkp, relrsq;
+    double a, b;             // step sizes, rounded to the solve precision
+    double source_norm;
+    double size_r, size_relr;
+    double rsqmin, relrsqmin;  // stopping thresholds (squared, relative)
+    double msq_x4;
+    double rsqstop;
+    double rsq_ru;           // mixed CG: |r|^2 at the last reliable update
+    int iteration;           // the reference's `iteration`
+    int niter;               // restart interval (inv_arg->max)
+    int stop_at;             // chunk-local iteration at which the device stopped
+    int converged;           // multi-shift: rsq <= rsqstop seen
+    int prec_single;         // 1: round a, b to float like the F build
+    int num_now;             // multi-shift: active shifts
+    int j_low;
+    int n_shifts;
+    int first_iter;
+    int axpy_skip_at;        // mixed CG: chunk iteration whose p update the host redoes
+    int max_cg;              // multi-shift: iteration cap (max * nrestart)
+    int error;
+    unsigned int counter;    // last-block counter of the grid reductions
+    unsigned int counter2;
+    // multi-shift recurrences (ks_multicg_offset.cpp:475-498, 587-598)
+    double shifts[kMaxShifts];
+    double zeta_i[kMaxShifts], zeta_im1[kMaxShifts], zeta_ip1[kMaxShifts];
+    double beta_i[kMaxShifts], beta_im1[kMaxShifts], alpha[kMaxShifts];
+    int finished[kMaxShifts];
+};
+
+// ----------------------------------------------------------------------------
+// Kernel launchers (implemented in the .cu files)
+// ----------------------------------------------------------------------------
+struct Launch {
+    cudaStream_t stream;
+    const Geom *g;
+};
+
+// out[cb] = D in[1-cb];  links = block of output parity cb
+void dslash(Prec p, const Launch &L, VecBlock out, VecBlock in, const LinkSet &links, int cb);
+// ttt[cb] = D tmp[1-cb] + m4 * p[cb];  state->pkp = sum p.ttt; state->a = -rsq/pkp;
+// `gate`: chunk-local iteration index k, skipped when k > state->stop_at (k < 0: never)
+// mode 0: CG (a from rsq/pkp), mode 1: multi-shift (shift recurrences)
+void dslash_mdagm_dot(Prec p, const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &links,
+                      VecBlock pv, double m4, int cb, SolverState *st, double *partials, int gate,
+                      int mode);
+// plain dslash gated by the chunk iteration (first half of M^dag M)
+void dslash_gated(Prec p, const Launch &L, VecBlock out, VecBlock in, const LinkSet &links,
+                  int cb, SolverState *st, int gate);
+
+// BLAS (blas.cu) ---------------------------------------------------------------
+// state->source_norm = |v|^2
+void norm2_to_state(Prec p, const Launch &L, VecBlock v, SolverState *st, double *partials,
+                    int which);
+// calc_rsq (ks_d_congrad_fn.cpp:82-99): ttt += (-m4) x; r = b + ttt; p = r; rsq = |r|^2
+void cg_restart_residual(Prec p, const Launch &L, VecBlock ttt, VecBlock x, VecBlock b,
+                         VecBlock r, VecBlock pv, SolverState *st, double *partials, bool relres);
+// calc_rsq2 (:131-147) + stop test: x += a p; r += a ttt; rsq = |r|^2 -> b, size_r
+void cg_update(Prec p, const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlock ttt,
+               SolverState *st, double *partials, int gate, bool relres);
+// axpy (:178-188): p = r + b p
+void cg_axpy(Prec p, const Launch &L, VecBlock r, VecBlock pv, SolverState *st, int gate);
+// multi-shift: r += beta_low ttt; rsq; convergence test (ks_multicg_offset.cpp:504-520)
+void ms_residual(Prec p, const Launch &L, VecBlock r, VecBlock ttt, SolverState *st,
+                 double *partials, int gate);
+// multi-shift: update_pm / update_dest for all active shifts in one pass
+void ms_update(Prec p, const Launch &L, Prec xprec, VecBlock *x, VecBlock *pv, VecBlock r,
+               int n, SolverState *st, int gate);
+
+// elementwise helpers
+void vec_copy(Prec dst_p, VecBlock dst, Prec src_p, VecBlock src, const Launch &L);
+void vec_zero(Prec p, VecBlock v, const Launch &L);
+// y += x  (x in xp, y in yp; used for reliable updates x_fp64 += x_sloppy)
+void vec_add(Prec yp, VecBlock y, Prec xp, VecBlock x, const Launch &L);
+// r = b + (ttt - m4 x) with ttt = D D x: true residual; |r|^2 -> *out (device)
+void cg_true_residual(Prec p, const Launch &L, VecBlock ttt, VecBlock x, VecBlock b, VecBlock r,
+                      SolverState *st, double *partials, double *out);
+// |v|^2 -> *out (device)
+void norm2_dev(Prec p, const Launch &L, VecBlock v, SolverState *st, double *partials, double *out);
+
+// Mixed-precision CG inner-loop kernels (sloppy precision p, FP64 reductions)
+// state: rsq (sloppy), pkp, a, b as for CG; reliable-update trigger in host
+void mx_update(Prec p, const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlock ttt,
+               SolverState *st, double *partials, int gate, double delta2);
+
+// layout remap (remap.cu) -------------------------------------------------------
+// raw MILC block (6 reals/site, AoS) <-> device block
+void vec_from_raw(Prec p, VecBlock dst, const void *raw_dev, bool raw_double, const Launch &L);
+void vec_to_raw(Prec p, void *raw_dev, bool raw_double, VecBlock src, const Launch &L);
+// raw MILC link field (72 reals/site over all V sites) -> slot `slot` (0..3) of both blocks
+void links_from_raw(Prec p, LinkSet &ls, const void *raw_dev, bool raw_double, int slot,
+                    const Launch &L);
+// slot -> raw (forward slots only are extracted by the API)
+void links_to_raw(Prec p, void *raw_dev, bool raw_double, const LinkSet &ls, int slot,
+                  const Launch &L);
+// convert a link set between precisions (FP64 -> FP32 / half)
+void links_convert(Prec dst_p, LinkSet &dst, Prec src_p, const LinkSet &src, const Launch &L);
+// fills ls_half.link_max[] from the ranges of `src` (fat and Naik slots)
+void links_absmax(Prec p, const LinkSet &src, LinkSet &ls_half, const Launch &L, double *scratch);
+
+}  // namespace qb

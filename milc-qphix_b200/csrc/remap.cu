@@ -1,0 +1,251 @@
+// Layout remap between MILC's raw arrays and the device field layouts (K6),
+// and precision conversion of link sets.
+//
+// Reference: QPHIX_F3_create_V_from_raw / extract_V_to_raw
+// (qphix_f3.cpp:63-159, 474-543) and asqtad_create_L_from_raw /
+// extract_L_to_raw (qphix_f3.cpp:954-1070, 1086-1192).  The raw order inside
+// a parity block is the device block order, so the remap is a pure
+// transpose (AoS reals -> component-major complex) plus the split of the
+// 4 link families into the 16-matrix block of each output parity.
+#include <cstring>
+
+#include "device_common.cuh"
+
+namespace qb {
+
+template <typename S, typename RAW>
+__global__ void k_vec_from_raw(VecView<S> d, const RAW *raw)
+{
+    using A = typename Acc<S>::type;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= d.vh) return;
+    A v[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) v[i] = (A)raw[6 * (size_t)j + i];
+    d.store(j, v);
+}
+
+template <typename S, typename RAW>
+__global__ void k_vec_to_raw(RAW *raw, VecView<S> s)
+{
+    using A = typename Acc<S>::type;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= s.vh) return;
+    A v[6];
+    s.load(j, v);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) raw[6 * (size_t)j + i] = (RAW)v[i];
+}
+
+template <typename S, typename RAW>
+static void vfr(const Launch &L, VecBlock d, const void *raw)
+{
+    k_vec_from_raw<S, RAW><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(view<S>(d, L.g->vh),
+                                                                        static_cast<const RAW *>(raw));
+}
+
+template <typename S, typename RAW>
+static void vtr(const Launch &L, void *raw, VecBlock s)
+{
+    k_vec_to_raw<S, RAW><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(static_cast<RAW *>(raw),
+                                                                      view<S>(s, L.g->vh));
+}
+
+void vec_from_raw(Prec p, VecBlock dst, const void *raw_dev, bool raw_double, const Launch &L)
+{
+    if (raw_double) {
+        switch (p) {
+        case Prec::Double: vfr<double, double>(L, dst, raw_dev); break;
+        case Prec::Single: vfr<float, double>(L, dst, raw_dev); break;
+        case Prec::Half: vfr<__half, double>(L, dst, raw_dev); break;
+        }
+    } else {
+        switch (p) {
+        case Prec::Double: vfr<double, float>(L, dst, raw_dev); break;
+        case Prec::Single: vfr<float, float>(L, dst, raw_dev); break;
+        case Prec::Half: vfr<__half, float>(L, dst, raw_dev); break;
+        }
+    }
+}
+
+void vec_to_raw(Prec p, void *raw_dev, bool raw_double, VecBlock src, const Launch &L)
+{
+    if (raw_double) {
+        switch (p) {
+        case Prec::Double: vtr<double, double>(L, raw_dev, src); break;
+        case Prec::Single: vtr<float, double>(L, raw_dev, src); break;
+        case Prec::Half: vtr<__half, double>(L, raw_dev, src); break;
+        }
+    } else {
+        switch (p) {
+        case Prec::Double: vtr<double, float>(L, raw_dev, src); break;
+        case Prec::Single: vtr<float, float>(L, raw_dev, src); break;
+        case Prec::Half: vtr<__half, float>(L, raw_dev, src); break;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ links --
+// one thread per (raw site, dir, complex element); raw reads are coalesced
+template <typename D, typename RAW>
+__global__ void k_links_from_raw(D *blk0, D *blk1, const RAW *raw, int slot, int vh)
+{
+    const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t total = (size_t)2 * vh * 36;
+    if (idx >= total) return;
+    const int e = idx % 9;
+    const int dir = (idx / 9) % 4;
+    const size_t s = idx / 36;
+    const int cb = s >= (size_t)vh;
+    const int j = (int)(s - (size_t)cb * vh);
+    const int mat = 4 * slot + dir;
+    D *blk = cb ? blk1 : blk0;
+    D z;
+    z.x = raw[2 * idx];
+    z.y = raw[2 * idx + 1];
+    blk[((size_t)mat * 9 + e) * vh + j] = z;
+}
+
+template <typename S, typename RAW>
+__global__ void k_links_to_raw(RAW *raw, const S *blk0, const S *blk1, int slot, int vh)
+{
+    const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t total = (size_t)2 * vh * 36;
+    if (idx >= total) return;
+    const int e = idx % 9;
+    const int dir = (idx / 9) % 4;
+    const size_t s = idx / 36;
+    const int cb = s >= (size_t)vh;
+    const int j = (int)(s - (size_t)cb * vh);
+    const int mat = 4 * slot + dir;
+    const S *blk = cb ? blk1 : blk0;
+    const S z = blk[((size_t)mat * 9 + e) * vh + j];
+    raw[2 * idx] = (RAW)z.x;
+    raw[2 * idx + 1] = (RAW)z.y;
+}
+
+static int grid_links(int vh) { return (int)(((size_t)2 * vh * 36 + kBlock - 1) / kBlock); }
+
+void links_from_raw(Prec p, LinkSet &ls, const void *raw_dev, bool raw_double, int slot, const Launch &L)
+{
+    const int vh = L.g->vh;
+    const int grid = grid_links(vh);
+    if (p == Prec::Double) {
+        if (raw_double)
+            k_links_from_raw<double2, double><<<grid, kBlock, 0, L.stream>>>(
+                (double2 *)ls.blk[0], (double2 *)ls.blk[1], (const double *)raw_dev, slot, vh);
+        else
+            k_links_from_raw<double2, float><<<grid, kBlock, 0, L.stream>>>(
+                (double2 *)ls.blk[0], (double2 *)ls.blk[1], (const float *)raw_dev, slot, vh);
+    } else if (p == Prec::Single) {
+        if (raw_double)
+            k_links_from_raw<float2, double><<<grid, kBlock, 0, L.stream>>>(
+                (float2 *)ls.blk[0], (float2 *)ls.blk[1], (const double *)raw_dev, slot, vh);
+        else
+            k_links_from_raw<float2, float><<<grid, kBlock, 0, L.stream>>>(
+                (float2 *)ls.blk[0], (float2 *)ls.blk[1], (const float *)raw_dev, slot, vh);
+    }
+}
+
+void links_to_raw(Prec p, void *raw_dev, bool raw_double, const LinkSet &ls, int slot, const Launch &L)
+{
+    const int vh = L.g->vh;
+    const int grid = grid_links(vh);
+    if (p == Prec::Double) {
+        if (raw_double)
+            k_links_to_raw<double2, double><<<grid, kBlock, 0, L.stream>>>(
+                (double *)raw_dev, (const double2 *)ls.blk[0], (const double2 *)ls.blk[1], slot, vh);
+        else
+            k_links_to_raw<double2, float><<<grid, kBlock, 0, L.stream>>>(
+                (float *)raw_dev, (const double2 *)ls.blk[0], (const double2 *)ls.blk[1], slot, vh);
+    } else if (p == Prec::Single) {
+        if (raw_double)
+            k_links_to_raw<float2, double><<<grid, kBlock, 0, L.stream>>>(
+                (double *)raw_dev, (const float2 *)ls.blk[0], (const float2 *)ls.blk[1], slot, vh);
+        else
+            k_links_to_raw<float2, float><<<grid, kBlock, 0, L.stream>>>(
+                (float *)raw_dev, (const float2 *)ls.blk[0], (const float2 *)ls.blk[1], slot, vh);
+    }
+}
+
+// max |component| over one family (fat: mats 0-7, Naik: mats 8-15) of both
+// parity blocks, for the 16-bit fixed-point ranges
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+k_absmax(const S *b0, const S *b1, size_t off, size_t n, unsigned int *out)
+{
+    float m = 0.f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const S a = b0[off + i], c = b1[off + i];
+        m = fmaxf(m, fmaxf(fmaxf(fabsf((float)a.x), fabsf((float)a.y)), fmaxf(fabsf((float)c.x), fabsf((float)c.y))));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));  // m >= 0: uint order = float order
+}
+
+void links_absmax(Prec p, const LinkSet &src, LinkSet &dst, const Launch &L, double *scratch)
+{
+    unsigned int *d = reinterpret_cast<unsigned int *>(scratch);
+    cudaMemsetAsync(d, 0, 2 * sizeof(unsigned int), L.stream);
+    const size_t n = (size_t)8 * 9 * L.g->vh;
+    const int grid = 148 * 8;
+    for (int f = 0; f < 2; ++f) {
+        if (p == Prec::Double)
+            k_absmax<double2><<<grid, kBlock, 0, L.stream>>>((const double2 *)src.blk[0], (const double2 *)src.blk[1], f * n, n, d + f);
+        else
+            k_absmax<float2><<<grid, kBlock, 0, L.stream>>>((const float2 *)src.blk[0], (const float2 *)src.blk[1], f * n, n, d + f);
+    }
+    unsigned int h[2] = {0, 0};
+    cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, L.stream);
+    cudaStreamSynchronize(L.stream);
+    for (int f = 0; f < 2; ++f) {
+        float v;
+        memcpy(&v, &h[f], sizeof(v));
+        dst.link_max[f] = v;
+    }
+}
+
+template <typename D, typename S>
+__global__ void k_links_convert(D *d, const S *s, size_t n, float inv_scale)
+{
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const S z = s[i];
+    if constexpr (std::is_same<D, short2>::value) {
+        short2 q;
+        q.x = (short)__float2int_rn((float)z.x * inv_scale);
+        q.y = (short)__float2int_rn((float)z.y * inv_scale);
+        d[i] = q;
+    } else {
+        D q;
+        q.x = z.x;
+        q.y = z.y;
+        d[i] = q;
+    }
+}
+
+void links_convert(Prec dst_p, LinkSet &dst, Prec src_p, const LinkSet &src, const Launch &L)
+{
+    const size_t n = (size_t)kMats * 9 * L.g->vh;
+    const int grid = (int)((n + kBlock - 1) / kBlock);
+    const size_t nh = n / 2;  // one family (8 matrices)
+    for (int cb = 0; cb < 2; ++cb) {
+        if (dst_p == Prec::Single && src_p == Prec::Double)
+            k_links_convert<float2, double2><<<grid, kBlock, 0, L.stream>>>((float2 *)dst.blk[cb], (const double2 *)src.blk[cb], n, 0.f);
+        else if (dst_p == Prec::Double && src_p == Prec::Single)
+            k_links_convert<double2, float2><<<grid, kBlock, 0, L.stream>>>((double2 *)dst.blk[cb], (const float2 *)src.blk[cb], n, 0.f);
+        else if (dst_p == Prec::Half) {
+            const int gh = (int)((nh + kBlock - 1) / kBlock);
+            for (int f = 0; f < 2; ++f) {
+                const float inv = dst.link_max[f] > 0 ? 32767.0f / dst.link_max[f] : 0.f;
+                short2 *d = (short2 *)dst.blk[cb] + f * nh;
+                if (src_p == Prec::Double)
+                    k_links_convert<short2, double2><<<gh, kBlock, 0, L.stream>>>(d, (const double2 *)src.blk[cb] + f * nh, nh, inv);
+                else
+                    k_links_convert<short2, float2><<<gh, kBlock, 0, L.stream>>>(d, (const float2 *)src.blk[cb] + f * nh, nh, inv);
+            }
+        }
+    }
+}
+
+}  // namespace qb

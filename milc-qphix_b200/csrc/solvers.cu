@@ -1,0 +1,671 @@
+// Solver drivers: CG and multi-shift CG with the reference's control flow,
+// and their mixed-precision counterparts.
+//
+// The iteration bodies run as device kernels with every scalar (rsq, pkp,
+// a, b, the shift recurrences) kept in a device-resident SolverState; the
+// host enqueues chunks of iterations and reads the state once per chunk.
+// Each kernel of iteration k of a chunk returns immediately when an earlier
+// iteration of the chunk already met the stop condition (k > stop_at), so a
+// chunk that overshoots costs a few empty launches, never extra arithmetic,
+// and the sequence of arithmetic is exactly the reference's.
+#include <cmath>
+
+#include "context.h"
+#include "device_common.cuh"
+
+namespace qb {
+
+namespace {
+
+struct Ws {
+    std::vector<VecBlock> v;
+    std::vector<Prec> p;
+    VecBlock get(Prec prec)
+    {
+        v.push_back(alloc_vec(prec));
+        p.push_back(prec);
+        return v.back();
+    }
+    ~Ws()
+    {
+        for (auto &b : v) free_vec(b);
+    }
+};
+
+inline double round_prec(double v, bool single) { return single ? (double)(float)v : v; }
+
+// |v|^2 with a wait
+double norm2_sync(Prec p, VecBlock v)
+{
+    Context &c = ctx();
+    const Launch L = c.launch();
+    norm2_dev(p, L, v, c.d_state, c.d_partials, c.d_scalars);
+    QB_CUDA(cudaMemcpyAsync(c.h_scalars, c.d_scalars, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    QB_CUDA(cudaStreamSynchronize(c.stream));
+    return c.h_scalars[0];
+}
+
+// event-timed launch bracket (kernel timing mode)
+struct TimedLaunches {
+    struct Mark { int kind; int gate; cudaEvent_t a, b; };
+    std::vector<Mark> marks;
+    bool on;
+    explicit TimedLaunches(bool enabled) : on(enabled) { ctx().ktimer.reset(); }
+    template <typename F> void run(int kind, int gate, F f)
+    {
+        if (!on) { f(); return; }
+        Context &c = ctx();
+        cudaEvent_t a = c.ktimer.next(), b = c.ktimer.next();
+        QB_CUDA(cudaEventRecord(a, c.stream));
+        f();
+        QB_CUDA(cudaEventRecord(b, c.stream));
+        marks.push_back({kind, gate, a, b});
+    }
+    // credit launches whose gate did work (gate <= stop_at); call after a sync
+    void collect(int stop_at)
+    {
+        if (!on) return;
+        Context &c = ctx();
+        for (auto &m : marks) {
+            if (m.gate >= 0 && m.gate > stop_at) continue;
+            float ms = 0;
+            QB_CUDA(cudaEventElapsedTime(&ms, m.a, m.b));
+            if (m.kind == 0) { c.stats.dslash_launches++; c.stats.dslash_ms += ms; }
+            else { c.stats.mdagm_launches++; c.stats.mdagm_ms += ms; }
+        }
+        marks.clear();
+        c.ktimer.reset();
+    }
+};
+
+int next_chunk(int current, double size_prev, double size_now, int done, double target, int cap)
+{
+    Context &c = ctx();
+    int chunk = current;
+    if (target > 0 && size_now > 0 && size_prev > size_now && done > 0) {
+        const double rate = std::log(size_prev / size_now) / done;
+        const double left = std::log(size_now / target) / rate;
+        chunk = (int)std::ceil(left) + 1;
+    } else {
+        chunk = current * 2;
+    }
+    if (chunk < 2) chunk = 2;
+    if (chunk > c.max_chunk) chunk = c.max_chunk;
+    if (cap > 0 && chunk > cap) chunk = cap;
+    return chunk;
+}
+
+}  // namespace
+
+// ===========================================================================
+// CG, reference control flow: QPHIX_fptype_asqtad_invert,
+// ks_d_congrad_fn.cpp:221-619, statement for statement; only the loops over
+// sites moved into kernels.
+// ===========================================================================
+int cg_reference(Prec P, const LinkSet &ls, SolveArgs &A)
+{
+    Context &c = ctx();
+    const Launch L = c.launch();
+    SolverState &S = *c.h_state;
+    const bool single = (P == Prec::Single);
+    auto R = [&](double v) { return round_prec(v, single); };
+    QPHIX_info_t *info = A.info;
+    QPHIX_invert_arg_t *inv = A.inv;
+    QPHIX_resid_arg_t *res = A.res;
+
+    VecBlock t_src, t_dest;
+    if (inv->parity != QPHIX_ODD) { t_src = A.in[0]; t_dest = A.out[0]; }
+    else { t_src = A.in[1]; t_dest = A.out[1]; }
+
+    const int niter = inv->max;
+    const int max_restarts = inv->nrestart;
+    const double rsqmin = R(res->resid);
+    const double relrsqmin = R(res->relresid);
+    const int max_cg = max_restarts * niter;
+    const double msq_x4 = R(4.0 * A.mass * A.mass);
+    int parity = inv->parity & 1;
+    int otherparity = 1 - parity;
+    int parity0 = inv->parity;
+    const double V = 2.0 * c.g.vh;
+    const bool relres = relrsqmin > 0;
+    if (niter <= 0) throw Error("invert: inv_arg->max must be positive");
+
+    Ws ws;
+    VecBlock ttt = ws.get(P), tmp = ws.get(P), cg_p = ws.get(P), resid = ws.get(P);
+    info->final_sec = wall_seconds();
+    info->final_flop = 0.;
+    TimedLaunches tl(c.kernel_timing);
+
+    auto conv = [&](double r1, double r2) {
+        return (rsqmin <= 0 || rsqmin > r1) && (relrsqmin <= 0 || relrsqmin > r2);
+    };
+
+    int total_iters = 0, iteration = 0, nrestart = 0;
+    double rsq = 0, relrsq = 0, source_norm = 0;
+    bool finished = false;
+    while (!finished) {
+        // start: (:309-350)
+        source_norm = norm2_sync(P, t_src);
+        nrestart = 0;
+        total_iters += iteration;
+        iteration = 0;
+        res->size_r = 0;
+        res->size_relr = 0;
+        if (source_norm == 0.0) {
+            vec_zero(P, t_dest, L);
+            QB_CUDA(cudaStreamSynchronize(c.stream));
+            info->final_sec = wall_seconds() - info->final_sec;
+            res->final_rel = 0;
+            res->final_rsq = 0;
+            res->final_iter = total_iters;
+            res->final_restart = nrestart;
+            c.stats.iterations = total_iters;
+            return iteration;
+        }
+        bool switch_parity = false;
+        for (;;) {
+            if ((iteration % niter == 0) || conv(res->size_r, res->size_relr)) {
+                // (re)initialisation with the true residual (:365-448)
+                S.msq_x4 = msq_x4;
+                S.counter = S.counter2 = 0;
+                upload_state();
+                tl.run(0, -1, [&] { dslash(P, L, tmp, t_dest, ls, otherparity); });
+                tl.run(0, -1, [&] { dslash(P, L, ttt, tmp, ls, parity); });
+                cg_restart_residual(P, L, ttt, t_dest, t_src, resid, cg_p, c.d_state, c.d_partials, relres);
+                download_state();
+                tl.collect(INT_MAX);
+                rsq = S.rsq;
+                if (relres) relrsq = R(std::sqrt(2 * S.relrsq / V));
+                res->final_rsq = R(rsq) / source_norm;
+                res->final_rel = R(relrsq);
+                iteration++;
+                if (iteration >= max_cg || nrestart >= max_restarts ||
+                    conv(res->final_rsq, res->final_rel)) {
+                    if (parity0 == QPHIX_EVENODD) {
+                        // (:437-444): the reference's parity bookkeeping, kept as is
+                        otherparity = parity0 & 1;
+                        parity = 1 - otherparity;
+                        parity0 = QPHIX_EVEN;
+                        t_src = A.in[1];
+                        t_dest = A.out[1];
+                        switch_parity = true;
+                    }
+                    break;
+                }
+                if (iteration != 0) nrestart++;
+            }
+            // iterations on the device (:450-576)
+            S.rsq = rsq;
+            S.relrsq = relrsq;
+            S.source_norm = source_norm;
+            S.rsqmin = rsqmin;
+            S.relrsqmin = relrsqmin;
+            S.msq_x4 = msq_x4;
+            S.iteration = iteration;
+            S.niter = niter;
+            S.stop_at = INT_MAX;
+            S.axpy_skip_at = -1;
+            S.prec_single = single;
+            S.size_r = res->size_r;
+            S.size_relr = res->size_relr;
+            S.counter = S.counter2 = 0;
+            upload_state();
+            int chunk = 8;
+            double size_prev = res->size_r > 0 ? res->size_r : 1.0;
+            for (;;) {
+                const int cap = niter - (S.iteration % niter);
+                for (int k = 0; k < chunk; ++k) {
+                    tl.run(0, k, [&] { dslash_gated(P, L, tmp, cg_p, ls, otherparity, c.d_state, k); });
+                    tl.run(1, k, [&] {
+                        dslash_mdagm_dot(P, L, ttt, tmp, ls, cg_p, -msq_x4, parity, c.d_state, c.d_partials, k, 0);
+                    });
+                    cg_update(P, L, t_dest, cg_p, resid, ttt, c.d_state, c.d_partials, k, relres);
+                    cg_axpy(P, L, resid, cg_p, c.d_state, k);
+                }
+                const int it0 = S.iteration;
+                QB_CUDA(cudaGetLastError());
+                download_state();
+                tl.collect(S.stop_at);
+                if (S.stop_at != INT_MAX) break;
+                if (S.iteration == it0) throw Error("invert: device iterations made no progress");
+                chunk = next_chunk(chunk, size_prev, S.size_r, S.iteration - it0, rsqmin, cap);
+                size_prev = S.size_r;
+            }
+            iteration = S.iteration;
+            rsq = S.rsq;
+            relrsq = S.relrsq;
+            res->size_r = S.size_r;
+            res->size_relr = S.size_relr;
+            res->final_rsq = res->size_r;
+        }
+        if (!switch_parity) finished = true;
+    }
+    info->final_sec = wall_seconds() - info->final_sec;
+    total_iters += iteration;
+    res->final_iter = total_iters;
+    res->final_restart = nrestart;
+    info->final_flop = 1187. * total_iters * V;
+    info->status = QPHIX_SUCCESS;
+    c.stats.iterations = total_iters;
+    c.stats.true_rsq = res->final_rsq;
+    return iteration;
+}
+
+// ===========================================================================
+// Mixed precision CG: FP64 solution and true residual, sloppy inner CG in
+// precision ps with reliable updates (the true residual is recomputed in
+// FP64 whenever the sloppy residual has dropped by `reliable_delta`).
+// Converges on the FP64 true residual |b - M x|^2 / |b|^2 < tol.
+// ===========================================================================
+namespace {
+
+struct MixedResult {
+    double true_rsq_rel = 0;
+    int iterations = 0;
+    int reliable_updates = 0;
+};
+
+MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, VecBlock x, VecBlock b,
+                       int parity, double mass, double tol, int max_cg, TimedLaunches &tl)
+{
+    Context &c = ctx();
+    const Launch L = c.launch();
+    SolverState &S = *c.h_state;
+    const int other = 1 - parity;
+    const double m4 = 4.0 * mass * mass;
+    const double delta2 = c.reliable_delta * c.reliable_delta;
+    MixedResult out;
+
+    const double bnorm = norm2_sync(Prec::Double, b);
+    if (bnorm == 0.0) {
+        vec_zero(Prec::Double, x, L);
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+        return out;
+    }
+    Ws ws;
+    VecBlock tmp64 = ws.get(Prec::Double), ttt64 = ws.get(Prec::Double), r64 = ws.get(Prec::Double);
+    VecBlock xs = ws.get(ps), rs = ws.get(ps), pv = ws.get(ps), tmps = ws.get(ps), ttts = ws.get(ps);
+
+    auto true_residual = [&]() {
+        S.msq_x4 = m4;
+        S.counter = S.counter2 = 0;
+        upload_state();
+        dslash(Prec::Double, L, tmp64, x, ls64, other);
+        dslash(Prec::Double, L, ttt64, tmp64, ls64, parity);
+        cg_true_residual(Prec::Double, L, ttt64, x, b, r64, c.d_state, c.d_partials, c.d_scalars);
+        QB_CUDA(cudaMemcpyAsync(c.h_scalars, c.d_scalars, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+        return c.h_scalars[0];
+    };
+
+    double rsq = true_residual();
+    out.true_rsq_rel = rsq / bnorm;
+    if (out.true_rsq_rel < tol) return out;
+
+    vec_copy(ps, rs, Prec::Double, r64, L);
+    vec_copy(ps, pv, ps, rs, L);
+    vec_zero(ps, xs, L);
+    S.rsq = rsq;
+    S.rsq_ru = rsq;
+    S.rsqstop = tol * bnorm;
+    S.msq_x4 = m4;
+    S.iteration = 0;
+    S.max_cg = max_cg;
+    S.stop_at = INT_MAX;
+    S.axpy_skip_at = -1;
+    S.prec_single = 0;
+    S.counter = S.counter2 = 0;
+    upload_state();
+    int chunk = 8;
+    for (;;) {
+        double size_prev = S.rsq;
+        for (;;) {
+            for (int k = 0; k < chunk; ++k) {
+                tl.run(0, k, [&] { dslash_gated(ps, L, tmps, pv, lss, other, c.d_state, k); });
+                tl.run(1, k, [&] {
+                    dslash_mdagm_dot(ps, L, ttts, tmps, lss, pv, -m4, parity, c.d_state, c.d_partials, k, 0);
+                });
+                mx_update(ps, L, xs, pv, rs, ttts, c.d_state, c.d_partials, k, delta2);
+                cg_axpy(ps, L, rs, pv, c.d_state, k);
+            }
+            const int it0 = S.iteration;
+            QB_CUDA(cudaGetLastError());
+            download_state();
+            tl.collect(S.stop_at);
+            if (S.stop_at != INT_MAX) break;
+            if (S.iteration == it0) throw Error("invert: device iterations made no progress");
+            const double target = std::max(S.rsqstop, delta2 * S.rsq_ru);
+            chunk = next_chunk(chunk, size_prev, S.rsq, S.iteration - it0, target, 0);
+            size_prev = S.rsq;
+        }
+        out.iterations = S.iteration;
+        const double oldrsq = S.oldrsq;
+        // reliable update: x += x_s, r = b - M x in FP64
+        vec_add(Prec::Double, x, ps, xs, L);
+        vec_zero(ps, xs, L);
+        rsq = true_residual();
+        out.reliable_updates++;
+        out.true_rsq_rel = rsq / bnorm;
+        if (out.true_rsq_rel < tol || S.iteration >= max_cg || !std::isfinite(rsq)) break;
+        vec_copy(ps, rs, Prec::Double, r64, L);
+        S.b = rsq / oldrsq;
+        S.rsq = rsq;
+        S.rsq_ru = rsq;
+        S.stop_at = INT_MAX;
+        S.axpy_skip_at = -1;
+        S.counter = S.counter2 = 0;
+        upload_state();
+        cg_axpy(ps, L, rs, pv, c.d_state, -1);  // p = r + beta p with the true residual
+    }
+    return out;
+}
+
+}  // namespace
+
+int cg_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, SolveArgs &A)
+{
+    Context &c = ctx();
+    QPHIX_info_t *info = A.info;
+    QPHIX_invert_arg_t *inv = A.inv;
+    QPHIX_resid_arg_t *res = A.res;
+    info->final_sec = wall_seconds();
+    TimedLaunches tl(c.kernel_timing);
+    const int max_cg = inv->max * inv->nrestart;
+    const double tol = res->resid;
+    int parity = inv->parity & 1;
+    int parity0 = inv->parity;
+    VecBlock b = (inv->parity != QPHIX_ODD) ? A.in[0] : A.in[1];
+    VecBlock x = (inv->parity != QPHIX_ODD) ? A.out[0] : A.out[1];
+    int total = 0, last = 0, rus = 0;
+    double worst = 0;
+    for (;;) {
+        MixedResult m = mixed_pass(ps, ls64, lss, x, b, parity, A.mass, tol, max_cg, tl);
+        total += m.iterations;
+        last = m.iterations;
+        rus += m.reliable_updates;
+        worst = std::max(worst, m.true_rsq_rel);
+        res->final_rsq = m.true_rsq_rel;
+        res->size_r = m.true_rsq_rel;
+        if (parity0 == QPHIX_EVENODD) {
+            // same parity sequence as the reference solver (ks_d_congrad_fn.cpp:437-444)
+            parity = 0;
+            parity0 = QPHIX_EVEN;
+            b = A.in[1];
+            x = A.out[1];
+            continue;
+        }
+        break;
+    }
+    res->final_rel = 0;
+    res->size_relr = 0;
+    res->final_iter = total;
+    res->final_restart = rus;
+    info->final_sec = wall_seconds() - info->final_sec;
+    info->final_flop = 1187. * total * 2.0 * c.g.vh;
+    info->status = QPHIX_SUCCESS;
+    c.stats.iterations = total;
+    c.stats.reliable_updates = rus;
+    c.stats.true_rsq = worst;
+    return last;
+}
+
+// ===========================================================================
+// Multi-shift CG, reference control flow: QPHIX_fptype_asqtad_invert_multi,
+// ks_multicg_offset.cpp:205-689.
+// ===========================================================================
+namespace {
+
+struct MsPass {
+    int iteration = 0;
+    bool converged = false;
+    double rsq = 0, source_norm = 0;
+};
+
+// one parity pass of the multi-shift recurrence; x[] in precision xp, the
+// Krylov vectors in precision p
+MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<VecBlock> &x,
+               std::vector<VecBlock> &pm, VecBlock ttt, VecBlock tmp, VecBlock resid, VecBlock *d_x,
+               VecBlock *d_p, int parity, const std::vector<double> &shifts, int j_low,
+               double offset_low, double rsqmin, int max_cg, bool single, TimedLaunches &tl)
+{
+    Context &c = ctx();
+    const Launch L = c.launch();
+    SolverState &S = *c.h_state;
+    const int n = (int)x.size();
+    const int other = 1 - parity;
+    MsPass out;
+    out.source_norm = norm2_sync(p, src);
+    for (int j = 0; j < n; ++j) vec_zero(xp, x[j], L);
+    for (int j = 0; j < n; ++j) vec_copy(p, pm[j], p, src, L);
+    vec_copy(p, resid, p, src, L);
+    out.rsq = out.source_norm;
+    if (out.source_norm == 0.) {
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+        return out;
+    }
+    S.rsqstop = rsqmin * out.source_norm;
+    for (int j = 0; j < n; ++j) {
+        S.shifts[j] = shifts[j];
+        S.zeta_im1[j] = S.zeta_i[j] = 1.0;
+        S.beta_im1[j] = -1.0;
+        S.alpha[j] = 0.0;
+    }
+    S.num_now = n;
+    S.n_shifts = n;
+    S.j_low = j_low;
+    S.rsq = out.rsq;
+    S.iteration = 0;
+    S.max_cg = max_cg;
+    S.first_iter = 1;
+    S.converged = 0;
+    S.stop_at = INT_MAX;
+    S.prec_single = single;
+    S.counter = S.counter2 = 0;
+    upload_state();
+    const double m4 = round_prec(-1.0 * offset_low, single);
+    int chunk = 8;
+    double size_prev = out.rsq;
+    for (;;) {
+        for (int k = 0; k < chunk; ++k) {
+            tl.run(0, k, [&] { dslash_gated(p, L, tmp, pm[j_low], ls, other, c.d_state, k); });
+            tl.run(1, k, [&] {
+                dslash_mdagm_dot(p, L, ttt, tmp, ls, pm[j_low], m4, parity, c.d_state, c.d_partials, k, 1);
+            });
+            ms_residual(p, L, resid, ttt, c.d_state, c.d_partials, k);
+            ms_update(p, L, xp, d_x, d_p, resid, n, c.d_state, k);
+        }
+        const int it0 = S.iteration;
+        QB_CUDA(cudaGetLastError());
+        download_state();
+        tl.collect(S.stop_at);
+        if (S.stop_at != INT_MAX) break;
+        if (S.iteration == it0) throw Error("invert_multi: device iterations made no progress");
+        chunk = next_chunk(chunk, size_prev, S.rsq, S.iteration - it0, S.rsqstop, max_cg - S.iteration);
+        size_prev = S.rsq;
+    }
+    out.iteration = S.iteration;
+    out.converged = S.converged != 0;
+    out.rsq = S.rsq;
+    return out;
+}
+
+void upload_blocks(VecBlock *d, const std::vector<VecBlock> &h)
+{
+    Context &c = ctx();
+    QB_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(VecBlock) * h.size(), cudaMemcpyHostToDevice, c.stream));
+    QB_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+}  // namespace
+
+int multishift_reference(Prec P, const LinkSet &ls, MultiArgs &A)
+{
+    Context &c = ctx();
+    const int n = A.n;
+    if (n <= 0) return 0;  // (:218-225)
+    if (n > kMaxShifts) throw Error("invert_multi: more offsets than MAXNDMASS (150)");
+    const bool single = (P == Prec::Single);
+    auto R = [&](double v) { return round_prec(v, single); };
+    QPHIX_info_t *info = A.info;
+    QPHIX_invert_arg_t *inv = A.inv;
+    int parity0 = inv->parity;
+    VecBlock t_src = (parity0 != QPHIX_ODD) ? A.in[0] : A.in[1];
+    std::vector<VecBlock> t_dest = (parity0 != QPHIX_ODD) ? A.out[0] : A.out[1];
+    const int niter = inv->max;
+    const int max_restarts = inv->nrestart;
+    const double rsqmin = R(A.res[0]->resid);
+    const int max_cg = max_restarts * niter;
+    int parity = parity0 & 1;
+    const double V = 2.0 * c.g.vh;
+
+    Ws ws;
+    VecBlock ttt = ws.get(P), tmp = ws.get(P), resid = ws.get(P);
+    std::vector<VecBlock> pm(n);
+    for (int j = 0; j < n; ++j) pm[j] = ws.get(P);
+    std::vector<double> shifts(n);
+    double offset_low = 1.0e+20;
+    int j_low = -1;
+    for (int j = 0; j < n; ++j) {  // (:332-342)
+        shifts[j] = R(R(A.mass[j] * A.mass[j]) * 4.0);
+        if (shifts[j] < offset_low) { offset_low = shifts[j]; j_low = j; }
+    }
+    for (int j = 0; j < n; ++j)
+        if (j != j_low) shifts[j] = R(shifts[j] - shifts[j_low]);
+    for (int j = 0; j < n; ++j) c.h_state->finished[j] = 0;
+
+    VecBlock *d_x = static_cast<VecBlock *>(dev_alloc(sizeof(VecBlock) * n));
+    VecBlock *d_p = static_cast<VecBlock *>(dev_alloc(sizeof(VecBlock) * n));
+    upload_blocks(d_p, pm);
+    TimedLaunches tl(c.kernel_timing);
+    info->final_sec = wall_seconds();
+    info->final_flop = 0.;
+    int total_iters = 0, iteration = 0;
+    const int nrestart = 0;
+    for (;;) {
+        upload_blocks(d_x, t_dest);
+        MsPass r = ms_pass(P, P, ls, t_src, t_dest, pm, ttt, tmp, resid, d_x, d_p, parity, shifts, j_low,
+                           offset_low, rsqmin, max_cg, single, tl);
+        iteration = r.iteration;
+        total_iters += r.iteration;
+        if (r.source_norm == 0.) {  // (:377-419)
+            for (int j = 0; j < n; ++j) {
+                A.res[j]->final_rsq = 0.;
+                A.res[j]->size_r = 0.;
+                A.res[j]->size_relr = 0.;
+                A.res[j]->final_iter = iteration;
+                A.res[j]->final_restart = nrestart;
+            }
+            break;
+        }
+        for (int j = 0; j < n; ++j) {  // (:544-550, 626-632)
+            A.res[j]->final_rsq = R(r.rsq) / r.source_norm;
+            A.res[j]->size_r = A.res[j]->final_rsq;
+            A.res[j]->size_relr = A.res[j]->final_rel;
+            A.res[j]->final_iter = iteration;
+            A.res[j]->final_restart = nrestart;
+        }
+        if (parity0 == QPHIX_EVENODD) {  // (:534-543, 644-653)
+            const int otherparity = parity0 & 1;
+            parity = 1 - otherparity;
+            parity0 = QPHIX_EVEN;
+            t_src = A.in[1];
+            t_dest = A.out[1];
+            continue;
+        }
+        break;
+    }
+    dev_free(d_x);
+    dev_free(d_p);
+    info->final_sec = wall_seconds() - info->final_sec;
+    info->final_flop = (1205. + 15. * n) * total_iters * V;
+    info->status = QPHIX_SUCCESS;
+    c.stats.iterations = total_iters;
+    c.stats.true_rsq = A.res[0]->final_rsq;
+    return iteration;
+}
+
+// ===========================================================================
+// Mixed-precision multi-shift: the shifted recurrence runs in the sloppy
+// precision with FP64 solution accumulation until the base residual reaches
+// the sloppy floor, then every shift is refined by mixed-precision CG
+// started from its multi-shift solution, to its own tolerance on the FP64
+// true residual.
+// ===========================================================================
+int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, MultiArgs &A)
+{
+    Context &c = ctx();
+    const int n = A.n;
+    if (n <= 0) return 0;
+    if (n > kMaxShifts) throw Error("invert_multi: more offsets than MAXNDMASS (150)");
+    QPHIX_info_t *info = A.info;
+    QPHIX_invert_arg_t *inv = A.inv;
+    int parity0 = inv->parity;
+    VecBlock src = (parity0 != QPHIX_ODD) ? A.in[0] : A.in[1];
+    std::vector<VecBlock> x = (parity0 != QPHIX_ODD) ? A.out[0] : A.out[1];
+    const int max_cg = inv->max * inv->nrestart;
+    int parity = parity0 & 1;
+    const double floor = (ps == Prec::Single) ? 1e-12 : 1e-6;
+    const double rsq_sloppy = std::max(A.res[0]->resid, floor);
+
+    Ws ws;
+    VecBlock ttt = ws.get(ps), tmp = ws.get(ps), resid = ws.get(ps), src_s = ws.get(ps);
+    std::vector<VecBlock> pm(n);
+    for (int j = 0; j < n; ++j) pm[j] = ws.get(ps);
+    std::vector<double> shifts(n);
+    double offset_low = 1.0e+20;
+    int j_low = -1;
+    for (int j = 0; j < n; ++j) {
+        shifts[j] = A.mass[j] * A.mass[j] * 4.0;
+        if (shifts[j] < offset_low) { offset_low = shifts[j]; j_low = j; }
+    }
+    for (int j = 0; j < n; ++j)
+        if (j != j_low) shifts[j] -= shifts[j_low];
+    for (int j = 0; j < n; ++j) c.h_state->finished[j] = 0;
+    VecBlock *d_x = static_cast<VecBlock *>(dev_alloc(sizeof(VecBlock) * n));
+    VecBlock *d_p = static_cast<VecBlock *>(dev_alloc(sizeof(VecBlock) * n));
+    upload_blocks(d_p, pm);
+    TimedLaunches tl(c.kernel_timing);
+    info->final_sec = wall_seconds();
+    int total = 0, last = 0, rus = 0;
+    double worst = 0;
+    for (;;) {
+        const Launch L = c.launch();
+        vec_copy(ps, src_s, Prec::Double, src, L);
+        upload_blocks(d_x, x);
+        MsPass r = ms_pass(ps, Prec::Double, lss, src_s, x, pm, ttt, tmp, resid, d_x, d_p,
+                           parity, shifts, j_low, offset_low, rsq_sloppy, max_cg, false, tl);
+        total += r.iteration;
+        last = r.iteration;
+        for (int j = 0; j < n; ++j) {
+            const double tol = A.res[j]->resid > 0 ? A.res[j]->resid : A.res[0]->resid;
+            MixedResult m = mixed_pass(ps, ls64, lss, x[j], src, parity, A.mass[j], tol, max_cg, tl);
+            total += m.iterations;
+            rus += m.reliable_updates;
+            worst = std::max(worst, m.true_rsq_rel);
+            A.res[j]->final_rsq = m.true_rsq_rel;
+            A.res[j]->size_r = m.true_rsq_rel;
+            A.res[j]->size_relr = A.res[j]->final_rel;
+            A.res[j]->final_iter = r.iteration + m.iterations;
+            A.res[j]->final_restart = m.reliable_updates;
+        }
+        if (parity0 == QPHIX_EVENODD) {
+            parity = 0;
+            parity0 = QPHIX_EVEN;
+            src = A.in[1];
+            x = A.out[1];
+            continue;
+        }
+        break;
+    }
+    dev_free(d_x);
+    dev_free(d_p);
+    info->final_sec = wall_seconds() - info->final_sec;
+    info->final_flop = (1205. + 15. * n) * total * 2.0 * c.g.vh;
+    info->status = QPHIX_SUCCESS;
+    c.stats.iterations = total;
+    c.stats.reliable_updates = rus;
+    c.stats.true_rsq = worst;
+    return last;
+}
+
+}  // namespace qb

@@ -1,0 +1,95 @@
+"""GPU: multi-shift CG through the C ABI against the oracle.
+
+Reference mode (FP64 D3 / FP32 F3): the reference's recurrence on the
+device; FP64 must give the oracle's iteration count, flop count and
+solutions to 1e-10.  Mixed mode (D3 with a 32- or 16-bit inner solve): every
+shift reaches its FP64 true-residual tolerance.
+"""
+import numpy as np
+import pytest
+
+from conftest import fields, orc, rel_err, synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _masses(m0=0.05, n=5):
+    sig = np.logspace(-3, 0, n)
+    m = np.sqrt(m0 ** 2 + sig / 4)
+    return np.concatenate([m[2:], m[:2]])  # the lightest mass is not first
+
+
+def _multi(lib, prec, links, src, masses, parity, **kw):
+    L = lib.create_L(prec, links)
+    b = lib.create_V(prec, src, parity)
+    outs = [lib.create_V(prec, np.zeros_like(src), parity) for _ in masses]
+    it, info, res = lib.invert_multi(prec, L, outs, b, masses, parity=parity, **kw)
+    assert info.status == 0, lib.last_error()
+    xs = [lib.extract_V(prec, o, parity) for o in outs]
+    for h in outs + [b]:
+        lib.destroy_V(prec, h)
+    lib.destroy_L(prec, L)
+    return it, xs, res, info
+
+
+@pytest.mark.parametrize("parity", ["even", "odd", "evenodd"])
+def test_multishift_fp64_matches_oracle(gpu, parity):
+    dims = (8, 8, 8, 8)
+    lib = gpu.use(dims)
+    lib.set_inner_precision("double")
+    links = fields(dims)
+    src = synthetic.gaussian_source(dims, seed=2002, parity="evenodd")
+    masses = _masses()
+    it, xs, res, info = _multi(lib, "D", links, src, masses, parity, max_iter=1000, nrestart=5, resid=1e-20)
+    ito, xo, reso, info_o = orc.invert_multi(dims, links, src, masses, parity, "D", 1000, 5, 1e-20)
+    assert it == ito
+    assert [r.final_iter for r in res] == [r.final_iter for r in reso]
+    assert info.final_flop == info_o.final_flop
+    for a, b in zip(xs, xo):
+        assert rel_err(a, b) < 1e-10
+
+
+def test_multishift_fp64_not_converged_path(gpu):
+    """Iteration cap reached (ks_multicg_offset.cpp:626-653)."""
+    dims = (8, 4, 4, 8)
+    lib = gpu.use(dims)
+    lib.set_inner_precision("double")
+    links = fields(dims)
+    src = synthetic.gaussian_source(dims, seed=3, parity="evenodd")
+    masses = _masses(0.01, 4)
+    it, xs, res, info = _multi(lib, "D", links, src, masses, "even", max_iter=10, nrestart=3, resid=1e-30)
+    ito, xo, reso, _ = orc.invert_multi(dims, links, src, masses, "even", "D", 10, 3, 1e-30)
+    assert it == ito == 30
+    assert abs(res[0].final_rsq - reso[0].final_rsq) <= 1e-8 * reso[0].final_rsq
+    for a, b in zip(xs, xo):
+        assert rel_err(a, b) < 1e-10
+
+
+def test_multishift_fp32_close(gpu):
+    dims = (8, 8, 8, 8)
+    lib = gpu.use(dims)
+    links = fields(dims)
+    src = synthetic.gaussian_source(dims, seed=2002, parity="evenodd")
+    masses = _masses()
+    it, xs, res, info = _multi(lib, "F", links, src, masses, "even", max_iter=1000, nrestart=5, resid=1e-12)
+    ito, xo, reso, _ = orc.invert_multi(dims, links, src, masses, "even", "F", 1000, 5, 1e-12)
+    assert abs(it - ito) <= 5
+    for a, b in zip(xs, xo):
+        assert rel_err(a, b) < 2e-5
+
+
+@pytest.mark.parametrize("inner", ["single", "half"])
+def test_multishift_mixed_every_shift_converges(gpu, inner):
+    dims = (8, 8, 8, 8)
+    lib = gpu.use(dims)
+    links = fields(dims)
+    src = synthetic.gaussian_source(dims, seed=2002, parity="evenodd")
+    masses = _masses(0.02, 6)
+    lib.set_inner_precision(inner)
+    try:
+        it, xs, res, info = _multi(lib, "D", links, src, masses, "even", max_iter=4000, nrestart=5, resid=1e-20)
+    finally:
+        lib.set_inner_precision("double")
+    for m, x, r in zip(masses, xs, res):
+        assert r.final_rsq < 1e-20
+        assert orc.true_residual(dims, links, x, src, m, "even") < 1e-20
