@@ -130,8 +130,9 @@ def max_over_ranks(pg, v):
     return float(t.item())
 
 
-def make_inputs(device):
-    links = synthetic.asqtad_links(DIMS, seed=LINK_SEED, device=device)
+def make_inputs(device=None):
+    # the eigendecompositions of the generator run on the host (torch CPU)
+    links = synthetic.asqtad_links(DIMS, seed=LINK_SEED)
     src = synthetic.gaussian_source(DIMS, seed=SRC_SEED, parity="even")
     return links, src
 
@@ -143,7 +144,7 @@ def run_gpu(args):
     import torch
 
     torch.cuda.set_device(local)
-    links, src = make_inputs(f"cuda:{local}")
+    links, src = make_inputs()
     V = int(np.prod(DIMS))
     Vh = V // 2
     lib = capi.QphixLib(LIB_PATH)

@@ -46,6 +46,7 @@ typedef struct {
   int mdagm_launches;     /* fused Dslash + M^dag M epilogue launches (timing on) */
   double mdagm_ms;        /* their summed device time */
   double true_rsq;        /* final |b - M x|^2 / |b|^2 (largest over masses) */
+  int escalated;          /* 1 if a 16-bit inner solve stalled and continued in FP32 */
 } QPHIX_B200_stats_t;
 
 QPHIX_status_t QPHIX_B200_get_last_stats(QPHIX_B200_stats_t *stats);

@@ -80,7 +80,7 @@ class Stats(C.Structure):
     _fields_ = [("solve_ms", C.c_double), ("iterations", C.c_int),
                 ("reliable_updates", C.c_int), ("dslash_launches", C.c_int),
                 ("dslash_ms", C.c_double), ("mdagm_launches", C.c_int),
-                ("mdagm_ms", C.c_double), ("true_rsq", C.c_double)]
+                ("mdagm_ms", C.c_double), ("true_rsq", C.c_double), ("escalated", C.c_int)]
 
 
 PRECISION = {"half": 0, "single": 1, "double": 2}

@@ -98,6 +98,7 @@ void init_context(QPHIX_layout_t *layout)
         QB_CUDA(cudaEventCreate(&c.ev_user[i]));
     }
     c.inner = env_precision(Prec::Double);
+    c.verbose = std::getenv("QPHIX_B200_VERBOSE") ? std::atoi(std::getenv("QPHIX_B200_VERBOSE")) : 0;
     c.initialized = true;
 }
 
@@ -313,6 +314,16 @@ QPHIX_status_t asqtad_dslash(typename Api<Real>::FL *H, typename Api<Real>::CV *
     });
 }
 
+// FP32 copy of a D3 link set, made on first use
+const LinkSet &single_links(QPHIX_D3_FermionLinksAsqtad *H)
+{
+    if (!H->sloppy_single.valid) {
+        H->sloppy_single = alloc_links(Prec::Single);
+        links_convert(Prec::Single, H->sloppy_single, Prec::Double, H->links, ctx().launch());
+    }
+    return H->sloppy_single;
+}
+
 template <typename Real>
 int asqtad_invert(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_invert_arg_t *inv, QPHIX_resid_arg_t *res,
                   Real mass, typename Api<Real>::CV *out, typename Api<Real>::CV *in)
@@ -351,8 +362,13 @@ int asqtad_invert(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_invert_ar
                 }
                 return H->sloppy_half;
             }();
-            if constexpr (std::is_same<Real, double>::value) iters = cg_mixed(inner, H->links, lss, a);
-            else throw Error("asqtad_invert: mixed precision is available through the D3 API");
+            if constexpr (std::is_same<Real, double>::value) {
+                const LinkSet *up = nullptr;
+                if (inner == Prec::Half) up = &single_links(H);
+                iters = cg_mixed(inner, H->links, lss, up, a);
+            } else {
+                throw Error("asqtad_invert: mixed precision is available through the D3 API");
+            }
         }
         QB_CUDA(cudaEventRecord(c.ev_solve[1], c.stream));
         QB_CUDA(cudaEventSynchronize(c.ev_solve[1]));
@@ -415,7 +431,8 @@ int asqtad_invert_multi(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_inv
                 }
                 lss = &H->sloppy_half;
             }
-            iters = multishift_mixed(inner, H->links, *lss, a);
+            const LinkSet *up = inner == Prec::Half ? &single_links(H) : nullptr;
+            iters = multishift_mixed(inner, H->links, *lss, up, a);
         } else {
             throw Error("asqtad_invert_multi: mixed precision is available through the D3 API");
         }
@@ -593,6 +610,7 @@ QPHIX_status_t QPHIX_B200_get_last_stats(QPHIX_B200_stats_t *s)
         s->mdagm_launches = t.mdagm_launches;
         s->mdagm_ms = t.mdagm_ms;
         s->true_rsq = t.true_rsq;
+        s->escalated = t.escalated;
     });
 }
 QPHIX_status_t QPHIX_B200_set_kernel_timing(int on) { return guarded([&] { ctx().kernel_timing = on ? 1 : 0; }); }

@@ -70,9 +70,13 @@ k_cg_restart(VecView<S> ttt, VecView<S> x, VecView<S> b, VecView<S> r, VecView<S
             rv[i] = bv[i] + t[i];
         }
         ttt.store(j, t);
-        r.store(j, rv);
-        if constexpr (std::is_same<S, __half>::value) r.load(j, rv);
-        if (setp) pv.store(j, rv);
+        r.store(j, rv);  // rv now holds the stored (rounded) residual
+        if (setp) {
+            A pc[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) pc[i] = rv[i];
+            pv.store(j, pc);
+        }
 #pragma unroll
         for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
         if (relres) s[1] = relres_term(rv, xv);
@@ -114,10 +118,6 @@ k_cg_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverSta
         }
         x.store(j, xv);
         r.store(j, rv);
-        if constexpr (std::is_same<S, __half>::value) {
-            r.load(j, rv);
-            x.load(j, xv);
-        }
 #pragma unroll
         for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
         if (relres) s[1] = relres_term(rv, xv);
@@ -177,7 +177,6 @@ k_ms_residual(VecView<S> r, VecView<S> ttt, SolverState *st, double *partials, i
 #pragma unroll
         for (int i = 0; i < 6; ++i) rv[i] = rv[i] + bl * t[i];
         r.store(j, rv);
-        if constexpr (std::is_same<S, __half>::value) r.load(j, rv);
 #pragma unroll
         for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
     }
@@ -280,7 +279,6 @@ k_mx_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverSta
         }
         x.store(j, xv);
         r.store(j, rv);
-        if constexpr (std::is_same<S, __half>::value) r.load(j, rv);
 #pragma unroll
         for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
     }

@@ -45,6 +45,7 @@ struct Stats {
     int mdagm_launches = 0;
     double mdagm_ms = 0;
     double true_rsq = 0;
+    int escalated = 0;
 };
 
 // CUDA-event timing of individual kernel launches inside a solve
@@ -82,6 +83,7 @@ struct Context {
     double reliable_delta = 0.1;
     int kernel_timing = 0;
     int max_chunk = 64;
+    int verbose = 0;
     Stats stats;
     KernelTimer ktimer;
     std::string last_error;
@@ -171,7 +173,7 @@ struct SolveArgs {
 // precision p (Single for the F3 API, Double for D3)
 int cg_reference(Prec p, const LinkSet &ls, SolveArgs &a);
 // mixed precision: sloppy p_s inner CG, FP64 reliable updates
-int cg_mixed(Prec ps, const LinkSet &ls64, const LinkSet &ls_s, SolveArgs &a);
+int cg_mixed(Prec ps, const LinkSet &ls64, const LinkSet &ls_s, const LinkSet *ls_up, SolveArgs &a);
 
 struct MultiArgs {
     QPHIX_info_t *info;
@@ -183,6 +185,6 @@ struct MultiArgs {
     VecBlock in[2];
 };
 int multishift_reference(Prec p, const LinkSet &ls, MultiArgs &a);
-int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &ls_s, MultiArgs &a);
+int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &ls_s, const LinkSet *ls_up, MultiArgs &a);
 
 }  // namespace qb

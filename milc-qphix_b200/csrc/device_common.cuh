@@ -56,27 +56,42 @@ template <> struct VecView<float> {
     }
 };
 
-// half storage: per-site norm = max |component|, components stored as v/norm
+// 16-bit storage: per-site norm = max |component| of the site (float), each
+// component stored as 16-bit fixed point q = round(32767 v / norm).  Inside a
+// normalised site fixed point keeps 15 bits where FP16 keeps 11.
 template <> struct VecView<__half> {
-    __half2 *p;
+    short2 *p;
     float *norm;
     int vh;
     __device__ __forceinline__ void load(int j, float v[6]) const {
-        const float n = __ldg(norm + j);
-        const float2 a = __half22float2(p[j]), b = __half22float2(p[vh + j]),
-                     c = __half22float2(p[2 * vh + j]);
+        const float n = __ldg(norm + j) * (1.0f / 32767.0f);
+        const short2 a = __ldg(p + j), b = __ldg(p + vh + j), c = __ldg(p + 2 * vh + j);
         v[0] = a.x * n; v[1] = a.y * n; v[2] = b.x * n; v[3] = b.y * n; v[4] = c.x * n; v[5] = c.y * n;
     }
-    __device__ __forceinline__ void load_cg(int j, float v[6]) const { load(j, v); }
-    __device__ __forceinline__ void store(int j, const float v[6]) const {
+    __device__ __forceinline__ void load_cg(int j, float v[6]) const {
+        const float n = __ldcg(norm + j) * (1.0f / 32767.0f);
+        const short2 a = __ldcg(p + j), b = __ldcg(p + vh + j), c = __ldcg(p + 2 * vh + j);
+        v[0] = a.x * n; v[1] = a.y * n; v[2] = b.x * n; v[3] = b.y * n; v[4] = c.x * n; v[5] = c.y * n;
+    }
+    // Stores v and replaces it by the value a later load returns, so callers
+    // never read back what they just wrote (a read-only-path load of data
+    // written by the same kernel is not coherent).
+    __device__ __forceinline__ void store(int j, float v[6]) const {
         float m = 0.f;
 #pragma unroll
         for (int k = 0; k < 6; ++k) m = fmaxf(m, fabsf(v[k]));
-        const float inv = m > 0.f ? 1.0f / m : 0.f;
+        const float inv = m > 0.f ? 32767.0f / m : 0.f;
+        const float n = m * (1.0f / 32767.0f);
+        short q[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            q[k] = (short)__float2int_rn(v[k] * inv);
+            v[k] = q[k] * n;
+        }
         norm[j] = m;
-        p[j] = __floats2half2_rn(v[0] * inv, v[1] * inv);
-        p[vh + j] = __floats2half2_rn(v[2] * inv, v[3] * inv);
-        p[2 * vh + j] = __floats2half2_rn(v[4] * inv, v[5] * inv);
+        p[j] = make_short2(q[0], q[1]);
+        p[vh + j] = make_short2(q[2], q[3]);
+        p[2 * vh + j] = make_short2(q[4], q[5]);
     }
 };
 
@@ -88,7 +103,7 @@ template <> __host__ __device__ inline VecView<float> view<float>(VecBlock b, in
     return VecView<float>{static_cast<float2 *>(b.data), vh};
 }
 template <> __host__ __device__ inline VecView<__half> view<__half>(VecBlock b, int vh) {
-    return VecView<__half>{static_cast<__half2 *>(b.data), b.norm, vh};
+    return VecView<__half>{static_cast<short2 *>(b.data), b.norm, vh};
 }
 
 // ------------------------------------------------------------------ links --

@@ -85,18 +85,11 @@ k_dslash_mdagm(DslashArgs<S> a, VecView<S> pv, double m4, SolverState *st, doubl
         const A m = (A)m4;
 #pragma unroll
         for (int i = 0; i < 6; ++i) acc[i] = acc[i] + m * p[i];
-        a.out.store(j, acc);
         // the product is formed from the stored (rounded) value, as the
-        // reference reads ttt back from memory
-        A t[6];
-        if constexpr (std::is_same<S, __half>::value) {
-            a.out.load(j, t);
-        } else {
+        // reference reads ttt back from memory; store() leaves it in acc
+        a.out.store(j, acc);
 #pragma unroll
-            for (int i = 0; i < 6; ++i) t[i] = acc[i];
-        }
-#pragma unroll
-        for (int i = 0; i < 6; ++i) dot[0] += (double)(p[i] * t[i]);
+        for (int i = 0; i < 6; ++i) dot[0] += (double)(p[i] * acc[i]);
     }
     grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) {
         st->pkp = tot[0];

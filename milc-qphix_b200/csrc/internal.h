@@ -21,8 +21,9 @@ namespace qb {
 //                  c2[c*Vh + j]  (double2 / float2).  A warp reading 32
 //                  consecutive sites issues one fully used 512 B / 256 B
 //                  transaction per component.
-// Half vector    : half2 h[c*Vh + j] holding v/norm[j], float norm[j] = max
-//                  |component| of the site (per-site scaling).
+// 16-bit vector  : short2 q[c*Vh + j], 16-bit fixed point of v/norm[j],
+//                  float norm[j] = max |component| of the site (per-site
+//                  scaling).
 // Link block     : the 16 matrices an output site needs, matrix-major then
 //                  complex element then site: m2[(mat*9 + e)*Vh + j],
 //                  e = 3*row + col, mat = 4*slot + dir with slot
@@ -50,7 +51,7 @@ inline size_t prec_real_bytes(Prec p) { return p == Prec::Double ? 8 : (p == Pre
 
 // One parity block of a colour vector in device memory.
 struct VecBlock {
-    void *data = nullptr;   // cx_t<R>[3*Vh]   (half: half2[3*Vh])
+    void *data = nullptr;   // cx_t<R>[3*Vh]   (16-bit: short2[3*Vh])
     float *norm = nullptr;  // half only: float[Vh]
 };
 

@@ -263,12 +263,16 @@ struct MixedResult {
     double true_rsq_rel = 0;
     int iterations = 0;
     int reliable_updates = 0;
+    int escalated = 0;
 };
 
-MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, VecBlock x, VecBlock b,
-                       int parity, double mass, double tol, int max_cg, TimedLaunches &tl)
+// `ls_up`: FP32 links to continue with when a 16-bit inner solve stops
+// converging (see below); may be null.
+MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const LinkSet *ls_up, VecBlock x,
+                       VecBlock b, int parity, double mass, double tol, int max_cg, TimedLaunches &tl)
 {
     Context &c = ctx();
+    const LinkSet *ls_cur = &lss;
     const Launch L = c.launch();
     SolverState &S = *c.h_state;
     const int other = 1 - parity;
@@ -317,13 +321,14 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, VecBloc
     S.counter = S.counter2 = 0;
     upload_state();
     int chunk = 8;
+    int stalled = 0;
     for (;;) {
         double size_prev = S.rsq;
         for (;;) {
             for (int k = 0; k < chunk; ++k) {
-                tl.run(0, k, [&] { dslash_gated(ps, L, tmps, pv, lss, other, c.d_state, k); });
+                tl.run(0, k, [&] { dslash_gated(ps, L, tmps, pv, *ls_cur, other, c.d_state, k); });
                 tl.run(1, k, [&] {
-                    dslash_mdagm_dot(ps, L, ttts, tmps, lss, pv, -m4, parity, c.d_state, c.d_partials, k, 0);
+                    dslash_mdagm_dot(ps, L, ttts, tmps, *ls_cur, pv, -m4, parity, c.d_state, c.d_partials, k, 0);
                 });
                 mx_update(ps, L, xs, pv, rs, ttts, c.d_state, c.d_partials, k, delta2);
                 cg_axpy(ps, L, rs, pv, c.d_state, k);
@@ -340,13 +345,36 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, VecBloc
         }
         out.iterations = S.iteration;
         const double oldrsq = S.oldrsq;
+        const double sloppy_rsq = S.rsq;
         // reliable update: x += x_s, r = b - M x in FP64
         vec_add(Prec::Double, x, ps, xs, L);
         vec_zero(ps, xs, L);
+        const double prev_true = rsq;
         rsq = true_residual();
         out.reliable_updates++;
         out.true_rsq_rel = rsq / bnorm;
+        if (c.verbose)
+            std::fprintf(stderr, "qphix_b200 mixed CG: iter %d RU %d prec %d sloppy %.3e true %.3e\n",
+                         S.iteration, out.reliable_updates, (int)ps, sloppy_rsq / bnorm, rsq / bnorm);
         if (out.true_rsq_rel < tol || S.iteration >= max_cg || !std::isfinite(rsq)) break;
+        // A 16-bit inner solve perturbs the operator by ~1e-4 relative; once
+        // the residual lives in the lowest modes of an ill-conditioned system
+        // the corrections stop reducing the true residual.  Two reliable
+        // updates in a row that fail to halve it switch the inner solve to FP32.
+        stalled = (rsq > 0.25 * prev_true) ? stalled + 1 : 0;
+        if (stalled >= 2 && ps == Prec::Half && ls_up && ls_up->valid) {
+            VecBlock p32 = ws.get(Prec::Single);
+            vec_copy(Prec::Single, p32, Prec::Half, pv, L);
+            pv = p32;
+            xs = ws.get(Prec::Single);
+            rs = ws.get(Prec::Single);
+            tmps = ws.get(Prec::Single);
+            ttts = ws.get(Prec::Single);
+            ps = Prec::Single;
+            ls_cur = ls_up;
+            stalled = 0;
+            out.escalated = 1;
+        }
         vec_copy(ps, rs, Prec::Double, r64, L);
         S.b = rsq / oldrsq;
         S.rsq = rsq;
@@ -362,7 +390,7 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, VecBloc
 
 }  // namespace
 
-int cg_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, SolveArgs &A)
+int cg_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const LinkSet *ls_up, SolveArgs &A)
 {
     Context &c = ctx();
     QPHIX_info_t *info = A.info;
@@ -379,7 +407,8 @@ int cg_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, SolveArgs &A)
     int total = 0, last = 0, rus = 0;
     double worst = 0;
     for (;;) {
-        MixedResult m = mixed_pass(ps, ls64, lss, x, b, parity, A.mass, tol, max_cg, tl);
+        MixedResult m = mixed_pass(ps, ls64, lss, ls_up, x, b, parity, A.mass, tol, max_cg, tl);
+        c.stats.escalated |= m.escalated;
         total += m.iterations;
         last = m.iterations;
         rus += m.reliable_updates;
@@ -486,6 +515,13 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
     out.iteration = S.iteration;
     out.converged = S.converged != 0;
     out.rsq = S.rsq;
+    if (c.verbose) {
+        std::fprintf(stderr, "qphix_b200 multi-shift: iter %d converged %d rsq/src %.3e active %d pkp %.3e\n",
+                     S.iteration, out.converged, S.rsq / out.source_norm, S.num_now, S.pkp);
+        for (int j = 0; j < n; ++j)
+            std::fprintf(stderr, "  shift %d: %.4e beta %.4e zeta %.4e alpha %.4e finished %d\n", j, S.shifts[j],
+                         S.beta_i[j], S.zeta_ip1[j], S.alpha[j], S.finished[j]);
+    }
     return out;
 }
 
@@ -591,7 +627,7 @@ int multishift_reference(Prec P, const LinkSet &ls, MultiArgs &A)
 // started from its multi-shift solution, to its own tolerance on the FP64
 // true residual.
 // ===========================================================================
-int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, MultiArgs &A)
+int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const LinkSet *ls_up, MultiArgs &A)
 {
     Context &c = ctx();
     const int n = A.n;
@@ -638,7 +674,8 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, MultiArgs
         last = r.iteration;
         for (int j = 0; j < n; ++j) {
             const double tol = A.res[j]->resid > 0 ? A.res[j]->resid : A.res[0]->resid;
-            MixedResult m = mixed_pass(ps, ls64, lss, x[j], src, parity, A.mass[j], tol, max_cg, tl);
+            MixedResult m = mixed_pass(ps, ls64, lss, ls_up, x[j], src, parity, A.mass[j], tol, max_cg, tl);
+            c.stats.escalated |= m.escalated;
             total += m.iterations;
             rus += m.reliable_updates;
             worst = std::max(worst, m.true_rsq_rel);

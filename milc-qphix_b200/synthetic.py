@@ -92,7 +92,8 @@ def random_su3(n, eps, rng, device=None):
     torch, dev = _torch_device(device)
     a = rng.standard_normal((n, 3, 3)) + 1j * rng.standard_normal((n, 3, 3))
     out = np.empty((n, 3, 3), dtype=np.complex128)
-    chunk = 1 << 21
+    # batched eigh: the GPU solver takes at most ~1e5 matrices per call
+    chunk = 1 << 16 if str(dev).startswith("cuda") else 1 << 21
     for s in range(0, n, chunk):
         A = torch.from_numpy(a[s:s + chunk]).to(dev)
         H = 0.5 * (A + A.mH)
