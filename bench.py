@@ -366,11 +366,64 @@ def run_reference(args):
 
 # iterations the FP64 CG (reference control flow) needs on this workload; the
 # GPU arm measures it on every run and reports it as fp64_cg.iterations
-FP64_ITERATIONS = 1500
+FP64_ITERATIONS = 808
+
+
+def run_profile_dslash(args):
+    """--mode dslash: one FP32 and one FP64 Dslash launch after a warm-up
+    (small-lattice capture target for ncu)."""
+    dims = tuple(int(v) for v in args.lattice.split("x"))
+    links = synthetic.asqtad_links(dims, seed=LINK_SEED)
+    V = int(np.prod(dims))
+    lib = capi.QphixLib(LIB_PATH)
+    assert lib.init(dims) == 0, lib.last_error()
+    out = {}
+    for prec in ("F", "D"):
+        L = lib.create_L(prec, links)
+        vin = lib.create_V(prec, np.random.default_rng(1).standard_normal(V * 6))
+        vout = lib.create_V(prec, np.zeros(V * 6))
+        ms = lib.dslash_timed(prec, L, vout, vin, "even", args.reps)
+        nbytes = (DSLASH_BYTES_F32 if prec == "F" else DSLASH_BYTES_F64) * (V // 2)
+        out[prec] = {"us": ms * 1e3, "gbs": nbytes / (ms * 1e-3) / 1e9}
+        lib.destroy_V(prec, vin)
+        lib.destroy_V(prec, vout)
+        lib.destroy_L(prec, L)
+    lib.finalize()
+    print(json.dumps({"mode": "dslash", "lattice": args.lattice, "reps": args.reps, **out}))
+
+
+def run_profile_mixed(args):
+    """--mode mixed: only the timed mixed-precision solves (ncu launch list)."""
+    links, src = make_inputs()
+    lib = capi.QphixLib(LIB_PATH)
+    assert lib.init(DIMS) == 0, lib.last_error()
+    L = lib.create_L("D", links)
+    b = lib.create_V("D", src, "even")
+    lib.set_inner_precision(args.inner)
+    res_all = []
+    for _ in range(args.warmup + args.steps):
+        x = lib.create_V("D", np.zeros_like(src), "even")
+        lib.timer_start()
+        it, info, res = lib.invert("D", L, x, b, MASS, parity="even", max_iter=MAX_ITER, nrestart=NRESTART,
+                                   resid=RESID)
+        ms = lib.timer_stop()
+        st = lib.last_stats()
+        res_all.append({"ms": ms, "iterations": st.iterations, "reliable_updates": st.reliable_updates,
+                        "true_rsq_rel": res.final_rsq})
+        lib.destroy_V("D", x)
+    lib.destroy_V("D", b)
+    lib.destroy_L("D", L)
+    lib.finalize()
+    print(json.dumps({"mode": "mixed", "inner": args.inner, "solves": res_all}))
 
 
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--mode", default="bench", choices=["bench", "dslash", "mixed"],
+                    help="bench: the benchmark line; dslash/mixed: small profiling targets")
+    ap.add_argument("--lattice", default="16x16x16x32")
+    ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--inner", default="single", choices=["single", "half", "double"])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -378,6 +431,12 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.mode == "dslash":
+        run_profile_dslash(args)
+        return
+    if args.mode == "mixed":
+        run_profile_mixed(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
