@@ -92,6 +92,8 @@ void init_context(QPHIX_layout_t *layout)
     std::memset(c.h_state, 0, sizeof(SolverState));
     QB_CUDA(cudaMalloc(&c.d_partials, sizeof(double) * 4 * kMaxPartials));
     QB_CUDA(cudaMalloc(&c.d_scalars, sizeof(double) * 64));
+    QB_CUDA(cudaMalloc(&c.d_err, sizeof(int)));
+    QB_CUDA(cudaMemset(c.d_err, 0, sizeof(int)));
     QB_CUDA(cudaMallocHost(&c.h_scalars, sizeof(double) * 64));
     for (int i = 0; i < 2; ++i) {
         QB_CUDA(cudaEventCreate(&c.ev_solve[i]));
@@ -111,6 +113,8 @@ void finalize_context()
     cudaFreeHost(c.h_state);
     cudaFree(c.d_partials);
     cudaFree(c.d_scalars);
+    cudaFree(c.d_err);
+    c.d_err = nullptr;
     cudaFreeHost(c.h_scalars);
     for (int i = 0; i < 2; ++i) {
         cudaEventDestroy(c.ev_solve[i]);
@@ -163,7 +167,7 @@ typename Api<Real>::CV *create_V(Real *src, QPHIX_evenodd_t evenodd)
             vec_from_raw(Api<Real>::prec, V->blk[cb], stage, sizeof(Real) == 8, c.launch());
         }
         dev_free(stage);
-        QB_CUDA(cudaStreamSynchronize(c.stream));
+        sync_check();
         QB_CUDA(cudaGetLastError());
         V->even = V->blk[0].data;
         V->odd = V->blk[1].data;
@@ -192,7 +196,7 @@ void extract_V(Real *dest, typename Api<Real>::CV *V)
             QB_CUDA(cudaMemcpyAsync(dest + cb * nblk, stage, nblk * sizeof(Real), cudaMemcpyDeviceToHost, c.stream));
         }
         dev_free(stage);
-        QB_CUDA(cudaStreamSynchronize(c.stream));
+        sync_check();
         QB_CUDA(cudaGetLastError());
     });
 }
@@ -203,7 +207,7 @@ void destroy_V(typename Api<Real>::CV *V)
     if (!V) return;
     guarded([&] {
         for (auto &b : V->blk) free_vec(b);
-        if (ctx().initialized) QB_CUDA(cudaStreamSynchronize(ctx().stream));
+        if (ctx().initialized) sync_check();
     });
     delete V;
 }
@@ -241,13 +245,12 @@ typename Api<Real>::FL *create_L(Real *fat, Real *lng, Real *fatback, Real *lngb
             links_from_raw(Api<Real>::prec, H->links, stage, sizeof(Real) == 8, slot, c.launch());
         }
         dev_free(stage);
-        QB_CUDA(cudaStreamSynchronize(c.stream));
+        sync_check();
         QB_CUDA(cudaGetLastError());
-        const size_t famoff = (size_t)8 * 9 * c.g.vh * (sizeof(Real) * 2);
-        H->fateven = H->links.blk[0];
-        H->fatodd = H->links.blk[1];
-        H->lngeven = static_cast<char *>(H->links.blk[0]) + famoff;
-        H->lngodd = static_cast<char *>(H->links.blk[1]) + famoff;
+        // fat and Naik links of an output parity share one block (grouped by
+        // direction), so both pointer pairs name the same blocks
+        H->fateven = H->lngeven = H->links.blk[0];
+        H->fatodd = H->lngodd = H->links.blk[1];
     });
     if (s != QPHIX_SUCCESS && H) {
         free_link_handle(H);
@@ -275,10 +278,10 @@ void extract_L(Real *fat, Real *lng, typename Api<Real>::FL *H, QPHIX_evenodd_t 
             if (evenodd & QPHIX_ODD)
                 QB_CUDA(cudaMemcpyAsync(dst[f] + nhalf, stage + nhalf, nhalf * sizeof(Real), cudaMemcpyDeviceToHost,
                                         c.stream));
-            QB_CUDA(cudaStreamSynchronize(c.stream));
+            sync_check();
         }
         dev_free(stage);
-        QB_CUDA(cudaStreamSynchronize(c.stream));
+        sync_check();
         QB_CUDA(cudaGetLastError());
     });
 }
@@ -289,7 +292,7 @@ void destroy_L(typename Api<Real>::FL *H)
     if (!H) return;
     guarded([&] {
         free_link_handle(H);
-        if (ctx().initialized) QB_CUDA(cudaStreamSynchronize(ctx().stream));
+        if (ctx().initialized) sync_check();
     });
     delete H;
 }
@@ -309,7 +312,7 @@ QPHIX_status_t asqtad_dslash(typename Api<Real>::FL *H, typename Api<Real>::CV *
         if (!(out->parity & parity) || !(in->parity & need_in))
             throw Error("asqtad_dslash: vectors lack the parities the operator needs");
         dslash(Api<Real>::prec, c.launch(), out->blk[cb], in->blk[1 - cb], H->links, cb);
-        QB_CUDA(cudaStreamSynchronize(c.stream));
+        sync_check();
         QB_CUDA(cudaGetLastError());
     });
 }
@@ -372,6 +375,7 @@ int asqtad_invert(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_invert_ar
         }
         QB_CUDA(cudaEventRecord(c.ev_solve[1], c.stream));
         QB_CUDA(cudaEventSynchronize(c.ev_solve[1]));
+        sync_check();
         float ms = 0;
         QB_CUDA(cudaEventElapsedTime(&ms, c.ev_solve[0], c.ev_solve[1]));
         c.stats.solve_ms = ms;
@@ -438,6 +442,7 @@ int asqtad_invert_multi(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_inv
         }
         QB_CUDA(cudaEventRecord(c.ev_solve[1], c.stream));
         QB_CUDA(cudaEventSynchronize(c.ev_solve[1]));
+        sync_check();
         float ms = 0;
         QB_CUDA(cudaEventElapsedTime(&ms, c.ev_solve[0], c.ev_solve[1]));
         c.stats.solve_ms = ms;
@@ -460,11 +465,14 @@ QPHIX_status_t dslash_timed(void *links, void *out, void *in, QPHIX_evenodd_t pa
         if (parity != QPHIX_EVEN && parity != QPHIX_ODD) throw Error("dslash_timed: parity must be EVEN or ODD");
         const int cb = parity == QPHIX_EVEN ? 0 : 1;
         if (!O->blk[cb].data || !I->blk[1 - cb].data) throw Error("dslash_timed: vectors lack the needed parity");
+        // one untimed launch first: module loading and one-time kernel set-up
+        dslash(Api<Real>::prec, c.launch(), O->blk[cb], I->blk[1 - cb], H->links, cb);
         QB_CUDA(cudaEventRecord(c.ev_user[0], c.stream));
         for (int r = 0; r < reps; ++r)
             dslash(Api<Real>::prec, c.launch(), O->blk[cb], I->blk[1 - cb], H->links, cb);
         QB_CUDA(cudaEventRecord(c.ev_user[1], c.stream));
         QB_CUDA(cudaEventSynchronize(c.ev_user[1]));
+        sync_check();
         float t = 0;
         QB_CUDA(cudaEventElapsedTime(&t, c.ev_user[0], c.ev_user[1]));
         *ms = t / reps;

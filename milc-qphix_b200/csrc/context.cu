@@ -86,7 +86,20 @@ void download_state()
 {
     Context &c = ctx();
     QB_CUDA(cudaMemcpyAsync(c.h_state, c.d_state, sizeof(SolverState), cudaMemcpyDeviceToHost, c.stream));
+    sync_check();
+}
+
+void sync_check()
+{
+    Context &c = ctx();
     QB_CUDA(cudaStreamSynchronize(c.stream));
+    if (!c.d_err) return;
+    int e = 0;
+    QB_CUDA(cudaMemcpy(&e, c.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        QB_CUDA(cudaMemset(c.d_err, 0, sizeof(int)));
+        throw Error("a Dslash pipeline wait timed out on the GPU; the call's results are invalid");
+    }
 }
 
 }  // namespace qb

@@ -88,7 +88,9 @@ struct Context {
     KernelTimer ktimer;
     std::string last_error;
 
-    Launch launch() const { return Launch{stream, &g}; }
+    int *d_err = nullptr;            // kernel failure word (bounded waits)
+
+    Launch launch() const { return Launch{stream, &g, d_err}; }
 };
 
 Context &ctx();
@@ -104,6 +106,7 @@ void free_links(LinkSet &ls);
 
 void upload_state();    // h_state -> d_state (async)
 void download_state();  // d_state -> h_state, waits
+void sync_check();      // waits for the stream; throws if a kernel reported a failed wait
 
 double wall_seconds();
 

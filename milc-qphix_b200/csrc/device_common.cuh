@@ -109,48 +109,57 @@ template <> __host__ __device__ inline VecView<__half> view<__half>(VecBlock b, 
 // ------------------------------------------------------------------ links --
 // Streaming loads (evict-first): every link is used once per Dslash, so
 // links must not displace the gathered colour vectors from L1/L2.
+// Layout: see link_cx_index (internal.h).  Each precision loads whole
+// 16-byte chunks, as many per batch as the arithmetic that follows needs, so
+// a thread keeps 150-300 bytes of loads in flight.
+
 template <typename S> struct LinkView;
 
+// FP64: one matrix (9 double2 chunks) at a time
 template <> struct LinkView<double> {
     const double2 *p;
     int vh;
-    __device__ __forceinline__ void load(int mat, int j, double u[18]) const {
-        const double2 *q = p + (size_t)mat * 9 * vh + j;
+    __device__ __forceinline__ void load_mat(int d, int s, int j, double u[18]) const {
 #pragma unroll
         for (int e = 0; e < 9; ++e) {
-            const double2 z = __ldcs(q + (size_t)e * vh);
+            const double2 z = __ldcs(p + link_cx_index(1, d, 9 * s + e, j, vh));
             u[2 * e] = z.x; u[2 * e + 1] = z.y;
         }
     }
 };
 
+// FP32: a forward/backward pair (slots 2h, 2h+1) is 18 complex = 9 float4
 template <> struct LinkView<float> {
-    const float2 *p;
+    const float4 *p;
     int vh;
-    __device__ __forceinline__ void load(int mat, int j, float u[18]) const {
-        const float2 *q = p + (size_t)mat * 9 * vh + j;
+    __device__ __forceinline__ void load_pair(int d, int h, int j, float u[36]) const {
+        const float4 *q = p + ((size_t)d * 18 + 9 * h) * vh + j;
 #pragma unroll
-        for (int e = 0; e < 9; ++e) {
-            const float2 z = __ldcs(q + (size_t)e * vh);
-            u[2 * e] = z.x; u[2 * e + 1] = z.y;
+        for (int c = 0; c < 9; ++c) {
+            const float4 z = __ldcs(q + (size_t)c * vh);
+            u[4 * c] = z.x; u[4 * c + 1] = z.y; u[4 * c + 2] = z.z; u[4 * c + 3] = z.w;
         }
     }
 };
 
-// 16-bit fixed point links: value = q * link_max / 32767, one range for the
-// fat slots (mat < 8) and one for the Naik slots
+// 16-bit fixed point: value = q * link_max / 32767 with one range for the fat
+// slots and one for the Naik slots; all four matrices of a direction are
+// 36 complex = 9 chunks of 16 bytes
 template <> struct LinkView<__half> {
-    const short2 *p;
+    const int4 *p;
     int vh;
     float scale_fat, scale_long;
-    __device__ __forceinline__ void load(int mat, int j, float u[18]) const {
-        const short2 *q = p + (size_t)mat * 9 * vh + j;
-        const float scale = mat < 8 ? scale_fat : scale_long;
+    __device__ __forceinline__ void load_quad(int d, int j, int4 raw[9]) const {
+        const int4 *q = p + (size_t)d * 9 * vh + j;
 #pragma unroll
-        for (int e = 0; e < 9; ++e) {
-            const short2 z = __ldcs(q + (size_t)e * vh);
-            u[2 * e] = z.x * scale; u[2 * e + 1] = z.y * scale;
-        }
+        for (int c = 0; c < 9; ++c) raw[c] = __ldcs(q + (size_t)c * vh);
+    }
+    // matrix of slot s out of the raw chunks
+    __device__ __forceinline__ void unpack(const int4 raw[9], int s, float u[18]) const {
+        const float sc = s < 2 ? scale_fat : scale_long;
+        const short *h = reinterpret_cast<const short *>(raw);
+#pragma unroll
+        for (int e = 0; e < 18; ++e) u[e] = h[18 * s + e] * sc;
     }
 };
 
@@ -258,5 +267,76 @@ __device__ __forceinline__ bool gated_off(const SolverState *st, int gate)
 }
 
 inline int grid_for(int n) { return (n + kBlock - 1) / kBlock; }
+
+// ------------------------------------------------- TMA bulk copies (sm_100a) --
+// 1-D bulk copy global -> shared completing on an mbarrier (no multicast).
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// order this thread's earlier generic-proxy shared accesses before later
+// async-proxy (bulk copy) writes to shared memory
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// dst, src 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                         uint64_t policy)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+
+// L2 eviction policy for data read exactly once (links)
+__device__ __forceinline__ uint64_t policy_evict_first()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: gives up after `limit` polls (each poll may suspend the
+// thread for a short, hardware-defined time) and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t limit = 1u << 22)
+{
+    for (uint32_t i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
 
 }  // namespace qb

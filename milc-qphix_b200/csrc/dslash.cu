@@ -14,6 +14,9 @@
 //
 // Roofline: 1146 flop per site against >= 1200 B (FP32, 18-real links):
 // memory bound on HBM.
+#include <cstdlib>
+#include <cstring>
+
 #include "device_common.cuh"
 
 namespace qb {
@@ -27,31 +30,106 @@ struct DslashArgs {
     int cb;
 };
 
+// Neighbour k of output site s: one hop 2*d (backward) / 2*d+1 (forward),
+// three hops 8+2*d / 9+2*d (the reference's NeighTable order).
 template <typename S, typename A>
 __device__ __forceinline__ void dslash_site(const DslashArgs<S> &a, int j, A acc[6])
 {
     const SiteCoords s = decode(a.g, a.cb, j);
 #pragma unroll
     for (int i = 0; i < 6; ++i) acc[i] = A(0);
+    if constexpr (std::is_same<S, double>::value) {
+        // FP64: one matrix and its neighbour per batch (192 bytes in flight)
 #pragma unroll
-    for (int dir = 0; dir < 4; ++dir) {
-        A u[18], v[6];
-        // fat link, forward:  F_dir(x) psi(x + dir)
-        a.in.load(neighbor(a.g, s, 2 * dir + 1), v);
-        a.links.load(0 * 4 + dir, j, u);
-        mv_add(acc, u, v);
-        // fat link, backward: -B_dir(x)^dag psi(x - dir)
-        a.in.load(neighbor(a.g, s, 2 * dir), v);
-        a.links.load(1 * 4 + dir, j, u);
-        mv_adj_sub(acc, u, v);
-        // Naik link, forward:  L_dir(x) psi(x + 3 dir)
-        a.in.load(neighbor(a.g, s, 8 + 2 * dir + 1), v);
-        a.links.load(2 * 4 + dir, j, u);
-        mv_add(acc, u, v);
-        // Naik link, backward: -LB_dir(x)^dag psi(x - 3 dir)
-        a.in.load(neighbor(a.g, s, 8 + 2 * dir), v);
-        a.links.load(3 * 4 + dir, j, u);
-        mv_adj_sub(acc, u, v);
+        for (int d = 0; d < 4; ++d) {
+#pragma unroll
+            for (int sl = 0; sl < 4; ++sl) {
+                const int k = (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1);
+                A u[18], v[6];
+                a.in.load(neighbor(a.g, s, k), v);
+                a.links.load_mat(d, sl, j, u);
+                if (sl & 1) mv_adj_sub(acc, u, v);
+                else mv_add(acc, u, v);
+            }
+        }
+    } else if constexpr (std::is_same<S, float>::value) {
+        // FP32: forward/backward pair, 9 float4 + 2 neighbours per batch
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int kf = 8 * h + 2 * d + 1, kb = 8 * h + 2 * d;
+                A u[36], vf[6], vb[6];
+                a.in.load(neighbor(a.g, s, kf), vf);
+                a.in.load(neighbor(a.g, s, kb), vb);
+                a.links.load_pair(d, h, j, u);
+                mv_add(acc, u, vf);
+                mv_adj_sub(acc, u + 18, vb);
+            }
+        }
+    } else {
+        // 16-bit: the four matrices of a direction, 9 x 16 bytes + 4 neighbours
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            int4 raw[9];
+            A v[4][6];
+#pragma unroll
+            for (int sl = 0; sl < 4; ++sl)
+                a.in.load(neighbor(a.g, s, (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1)), v[sl]);
+            a.links.load_quad(d, j, raw);
+#pragma unroll
+            for (int sl = 0; sl < 4; ++sl) {
+                A u[18];
+                a.links.unpack(raw, sl, u);
+                if (sl & 1) mv_adj_sub(acc, u, v[sl]);
+                else mv_add(acc, u, v[sl]);
+            }
+        }
+    }
+}
+
+// Scalar step after p.(M^dag M p) is known: CG (mode 0) a = -rsq/pkp;
+// multi-shift (mode 1) the shift recurrences.  Runs in one thread.
+__device__ __forceinline__ void mdagm_finalize(SolverState *st, double pkp, int mode)
+{
+    st->pkp = pkp;
+    st->iteration += 1;
+    if (mode == 0) {
+        st->a = round_to(-st->rsq / pkp, st->prec_single);
+    } else {
+        // multi-shift scalar recurrences (ks_multicg_offset.cpp:475-496);
+        // the values of the previous iteration are scrolled first
+        // (:617-622), which the reference does at the end of that iteration
+        const int single = st->prec_single;
+        const int jl = st->j_low;
+        if (!st->first_iter) {
+            for (int k = 0; k < st->num_now; ++k) {
+                st->beta_im1[k] = st->beta_i[k];
+                st->zeta_im1[k] = st->zeta_i[k];
+                st->zeta_i[k] = st->zeta_ip1[k];
+            }
+        }
+        st->first_iter = 0;
+        st->beta_i[jl] = round_to(-st->rsq / pkp, single);
+        st->zeta_ip1[jl] = 1.0;
+        int nn = st->num_now;
+        for (int k = 0; k < nn; ++k) {
+            if (k == jl) continue;
+            double z = round_to(round_to(st->zeta_i[k] * st->zeta_im1[k], single) * st->beta_im1[jl], single);
+            const double c1 = round_to(round_to(st->beta_i[jl] * st->alpha[jl], single) *
+                                           round_to(st->zeta_im1[k] - st->zeta_i[k], single), single);
+            const double c2 = round_to(round_to(st->zeta_im1[k] * st->beta_im1[jl], single) *
+                                           (1.0 + round_to(st->shifts[k] * st->beta_i[jl], single)), single);
+            const double den = round_to(c1 + c2, single);
+            if (den != 0.0) z = round_to(z / den, single);
+            else { z = 0.0; st->finished[k] = 1; }
+            st->zeta_ip1[k] = z;
+            if (st->zeta_i[k] != 0.0)
+                st->beta_i[k] = round_to(round_to(st->beta_i[jl] * z, single) / st->zeta_i[k], single);
+            else { st->zeta_ip1[k] = 0.0; st->beta_i[k] = 0.0; st->finished[k] = 1; }
+            if (st->finished[k] == 1 && k == nn - 1 && k > jl) nn--;
+        }
+        st->num_now = nn;
     }
 }
 
@@ -60,11 +138,11 @@ __global__ void __launch_bounds__(kBlock) k_dslash(DslashArgs<S> a, const Solver
 {
     using A = typename Acc<S>::type;
     if (st && gated_off(st, gate)) return;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= a.g.vh) return;
-    A acc[6];
-    dslash_site<S, A>(a, j, acc);
-    a.out.store(j, acc);
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.g.vh; j += gridDim.x * blockDim.x) {
+        A acc[6];
+        dslash_site<S, A>(a, j, acc);
+        a.out.store(j, acc);
+    }
 }
 
 // ttt = D tmp + m4 * p ;  pkp = sum p . ttt  (calc_pkp, ks_d_congrad_fn.cpp:159-171;
@@ -76,9 +154,8 @@ k_dslash_mdagm(DslashArgs<S> a, VecView<S> pv, double m4, SolverState *st, doubl
 {
     using A = typename Acc<S>::type;
     if (gated_off(st, gate)) return;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
     double dot[1] = {0.0};
-    if (j < a.g.vh) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.g.vh; j += gridDim.x * blockDim.x) {
         A acc[6], p[6];
         dslash_site<S, A>(a, j, acc);
         pv.load_cg(j, p);
@@ -91,47 +168,173 @@ k_dslash_mdagm(DslashArgs<S> a, VecView<S> pv, double m4, SolverState *st, doubl
 #pragma unroll
         for (int i = 0; i < 6; ++i) dot[0] += (double)(p[i] * acc[i]);
     }
-    grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) {
-        st->pkp = tot[0];
-        st->iteration += 1;
-        if (mode == 0) {
-            st->a = round_to(-st->rsq / tot[0], st->prec_single);
-        } else {
-            // multi-shift scalar recurrences (ks_multicg_offset.cpp:475-496);
-            // the values of the previous iteration are scrolled first
-            // (:617-622), which the reference does at the end of that iteration
-            const int single = st->prec_single;
-            const int jl = st->j_low;
-            if (!st->first_iter) {
-                for (int k = 0; k < st->num_now; ++k) {
-                    st->beta_im1[k] = st->beta_i[k];
-                    st->zeta_im1[k] = st->zeta_i[k];
-                    st->zeta_i[k] = st->zeta_ip1[k];
+    grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) { mdagm_finalize(st, tot[0], mode); });
+}
+
+// ---------------------------------------------------------------------------
+// TMA-pipelined Dslash.  A persistent CTA owns tiles of T consecutive output
+// sites; for each tile it visits the 4 directions in turn.  The link chunks
+// of one (tile, direction) -- C runs of T x 16 contiguous bytes in the link
+// block -- are brought into shared memory by cp.async.bulk copies issued by
+// one thread and completing on an mbarrier; NS such stages are in flight, so
+// HBM streaming no longer depends on how many loads a thread keeps in
+// registers.  Neighbour vectors are gathered from L2/L1 as in the plain
+// kernel.  Every mbarrier wait is bounded: on a timeout the CTA records the
+// failure in *err and stops.
+// ---------------------------------------------------------------------------
+template <typename S> struct TmaCfg;
+template <> struct TmaCfg<double> { static constexpr int C = 36, T = 128, NS = 2; };
+template <> struct TmaCfg<float> { static constexpr int C = 18, T = 128, NS = 3; };
+template <> struct TmaCfg<__half> { static constexpr int C = 9, T = 128, NS = 4; };
+
+template <typename S>
+constexpr size_t tma_smem_bytes()
+{
+    return (size_t)TmaCfg<S>::NS * TmaCfg<S>::C * TmaCfg<S>::T * 16 + TmaCfg<S>::NS * sizeof(uint64_t);
+}
+
+// contribution of direction d from the staged chunks (chunk q of this
+// thread's site at ch[q*T])
+template <typename S, typename A>
+__device__ __forceinline__ void tma_direction(const DslashArgs<S> &a, const SiteCoords &s, int d,
+                                              const uint4 *ch, A acc[6])
+{
+    constexpr int T = TmaCfg<S>::T;
+    A v[4][6];
+#pragma unroll
+    for (int sl = 0; sl < 4; ++sl)
+        a.in.load(neighbor(a.g, s, (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1)), v[sl]);
+    if constexpr (std::is_same<S, double>::value) {
+        const double2 *c2 = reinterpret_cast<const double2 *>(ch);
+#pragma unroll
+        for (int sl = 0; sl < 4; ++sl) {
+            A u[18];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) {
+                const double2 z = c2[(9 * sl + e) * T];
+                u[2 * e] = z.x; u[2 * e + 1] = z.y;
+            }
+            if (sl & 1) mv_adj_sub(acc, u, v[sl]);
+            else mv_add(acc, u, v[sl]);
+        }
+    } else if constexpr (std::is_same<S, float>::value) {
+        const float4 *c4 = reinterpret_cast<const float4 *>(ch);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            A u[36];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                const float4 z = c4[(9 * h + c) * T];
+                u[4 * c] = z.x; u[4 * c + 1] = z.y; u[4 * c + 2] = z.z; u[4 * c + 3] = z.w;
+            }
+            mv_add(acc, u, v[2 * h]);
+            mv_adj_sub(acc, u + 18, v[2 * h + 1]);
+        }
+    } else {
+        const int4 *c4 = reinterpret_cast<const int4 *>(ch);
+        int4 raw[9];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) raw[c] = c4[c * T];
+#pragma unroll
+        for (int sl = 0; sl < 4; ++sl) {
+            A u[18];
+            a.links.unpack(raw, sl, u);
+            if (sl & 1) mv_adj_sub(acc, u, v[sl]);
+            else mv_add(acc, u, v[sl]);
+        }
+    }
+}
+
+// MODE 0: out = D in.  MODE 1: out = D in + m4 p, p.out reduced, then the
+// solver's scalar step (mdagm_finalize).
+template <typename S, int MODE>
+__global__ void __launch_bounds__(TmaCfg<S>::T)
+k_dslash_tma(DslashArgs<S> a, const char *links, VecView<S> pv, double m4, SolverState *st, double *partials,
+             int gate, int mode, int *err)
+{
+    using A = typename Acc<S>::type;
+    constexpr int C = TmaCfg<S>::C, T = TmaCfg<S>::T, NS = TmaCfg<S>::NS;
+    if (st && gated_off(st, gate)) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint4 *buf = reinterpret_cast<uint4 *>(smem);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)NS * C * T * 16);
+    __shared__ int s_fail;
+    const int tid = threadIdx.x;
+    const int vh = a.g.vh;
+    const int ntiles = (vh + T - 1) / T;
+    const int my_tiles = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int total = 4 * my_tiles;
+    if (tid == 0) {
+        for (int b = 0; b < NS; ++b) mbar_init(&bars[b], 1);
+        fence_mbar_init();
+        s_fail = 0;
+    }
+    __syncthreads();
+    const uint64_t policy = policy_evict_first();
+    auto issue = [&](int g) {
+        const int tile = (int)blockIdx.x + (g >> 2) * (int)gridDim.x;
+        const int d = g & 3;
+        const int j0 = tile * T;
+        const int n = min(T, vh - j0);
+        const int b = g % NS;
+        mbar_arrive_expect_tx(&bars[b], (uint32_t)(C * n * 16));
+#pragma unroll 1
+        for (int q = 0; q < C; ++q)
+            bulk_g2s(buf + ((size_t)b * C + q) * T, links + ((((size_t)d * C + q) * vh + j0) << 4),
+                     (uint32_t)(n * 16), &bars[b], policy);
+    };
+    if (tid == 0) {
+        fence_proxy_async_smem();
+        for (int g = 0; g < NS - 1 && g < total; ++g) issue(g);
+    }
+    double dot[1] = {0.0};
+    A acc[6];
+    int g = 0;
+    for (; g < total; ++g) {
+        if (tid == 0 && g + NS - 1 < total) {
+            fence_proxy_async_smem();
+            issue(g + NS - 1);
+        }
+        const int tile = (int)blockIdx.x + (g >> 2) * (int)gridDim.x;
+        const int d = g & 3;
+        const int j = tile * T + tid;
+        const int b = g % NS;
+        if (d == 0) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) acc[i] = A(0);
+        }
+        if (!mbar_wait_bounded(&bars[b], (uint32_t)((g / NS) & 1))) s_fail = 1;
+        if (j < vh) {
+            const SiteCoords s = decode(a.g, a.cb, j);
+            tma_direction<S, A>(a, s, d, buf + (size_t)b * C * T + tid, acc);
+            if (d == 3) {
+                if constexpr (MODE == 0) {
+                    a.out.store(j, acc);
+                } else {
+                    A p[6];
+                    pv.load_cg(j, p);
+                    const A m = (A)m4;
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) acc[i] = acc[i] + m * p[i];
+                    a.out.store(j, acc);  // acc now holds the stored (rounded) value
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) dot[0] += (double)(p[i] * acc[i]);
                 }
             }
-            st->first_iter = 0;
-            st->beta_i[jl] = round_to(-st->rsq / tot[0], single);
-            st->zeta_ip1[jl] = 1.0;
-            int nn = st->num_now;
-            for (int k = 0; k < nn; ++k) {
-                if (k == jl) continue;
-                double z = round_to(round_to(st->zeta_i[k] * st->zeta_im1[k], single) * st->beta_im1[jl], single);
-                const double c1 = round_to(round_to(st->beta_i[jl] * st->alpha[jl], single) *
-                                               round_to(st->zeta_im1[k] - st->zeta_i[k], single), single);
-                const double c2 = round_to(round_to(st->zeta_im1[k] * st->beta_im1[jl], single) *
-                                               (1.0 + round_to(st->shifts[k] * st->beta_i[jl], single)), single);
-                const double den = round_to(c1 + c2, single);
-                if (den != 0.0) z = round_to(z / den, single);
-                else { z = 0.0; st->finished[k] = 1; }
-                st->zeta_ip1[k] = z;
-                if (st->zeta_i[k] != 0.0)
-                    st->beta_i[k] = round_to(round_to(st->beta_i[jl] * z, single) / st->zeta_i[k], single);
-                else { st->zeta_ip1[k] = 0.0; st->beta_i[k] = 0.0; st->finished[k] = 1; }
-                if (st->finished[k] == 1 && k == nn - 1 && k > jl) nn--;
-            }
-            st->num_now = nn;
         }
-    });
+        __syncthreads();
+        if (s_fail) break;
+    }
+    if (s_fail) {
+        if (tid == 0) {
+            atomicExch(err, 1);
+            // let copies still in flight land before the CTA's shared memory is released
+            for (int b = 0; b < NS; ++b) (void)mbar_wait_bounded(&bars[b], (uint32_t)(((g + b) / NS) & 1), 1u << 16);
+        }
+        return;
+    }
+    if constexpr (MODE == 1)
+        grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) { mdagm_finalize(st, tot[0], mode); });
 }
 
 template <typename S>
@@ -141,14 +344,65 @@ static DslashArgs<S> make_args(const Launch &L, VecBlock out, VecBlock in, const
     a.out = view<S>(out, L.g->vh);
     a.in = view<S>(in, L.g->vh);
     if constexpr (std::is_same<S, __half>::value) {
-        a.links = LinkView<__half>{static_cast<const short2 *>(ls.blk[cb]), L.g->vh,
+        a.links = LinkView<__half>{static_cast<const int4 *>(ls.blk[cb]), L.g->vh,
                                    ls.link_max[0] / 32767.0f, ls.link_max[1] / 32767.0f};
+    } else if constexpr (std::is_same<S, float>::value) {
+        a.links = LinkView<float>{static_cast<const float4 *>(ls.blk[cb]), L.g->vh};
     } else {
-        a.links = LinkView<S>{static_cast<const cx_t<S> *>(ls.blk[cb]), L.g->vh};
+        a.links = LinkView<double>{static_cast<const double2 *>(ls.blk[cb]), L.g->vh};
     }
     a.g = *L.g;
     a.cb = cb;
     return a;
+}
+
+// Grid of the site loops: every block resident at once (no partial last
+// wave), each thread striding over the sites.
+template <typename K>
+static int resident_grid(K kernel, int vh)
+{
+    static int per_sm = -1, sms = 0;
+    if (per_sm < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+    }
+    const int need = grid_for(vh);
+    const int full = per_sm * sms;
+    return need < full ? need : full;
+}
+
+// grid of the persistent TMA kernel: all CTAs resident
+template <typename S, int MODE>
+static int tma_grid(int vh)
+{
+    static int per_sm = -1, sms = 0;
+    if (per_sm < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(k_dslash_tma<S, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tma_smem_bytes<S>());
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dslash_tma<S, MODE>, TmaCfg<S>::T,
+                                                          tma_smem_bytes<S>()) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+    }
+    const int ntiles = (vh + TmaCfg<S>::T - 1) / TmaCfg<S>::T;
+    return ntiles < per_sm * sms ? ntiles : per_sm * sms;
+}
+
+// Dslash kernel choice: the TMA pipeline, or the plain register-streaming
+// kernel when QPHIX_B200_DSLASH=plain (kept for comparison measurements).
+static bool use_tma()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = std::getenv("QPHIX_B200_DSLASH");
+        v = (e && !std::strcmp(e, "plain")) ? 0 : 1;
+    }
+    return v == 1;
 }
 
 template <typename S>
@@ -156,7 +410,13 @@ static void launch_dslash(const Launch &L, VecBlock out, VecBlock in, const Link
                           const SolverState *st, int gate)
 {
     auto a = make_args<S>(L, out, in, ls, cb);
-    k_dslash<S><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, st, gate);
+    if (use_tma()) {
+        k_dslash_tma<S, 0><<<tma_grid<S, 0>(L.g->vh), TmaCfg<S>::T, tma_smem_bytes<S>(), L.stream>>>(
+            a, static_cast<const char *>(ls.blk[cb]), a.out, 0.0, const_cast<SolverState *>(st), nullptr, gate, 0,
+            L.err);
+    } else {
+        k_dslash<S><<<resident_grid(k_dslash<S>, L.g->vh), kBlock, 0, L.stream>>>(a, st, gate);
+    }
 }
 
 void dslash(Prec p, const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb)
@@ -184,8 +444,13 @@ static void launch_mdagm(const Launch &L, VecBlock ttt, VecBlock tmp, const Link
                          int gate, int mode)
 {
     auto a = make_args<S>(L, ttt, tmp, ls, cb);
-    k_dslash_mdagm<S><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, view<S>(pv, L.g->vh), m4, st,
-                                                                   partials, gate, mode);
+    if (use_tma()) {
+        k_dslash_tma<S, 1><<<tma_grid<S, 1>(L.g->vh), TmaCfg<S>::T, tma_smem_bytes<S>(), L.stream>>>(
+            a, static_cast<const char *>(ls.blk[cb]), view<S>(pv, L.g->vh), m4, st, partials, gate, mode, L.err);
+    } else {
+        k_dslash_mdagm<S><<<resident_grid(k_dslash_mdagm<S>, L.g->vh), kBlock, 0, L.stream>>>(
+            a, view<S>(pv, L.g->vh), m4, st, partials, gate, mode);
+    }
 }
 
 void dslash_mdagm_dot(Prec p, const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls,

@@ -24,21 +24,31 @@ namespace qb {
 // 16-bit vector  : short2 q[c*Vh + j], 16-bit fixed point of v/norm[j],
 //                  float norm[j] = max |component| of the site (per-site
 //                  scaling).
-// Link block     : the 16 matrices an output site needs, matrix-major then
-//                  complex element then site: m2[(mat*9 + e)*Vh + j],
-//                  e = 3*row + col, mat = 4*slot + dir with slot
-//                  0 fat forward F_dir(x), 1 fat backward B_dir(x),
-//                  2 Naik forward L_dir(x), 3 Naik backward LB_dir(x).
-//                  Every link is read once per Dslash as a contiguous,
-//                  coalesced stream; nothing about links is gathered.
-//                  The block for output parity cb is built from the raw
-//                  sites cb*Vh + j (qphix_f3.cpp:995-1018).
+// Link block     : the 16 matrices an output site needs, grouped by
+//                  direction d: slot s = 0 fat forward F_d(x), 1 fat backward
+//                  B_d(x), 2 Naik forward L_d(x), 3 Naik backward LB_d(x);
+//                  complex c = 9*s + 3*row + col, 36 per direction, stored in
+//                  16-byte chunks of k complex (k = 1 FP64, 2 FP32, 4 16-bit),
+//                  chunk-major then site: chunk q of direction d is element
+//                  (d*36/k + q)*Vh + j (see link_cx_index).  Every link is
+//                  read once per Dslash as a coalesced 16-byte stream;
+//                  nothing about links is gathered.  The block for output
+//                  parity cb is built from raw sites cb*Vh + j
+//                  (qphix_f3.cpp:995-1018).
 // Half links     : short2 fixed point per complex, value = q * link_max/32767
 //                  with one range for the fat slots and one for the Naik
 //                  slots (Naik links are ~1/24 the size of fat links).
 // ----------------------------------------------------------------------------
 constexpr int kMats = 16;
 constexpr int kLinkReals = kMats * 18;  // reals per site in a link block
+
+// index, in complex units of the block's precision, of complex c (0..35) of
+// direction d at site j; k = complex numbers per 16-byte chunk
+__host__ __device__ inline size_t link_cx_index(int k, int d, int c, int j, int vh)
+{
+    const int C = 36 / k;
+    return (((size_t)d * C + c / k) * vh + j) * k + (c % k);
+}
 
 template <typename R> struct Cx;
 template <> struct Cx<double> { using type = double2; };
@@ -106,6 +116,7 @@ struct SolverState {
 struct Launch {
     cudaStream_t stream;
     const Geom *g;
+    int *err;  // device word set by a kernel whose bounded wait gave up
 };
 
 // out[cb] = D in[1-cb];  links = block of output parity cb

@@ -86,40 +86,42 @@ void vec_to_raw(Prec p, void *raw_dev, bool raw_double, VecBlock src, const Laun
 }
 
 // ------------------------------------------------------------------ links --
-// one thread per (raw site, dir, complex element); raw reads are coalesced
+// complex numbers per 16-byte chunk of each precision's link block
+inline int link_k(Prec p) { return p == Prec::Double ? 1 : (p == Prec::Single ? 2 : 4); }
+
+// one thread per (raw site, dir, complex element) of one raw link family
+// (slot s); raw reads are coalesced
 template <typename D, typename RAW>
-__global__ void k_links_from_raw(D *blk0, D *blk1, const RAW *raw, int slot, int vh)
+__global__ void k_links_from_raw(D *blk0, D *blk1, const RAW *raw, int slot, int vh, int k)
 {
     const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     const size_t total = (size_t)2 * vh * 36;
     if (idx >= total) return;
     const int e = idx % 9;
-    const int dir = (idx / 9) % 4;
+    const int d = (idx / 9) % 4;
     const size_t s = idx / 36;
     const int cb = s >= (size_t)vh;
     const int j = (int)(s - (size_t)cb * vh);
-    const int mat = 4 * slot + dir;
     D *blk = cb ? blk1 : blk0;
     D z;
     z.x = raw[2 * idx];
     z.y = raw[2 * idx + 1];
-    blk[((size_t)mat * 9 + e) * vh + j] = z;
+    blk[link_cx_index(k, d, 9 * slot + e, j, vh)] = z;
 }
 
 template <typename S, typename RAW>
-__global__ void k_links_to_raw(RAW *raw, const S *blk0, const S *blk1, int slot, int vh)
+__global__ void k_links_to_raw(RAW *raw, const S *blk0, const S *blk1, int slot, int vh, int k)
 {
     const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     const size_t total = (size_t)2 * vh * 36;
     if (idx >= total) return;
     const int e = idx % 9;
-    const int dir = (idx / 9) % 4;
+    const int d = (idx / 9) % 4;
     const size_t s = idx / 36;
     const int cb = s >= (size_t)vh;
     const int j = (int)(s - (size_t)cb * vh);
-    const int mat = 4 * slot + dir;
     const S *blk = cb ? blk1 : blk0;
-    const S z = blk[((size_t)mat * 9 + e) * vh + j];
+    const S z = blk[link_cx_index(k, d, 9 * slot + e, j, vh)];
     raw[2 * idx] = (RAW)z.x;
     raw[2 * idx + 1] = (RAW)z.y;
 }
@@ -130,20 +132,21 @@ void links_from_raw(Prec p, LinkSet &ls, const void *raw_dev, bool raw_double, i
 {
     const int vh = L.g->vh;
     const int grid = grid_links(vh);
+    const int k = link_k(p);
     if (p == Prec::Double) {
         if (raw_double)
             k_links_from_raw<double2, double><<<grid, kBlock, 0, L.stream>>>(
-                (double2 *)ls.blk[0], (double2 *)ls.blk[1], (const double *)raw_dev, slot, vh);
+                (double2 *)ls.blk[0], (double2 *)ls.blk[1], (const double *)raw_dev, slot, vh, k);
         else
             k_links_from_raw<double2, float><<<grid, kBlock, 0, L.stream>>>(
-                (double2 *)ls.blk[0], (double2 *)ls.blk[1], (const float *)raw_dev, slot, vh);
+                (double2 *)ls.blk[0], (double2 *)ls.blk[1], (const float *)raw_dev, slot, vh, k);
     } else if (p == Prec::Single) {
         if (raw_double)
             k_links_from_raw<float2, double><<<grid, kBlock, 0, L.stream>>>(
-                (float2 *)ls.blk[0], (float2 *)ls.blk[1], (const double *)raw_dev, slot, vh);
+                (float2 *)ls.blk[0], (float2 *)ls.blk[1], (const double *)raw_dev, slot, vh, k);
         else
             k_links_from_raw<float2, float><<<grid, kBlock, 0, L.stream>>>(
-                (float2 *)ls.blk[0], (float2 *)ls.blk[1], (const float *)raw_dev, slot, vh);
+                (float2 *)ls.blk[0], (float2 *)ls.blk[1], (const float *)raw_dev, slot, vh, k);
     }
 }
 
@@ -151,50 +154,58 @@ void links_to_raw(Prec p, void *raw_dev, bool raw_double, const LinkSet &ls, int
 {
     const int vh = L.g->vh;
     const int grid = grid_links(vh);
+    const int k = link_k(p);
     if (p == Prec::Double) {
         if (raw_double)
             k_links_to_raw<double2, double><<<grid, kBlock, 0, L.stream>>>(
-                (double *)raw_dev, (const double2 *)ls.blk[0], (const double2 *)ls.blk[1], slot, vh);
+                (double *)raw_dev, (const double2 *)ls.blk[0], (const double2 *)ls.blk[1], slot, vh, k);
         else
             k_links_to_raw<double2, float><<<grid, kBlock, 0, L.stream>>>(
-                (float *)raw_dev, (const double2 *)ls.blk[0], (const double2 *)ls.blk[1], slot, vh);
+                (float *)raw_dev, (const double2 *)ls.blk[0], (const double2 *)ls.blk[1], slot, vh, k);
     } else if (p == Prec::Single) {
         if (raw_double)
             k_links_to_raw<float2, double><<<grid, kBlock, 0, L.stream>>>(
-                (double *)raw_dev, (const float2 *)ls.blk[0], (const float2 *)ls.blk[1], slot, vh);
+                (double *)raw_dev, (const float2 *)ls.blk[0], (const float2 *)ls.blk[1], slot, vh, k);
         else
             k_links_to_raw<float2, float><<<grid, kBlock, 0, L.stream>>>(
-                (float *)raw_dev, (const float2 *)ls.blk[0], (const float2 *)ls.blk[1], slot, vh);
+                (float *)raw_dev, (const float2 *)ls.blk[0], (const float2 *)ls.blk[1], slot, vh, k);
     }
 }
 
-// max |component| over one family (fat: mats 0-7, Naik: mats 8-15) of both
+// max |component| per family (fat: slots 0,1; Naik: slots 2,3) over both
 // parity blocks, for the 16-bit fixed-point ranges
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
-k_absmax(const S *b0, const S *b1, size_t off, size_t n, unsigned int *out)
+k_absmax(const S *b0, const S *b1, int vh, int k, unsigned int *out)
 {
-    float m = 0.f;
+    float m[2] = {0.f, 0.f};
+    const size_t n = (size_t)4 * 36 * vh;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const S a = b0[off + i], c = b1[off + i];
-        m = fmaxf(m, fmaxf(fmaxf(fabsf((float)a.x), fabsf((float)a.y)), fmaxf(fabsf((float)c.x), fabsf((float)c.y))));
+        const int d = (int)(i / ((size_t)36 * vh));
+        const size_t r = i % ((size_t)36 * vh);
+        const int c = (int)(r / vh);
+        const int j = (int)(r % vh);
+        const size_t at = link_cx_index(k, d, c, j, vh);
+        const S a = b0[at], e = b1[at];
+        const int f = (c / 9) >= 2;
+        m[f] = fmaxf(m[f], fmaxf(fmaxf(fabsf((float)a.x), fabsf((float)a.y)), fmaxf(fabsf((float)e.x), fabsf((float)e.y))));
     }
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));  // m >= 0: uint order = float order
+    for (int f = 0; f < 2; ++f) {
+        float v = m[f];
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(out + f, __float_as_uint(v));  // v >= 0: uint order = float order
+    }
 }
 
 void links_absmax(Prec p, const LinkSet &src, LinkSet &dst, const Launch &L, double *scratch)
 {
     unsigned int *d = reinterpret_cast<unsigned int *>(scratch);
     cudaMemsetAsync(d, 0, 2 * sizeof(unsigned int), L.stream);
-    const size_t n = (size_t)8 * 9 * L.g->vh;
     const int grid = 148 * 8;
-    for (int f = 0; f < 2; ++f) {
-        if (p == Prec::Double)
-            k_absmax<double2><<<grid, kBlock, 0, L.stream>>>((const double2 *)src.blk[0], (const double2 *)src.blk[1], f * n, n, d + f);
-        else
-            k_absmax<float2><<<grid, kBlock, 0, L.stream>>>((const float2 *)src.blk[0], (const float2 *)src.blk[1], f * n, n, d + f);
-    }
+    if (p == Prec::Double)
+        k_absmax<double2><<<grid, kBlock, 0, L.stream>>>((const double2 *)src.blk[0], (const double2 *)src.blk[1], L.g->vh, 1, d);
+    else
+        k_absmax<float2><<<grid, kBlock, 0, L.stream>>>((const float2 *)src.blk[0], (const float2 *)src.blk[1], L.g->vh, 2, d);
     unsigned int h[2] = {0, 0};
     cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, L.stream);
     cudaStreamSynchronize(L.stream);
@@ -205,46 +216,47 @@ void links_absmax(Prec p, const LinkSet &src, LinkSet &dst, const Launch &L, dou
     }
 }
 
+// precision conversion between link blocks (each in its own chunking)
 template <typename D, typename S>
-__global__ void k_links_convert(D *d, const S *s, size_t n, float inv_scale)
+__global__ void k_links_convert(D *dst, int kd, const S *src, int ks, int vh, float inv_fat, float inv_long)
 {
+    const size_t n = (size_t)4 * 36 * vh;
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const S z = s[i];
+    const int d = (int)(i / ((size_t)36 * vh));
+    const size_t r = i % ((size_t)36 * vh);
+    const int c = (int)(r / vh);
+    const int j = (int)(r % vh);
+    const S z = src[link_cx_index(ks, d, c, j, vh)];
+    D q;
     if constexpr (std::is_same<D, short2>::value) {
-        short2 q;
-        q.x = (short)__float2int_rn((float)z.x * inv_scale);
-        q.y = (short)__float2int_rn((float)z.y * inv_scale);
-        d[i] = q;
+        const float inv = (c / 9) >= 2 ? inv_long : inv_fat;
+        q.x = (short)__float2int_rn((float)z.x * inv);
+        q.y = (short)__float2int_rn((float)z.y * inv);
     } else {
-        D q;
         q.x = z.x;
         q.y = z.y;
-        d[i] = q;
     }
+    dst[link_cx_index(kd, d, c, j, vh)] = q;
 }
 
 void links_convert(Prec dst_p, LinkSet &dst, Prec src_p, const LinkSet &src, const Launch &L)
 {
-    const size_t n = (size_t)kMats * 9 * L.g->vh;
+    const int vh = L.g->vh;
+    const size_t n = (size_t)4 * 36 * vh;
     const int grid = (int)((n + kBlock - 1) / kBlock);
-    const size_t nh = n / 2;  // one family (8 matrices)
+    const float inv_fat = dst.link_max[0] > 0 ? 32767.0f / dst.link_max[0] : 0.f;
+    const float inv_long = dst.link_max[1] > 0 ? 32767.0f / dst.link_max[1] : 0.f;
+    const int kd = link_k(dst_p), ks = link_k(src_p);
     for (int cb = 0; cb < 2; ++cb) {
         if (dst_p == Prec::Single && src_p == Prec::Double)
-            k_links_convert<float2, double2><<<grid, kBlock, 0, L.stream>>>((float2 *)dst.blk[cb], (const double2 *)src.blk[cb], n, 0.f);
+            k_links_convert<float2, double2><<<grid, kBlock, 0, L.stream>>>((float2 *)dst.blk[cb], kd, (const double2 *)src.blk[cb], ks, vh, 0.f, 0.f);
         else if (dst_p == Prec::Double && src_p == Prec::Single)
-            k_links_convert<double2, float2><<<grid, kBlock, 0, L.stream>>>((double2 *)dst.blk[cb], (const float2 *)src.blk[cb], n, 0.f);
-        else if (dst_p == Prec::Half) {
-            const int gh = (int)((nh + kBlock - 1) / kBlock);
-            for (int f = 0; f < 2; ++f) {
-                const float inv = dst.link_max[f] > 0 ? 32767.0f / dst.link_max[f] : 0.f;
-                short2 *d = (short2 *)dst.blk[cb] + f * nh;
-                if (src_p == Prec::Double)
-                    k_links_convert<short2, double2><<<gh, kBlock, 0, L.stream>>>(d, (const double2 *)src.blk[cb] + f * nh, nh, inv);
-                else
-                    k_links_convert<short2, float2><<<gh, kBlock, 0, L.stream>>>(d, (const float2 *)src.blk[cb] + f * nh, nh, inv);
-            }
-        }
+            k_links_convert<double2, float2><<<grid, kBlock, 0, L.stream>>>((double2 *)dst.blk[cb], kd, (const float2 *)src.blk[cb], ks, vh, 0.f, 0.f);
+        else if (dst_p == Prec::Half && src_p == Prec::Double)
+            k_links_convert<short2, double2><<<grid, kBlock, 0, L.stream>>>((short2 *)dst.blk[cb], kd, (const double2 *)src.blk[cb], ks, vh, inv_fat, inv_long);
+        else if (dst_p == Prec::Half && src_p == Prec::Single)
+            k_links_convert<short2, float2><<<grid, kBlock, 0, L.stream>>>((short2 *)dst.blk[cb], kd, (const float2 *)src.blk[cb], ks, vh, inv_fat, inv_long);
     }
 }
 

@@ -41,7 +41,7 @@ double norm2_sync(Prec p, VecBlock v)
     const Launch L = c.launch();
     norm2_dev(p, L, v, c.d_state, c.d_partials, c.d_scalars);
     QB_CUDA(cudaMemcpyAsync(c.h_scalars, c.d_scalars, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    QB_CUDA(cudaStreamSynchronize(c.stream));
+    sync_check();
     return c.h_scalars[0];
 }
 
@@ -153,7 +153,7 @@ int cg_reference(Prec P, const LinkSet &ls, SolveArgs &A)
         res->size_relr = 0;
         if (source_norm == 0.0) {
             vec_zero(P, t_dest, L);
-            QB_CUDA(cudaStreamSynchronize(c.stream));
+            sync_check();
             info->final_sec = wall_seconds() - info->final_sec;
             res->final_rel = 0;
             res->final_rsq = 0;
@@ -283,7 +283,7 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
     const double bnorm = norm2_sync(Prec::Double, b);
     if (bnorm == 0.0) {
         vec_zero(Prec::Double, x, L);
-        QB_CUDA(cudaStreamSynchronize(c.stream));
+        sync_check();
         return out;
     }
     Ws ws;
@@ -298,7 +298,7 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
         dslash(Prec::Double, L, ttt64, tmp64, ls64, parity);
         cg_true_residual(Prec::Double, L, ttt64, x, b, r64, c.d_state, c.d_partials, c.d_scalars);
         QB_CUDA(cudaMemcpyAsync(c.h_scalars, c.d_scalars, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-        QB_CUDA(cudaStreamSynchronize(c.stream));
+        sync_check();
         return c.h_scalars[0];
     };
 
@@ -469,7 +469,7 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
     vec_copy(p, resid, p, src, L);
     out.rsq = out.source_norm;
     if (out.source_norm == 0.) {
-        QB_CUDA(cudaStreamSynchronize(c.stream));
+        sync_check();
         return out;
     }
     S.rsqstop = rsqmin * out.source_norm;
@@ -529,7 +529,7 @@ void upload_blocks(VecBlock *d, const std::vector<VecBlock> &h)
 {
     Context &c = ctx();
     QB_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(VecBlock) * h.size(), cudaMemcpyHostToDevice, c.stream));
-    QB_CUDA(cudaStreamSynchronize(c.stream));
+    sync_check();
 }
 
 }  // namespace
