@@ -242,6 +242,7 @@ def run_gpu(args):
     lib.destroy_V("D", vout)
     lib.destroy_V("D", b)
     lib.destroy_L("D", L)
+    tuning = {name: lib.dslash_variant(name) for name in ("single", "double", "half")}
     lib.finalize()
 
     peak, peak_kind = peaks()
@@ -280,7 +281,9 @@ def run_gpu(args):
         "dslash": {"f32_us": ms_f32 * 1e3, "f32_gbs": DSLASH_BYTES_F32 * Vh / (ms_f32 * 1e-3) / 1e9,
                    "f64_us": ms_f64 * 1e3, "f64_gbs": DSLASH_BYTES_F64 * Vh / (ms_f64 * 1e-3) / 1e9,
                    "f32_gflops": DSLASH_FLOPS * Vh / (ms_f32 * 1e-3) / 1e9,
-                   "bytes_per_site": {"f32": DSLASH_BYTES_F32, "f64": DSLASH_BYTES_F64}},
+                   "bytes_per_site": {"f32": DSLASH_BYTES_F32, "f64": DSLASH_BYTES_F64},
+                   "autotuner": {k: {"variant": ["resident-grid", "full-grid", "tma-pipeline"][v] if v >= 0 else None,
+                                     "us": [round(x, 2) for x in us]} for k, (v, us) in tuning.items()}},
         "roofline": {"kernel": "k_dslash<float> (K1) inside the timed solves", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": None,
@@ -384,7 +387,8 @@ def run_profile_dslash(args):
         vout = lib.create_V(prec, np.zeros(V * 6))
         ms = lib.dslash_timed(prec, L, vout, vin, "even", args.reps)
         nbytes = (DSLASH_BYTES_F32 if prec == "F" else DSLASH_BYTES_F64) * (V // 2)
-        out[prec] = {"us": ms * 1e3, "gbs": nbytes / (ms * 1e-3) / 1e9}
+        out[prec] = {"us": ms * 1e3, "gbs": nbytes / (ms * 1e-3) / 1e9,
+                     "variant": lib.dslash_variant("single" if prec == "F" else "double")}
         lib.destroy_V(prec, vin)
         lib.destroy_V(prec, vout)
         lib.destroy_L(prec, L)

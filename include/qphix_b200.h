@@ -69,6 +69,15 @@ QPHIX_status_t QPHIX_B200_D3_dslash_timed(void *links, void *out, void *in,
                                           QPHIX_evenodd_t parity, int reps,
                                           double *ms_per_call);
 
+/* Dslash kernel variant chosen by the library's autotuner for precision p:
+ * 0 register streaming over a resident grid, 1 register streaming with one
+ * thread per site, 2 TMA bulk-copy pipeline.  The first Dslash of each
+ * precision and lattice times all three on scratch vectors and keeps the
+ * fastest; us[3] receives those timings (microseconds per launch).  Returns
+ * -1 before the first Dslash in that precision.  QPHIX_B200_DSLASH=plain|
+ * full|tma in the environment forces a variant. */
+int QPHIX_B200_dslash_variant(QPHIX_B200_precision_t p, double us[3]);
+
 /* Host-side neighbour arithmetic used by the Dslash kernels (no GPU
  * needed): block index, in the opposite parity, of neighbour k of site
  * `site` of parity cb on lattice L[4] = {Nx,Ny,Nz,Nt}.  k follows the

@@ -135,6 +135,8 @@ class QphixLib:
                 f = getattr(L, f"QPHIX_B200_{P}3_dslash_timed")
                 f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                               C.POINTER(C.c_double)]
+            L.QPHIX_B200_dslash_variant.restype = C.c_int
+            L.QPHIX_B200_dslash_variant.argtypes = [C.c_int, C.POINTER(C.c_double)]
             L.QPHIX_B200_neighbor_index.restype = C.c_long
             L.QPHIX_B200_neighbor_index.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_long, C.c_int]
 
@@ -173,6 +175,11 @@ class QphixLib:
         if rc != 0:
             raise RuntimeError("dslash_timed failed: " + self.last_error())
         return ms.value
+
+    def dslash_variant(self, prec_name):
+        us = (C.c_double * 3)()
+        v = self.lib.QPHIX_B200_dslash_variant(PRECISION[prec_name], us)
+        return v, list(us)
 
     def neighbor_index(self, dims, cb, site, k):
         Ld = (C.c_int * 4)(*dims)

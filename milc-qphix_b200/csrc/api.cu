@@ -658,6 +658,16 @@ long QPHIX_B200_neighbor_index(const int L[4], int cb, long site, int k)
     const SiteCoords s = decode(g, cb, (int)site);
     return neighbor(g, s, k);
 }
+int QPHIX_B200_dslash_variant(QPHIX_B200_precision_t p, double us[3])
+{
+    if (p != QPHIX_B200_PREC_HALF && p != QPHIX_B200_PREC_SINGLE && p != QPHIX_B200_PREC_DOUBLE) return -1;
+    float t[3] = {0, 0, 0};
+    const int v = dslash_variant(static_cast<Prec>(p), t);
+    if (us)
+        for (int i = 0; i < 3; ++i) us[i] = t[i];
+    return v;
+}
+
 const char *QPHIX_B200_last_error(void) { return ctx().last_error.c_str(); }
 int QPHIX_B200_version(void) { return 100; }
 

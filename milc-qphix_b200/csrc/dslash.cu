@@ -393,38 +393,114 @@ static int tma_grid(int vh)
     return ntiles < per_sm * sms ? ntiles : per_sm * sms;
 }
 
-// Dslash kernel choice: the TMA pipeline, or the plain register-streaming
-// kernel when QPHIX_B200_DSLASH=plain (kept for comparison measurements).
-static bool use_tma()
+// ---------------------------------------------------------------------------
+// Kernel variants and the autotuner.
+//   0  register streaming, grid of resident blocks striding over the sites
+//   1  register streaming, one thread per site (full grid)
+//   2  TMA bulk-copy pipeline, persistent CTAs
+// The first Dslash of each (precision, volume) times every variant on scratch
+// vectors with the caller's links and keeps the fastest; QPHIX_B200_DSLASH=
+// plain|full|tma forces one.  The fused M^dag M kernel follows the choice.
+// ---------------------------------------------------------------------------
+constexpr int kVariants = 3;
+
+static int forced_variant()
 {
-    static int v = -1;
-    if (v < 0) {
+    static int v = -2;
+    if (v == -2) {
         const char *e = std::getenv("QPHIX_B200_DSLASH");
-        v = (e && !std::strcmp(e, "plain")) ? 0 : 1;
+        v = -1;
+        if (e && !std::strcmp(e, "plain")) v = 0;
+        if (e && !std::strcmp(e, "full")) v = 1;
+        if (e && !std::strcmp(e, "tma")) v = 2;
     }
-    return v == 1;
+    return v;
 }
 
+struct TuneEntry {
+    int vh = -1;
+    int variant = 0;
+    float us[kVariants] = {0, 0, 0};
+};
+static TuneEntry g_tune[3];  // per Prec
+
 template <typename S>
-static void launch_dslash(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb,
-                          const SolverState *st, int gate)
+static void launch_variant(int variant, const DslashArgs<S> &a, const LinkSet &ls, int cb, const Launch &L,
+                           const SolverState *st, int gate)
 {
-    auto a = make_args<S>(L, out, in, ls, cb);
-    if (use_tma()) {
+    if (variant == 2) {
         k_dslash_tma<S, 0><<<tma_grid<S, 0>(L.g->vh), TmaCfg<S>::T, tma_smem_bytes<S>(), L.stream>>>(
             a, static_cast<const char *>(ls.blk[cb]), a.out, 0.0, const_cast<SolverState *>(st), nullptr, gate, 0,
             L.err);
+    } else if (variant == 1) {
+        k_dslash<S><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, st, gate);
     } else {
         k_dslash<S><<<resident_grid(k_dslash<S>, L.g->vh), kBlock, 0, L.stream>>>(a, st, gate);
     }
 }
 
+template <typename S>
+static int tuned_variant(Prec p, const Launch &L, const DslashArgs<S> &a, const LinkSet &ls, int cb)
+{
+    const int f = forced_variant();
+    if (f >= 0) return f;
+    TuneEntry &t = g_tune[(int)p];
+    if (t.vh == L.g->vh) return t.variant;
+    // scratch vectors: the caller's output may alias nothing we may clobber twice
+    const size_t cx = p == Prec::Double ? 16 : (p == Prec::Single ? 8 : 4);
+    void *vin = nullptr, *vout = nullptr;
+    float *nin = nullptr, *nout = nullptr;
+    cudaMallocAsync(&vin, 3 * cx * L.g->vh, L.stream);
+    cudaMallocAsync(&vout, 3 * cx * L.g->vh, L.stream);
+    cudaMemsetAsync(vin, 0, 3 * cx * L.g->vh, L.stream);
+    if (p == Prec::Half) {
+        cudaMallocAsync(&nin, sizeof(float) * L.g->vh, L.stream);
+        cudaMallocAsync(&nout, sizeof(float) * L.g->vh, L.stream);
+        cudaMemsetAsync(nin, 0, sizeof(float) * L.g->vh, L.stream);
+    }
+    DslashArgs<S> s = a;
+    s.in = view<S>(VecBlock{vin, nin}, L.g->vh);
+    s.out = view<S>(VecBlock{vout, nout}, L.g->vh);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = 0;
+    for (int v = 0; v < kVariants; ++v) {
+        launch_variant<S>(v, s, ls, cb, L, nullptr, -1);  // warm
+        cudaEventRecord(e0, L.stream);
+        for (int r = 0; r < 3; ++r) launch_variant<S>(v, s, ls, cb, L, nullptr, -1);
+        cudaEventRecord(e1, L.stream);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        t.us[v] = ms * 1e3f / 3;
+        if (t.us[v] < t.us[best]) best = v;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeAsync(vin, L.stream);
+    cudaFreeAsync(vout, L.stream);
+    if (nin) cudaFreeAsync(nin, L.stream);
+    if (nout) cudaFreeAsync(nout, L.stream);
+    t.vh = L.g->vh;
+    t.variant = best;
+    return best;
+}
+
+template <typename S>
+static void launch_dslash(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb,
+                          const SolverState *st, int gate, Prec p)
+{
+    auto a = make_args<S>(L, out, in, ls, cb);
+    launch_variant<S>(tuned_variant<S>(p, L, a, ls, cb), a, ls, cb, L, st, gate);
+}
+
 void dslash(Prec p, const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb)
 {
     switch (p) {
-    case Prec::Double: launch_dslash<double>(L, out, in, ls, cb, nullptr, -1); break;
-    case Prec::Single: launch_dslash<float>(L, out, in, ls, cb, nullptr, -1); break;
-    case Prec::Half: launch_dslash<__half>(L, out, in, ls, cb, nullptr, -1); break;
+    case Prec::Double: launch_dslash<double>(L, out, in, ls, cb, nullptr, -1, p); break;
+    case Prec::Single: launch_dslash<float>(L, out, in, ls, cb, nullptr, -1, p); break;
+    case Prec::Half: launch_dslash<__half>(L, out, in, ls, cb, nullptr, -1, p); break;
     }
 }
 
@@ -432,19 +508,31 @@ void dslash_gated(Prec p, const Launch &L, VecBlock out, VecBlock in, const Link
                   SolverState *st, int gate)
 {
     switch (p) {
-    case Prec::Double: launch_dslash<double>(L, out, in, ls, cb, st, gate); break;
-    case Prec::Single: launch_dslash<float>(L, out, in, ls, cb, st, gate); break;
-    case Prec::Half: launch_dslash<__half>(L, out, in, ls, cb, st, gate); break;
+    case Prec::Double: launch_dslash<double>(L, out, in, ls, cb, st, gate, p); break;
+    case Prec::Single: launch_dslash<float>(L, out, in, ls, cb, st, gate, p); break;
+    case Prec::Half: launch_dslash<__half>(L, out, in, ls, cb, st, gate, p); break;
     }
+}
+
+int dslash_variant(Prec p, float us[3])
+{
+    const TuneEntry &t = g_tune[(int)p];
+    for (int v = 0; v < kVariants; ++v) us[v] = t.us[v];
+    if (forced_variant() >= 0) return forced_variant();
+    return t.vh < 0 ? -1 : t.variant;
 }
 
 template <typename S>
 static void launch_mdagm(const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls,
                          VecBlock pv, double m4, int cb, SolverState *st, double *partials,
-                         int gate, int mode)
+                         int gate, int mode, Prec p)
 {
     auto a = make_args<S>(L, ttt, tmp, ls, cb);
-    if (use_tma()) {
+    const int variant = tuned_variant<S>(p, L, a, ls, cb);
+    if (variant == 1) {
+        k_dslash_mdagm<S><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, view<S>(pv, L.g->vh), m4, st, partials,
+                                                                       gate, mode);
+    } else if (variant == 2) {
         k_dslash_tma<S, 1><<<tma_grid<S, 1>(L.g->vh), TmaCfg<S>::T, tma_smem_bytes<S>(), L.stream>>>(
             a, static_cast<const char *>(ls.blk[cb]), view<S>(pv, L.g->vh), m4, st, partials, gate, mode, L.err);
     } else {
@@ -458,9 +546,9 @@ void dslash_mdagm_dot(Prec p, const Launch &L, VecBlock ttt, VecBlock tmp, const
                       int mode)
 {
     switch (p) {
-    case Prec::Double: launch_mdagm<double>(L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode); break;
-    case Prec::Single: launch_mdagm<float>(L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode); break;
-    case Prec::Half: launch_mdagm<__half>(L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode); break;
+    case Prec::Double: launch_mdagm<double>(L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode, p); break;
+    case Prec::Single: launch_mdagm<float>(L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode, p); break;
+    case Prec::Half: launch_mdagm<__half>(L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode, p); break;
     }
 }
 

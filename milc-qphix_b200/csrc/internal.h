@@ -131,6 +131,9 @@ void dslash_mdagm_dot(Prec p, const Launch &L, VecBlock ttt, VecBlock tmp, const
 void dslash_gated(Prec p, const Launch &L, VecBlock out, VecBlock in, const LinkSet &links,
                   int cb, SolverState *st, int gate);
 
+// variant chosen by the Dslash autotuner for precision p; us = its timings
+int dslash_variant(Prec p, float us[3]);
+
 // BLAS (blas.cu) ---------------------------------------------------------------
 // state->source_norm = |v|^2
 void norm2_to_state(Prec p, const Launch &L, VecBlock v, SolverState *st, double *partials,
