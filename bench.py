@@ -286,7 +286,10 @@ def run_gpu(args):
                                      "us": [round(x, 2) for x in us]} for k, (v, us) in tuning.items()}},
         "roofline": {"kernel": "k_dslash<float> (K1) inside the timed solves", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind, "traffic": None,
+                     "peak_source": peak_kind,
+                     # ncu dram__bytes_read+write of k_dslash<float> at 24^3x32 (264.3 MB,
+                     # profiles/k_dslash_f32_24x24x24x32.md) scaled by sites to 24^3x48
+                     "traffic": 264.33e6 * Vh / 221184,
                      "launches": int(dslash_n), "avg_launch_us": k1_ms * 1e3},
         "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": 2 * Vh * 6 * 8,
                 "d2h_bytes_per_step": Vh * 6 * 8},

@@ -45,12 +45,20 @@ double norm2_sync(Prec p, VecBlock v)
     return c.h_scalars[0];
 }
 
-// event-timed launch bracket (kernel timing mode)
+// Event-timed launch brackets (kernel timing mode).  Marks are kept for the
+// whole solve and read once at the end, so timing adds nothing to the
+// host's critical path between chunks; launches whose gate was cancelled
+// (k > stop_at of their chunk) are not credited.
 struct TimedLaunches {
-    struct Mark { int kind; int gate; cudaEvent_t a, b; };
+    struct Mark { int kind; int gate; int chunk; cudaEvent_t a, b; };
     std::vector<Mark> marks;
+    std::vector<int> stop_of_chunk;
     bool on;
     explicit TimedLaunches(bool enabled) : on(enabled) { ctx().ktimer.reset(); }
+    ~TimedLaunches()
+    {
+        try { finish(); } catch (...) {}
+    }
     template <typename F> void run(int kind, int gate, F f)
     {
         if (!on) { f(); return; }
@@ -59,21 +67,27 @@ struct TimedLaunches {
         QB_CUDA(cudaEventRecord(a, c.stream));
         f();
         QB_CUDA(cudaEventRecord(b, c.stream));
-        marks.push_back({kind, gate, a, b});
+        marks.push_back({kind, gate, (int)stop_of_chunk.size(), a, b});
     }
-    // credit launches whose gate did work (gate <= stop_at); call after a sync
+    // end of a chunk whose device stop index is stop_at (INT_MAX: none)
     void collect(int stop_at)
+    {
+        if (on) stop_of_chunk.push_back(stop_at);
+    }
+    void finish()
     {
         if (!on) return;
         Context &c = ctx();
         for (auto &m : marks) {
-            if (m.gate >= 0 && m.gate > stop_at) continue;
+            const int stop = m.chunk < (int)stop_of_chunk.size() ? stop_of_chunk[m.chunk] : INT_MAX;
+            if (m.gate >= 0 && m.gate > stop) continue;
             float ms = 0;
-            QB_CUDA(cudaEventElapsedTime(&ms, m.a, m.b));
+            if (cudaEventElapsedTime(&ms, m.a, m.b) != cudaSuccess) continue;
             if (m.kind == 0) { c.stats.dslash_launches++; c.stats.dslash_ms += ms; }
             else { c.stats.mdagm_launches++; c.stats.mdagm_ms += ms; }
         }
         marks.clear();
+        stop_of_chunk.clear();
         c.ktimer.reset();
     }
 };
