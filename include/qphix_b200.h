@@ -9,6 +9,7 @@
 #define _QPHIX_B200_H
 
 #include <qphix_int.h>
+#include <qphix_d3.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -77,6 +78,22 @@ QPHIX_status_t QPHIX_B200_D3_dslash_timed(void *links, void *out, void *in,
  * -1 before the first Dslash in that precision.  QPHIX_B200_DSLASH=plain|
  * full|tma in the environment forces a variant. */
 int QPHIX_B200_dslash_variant(QPHIX_B200_precision_t p, double us[3]);
+
+/* Allocation-free application of the CG operator (no counterpart in the
+ * reference).  For callers that cannot allocate GPU memory at the point of
+ * use -- a memory budget reserved up front, another framework's allocator
+ * in charge, or no room for the synchronisation an allocation may cost.
+ *   out[parity] = D D in[parity] - 4 mass^2 in[parity]   (= -(4m^2 - D D) in,
+ *   the vector the reference CG forms in calc_pkp), *in_dot_out = in . out
+ * Its scratch (the intermediate D in, reduction partials) is a fixed array
+ * inside the library: at most 262144 sites per parity (larger lattices get
+ * QPHIX_FAIL), about 12.6 MB held on every GPU that loads the library until
+ * the process exits.  All calls share that array, so calls that overlap on
+ * the GPU race.  The first call on each device looks the array up; make it
+ * before any stream capture.  The call allocates nothing. */
+QPHIX_status_t QPHIX_B200_D3_asqtad_mdagm_noalloc(QPHIX_D3_FermionLinksAsqtad *L, QPHIX_D3_ColorVector *out,
+                                                 QPHIX_D3_ColorVector *in, QPHIX_D_Real mass,
+                                                 QPHIX_evenodd_t parity, double *in_dot_out);
 
 /* Host-side neighbour arithmetic used by the Dslash kernels (no GPU
  * needed): block index, in the opposite parity, of neighbour k of site

@@ -135,6 +135,9 @@ class QphixLib:
                 f = getattr(L, f"QPHIX_B200_{P}3_dslash_timed")
                 f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                               C.POINTER(C.c_double)]
+            L.QPHIX_B200_D3_asqtad_mdagm_noalloc.restype = C.c_int
+            L.QPHIX_B200_D3_asqtad_mdagm_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                                             C.c_int, C.POINTER(C.c_double)]
             L.QPHIX_B200_dslash_variant.restype = C.c_int
             L.QPHIX_B200_dslash_variant.argtypes = [C.c_int, C.POINTER(C.c_double)]
             L.QPHIX_B200_neighbor_index.restype = C.c_long
@@ -175,6 +178,12 @@ class QphixLib:
         if rc != 0:
             raise RuntimeError("dslash_timed failed: " + self.last_error())
         return ms.value
+
+    def mdagm_noalloc(self, L, out, inp, mass, parity):
+        """QPHIX_B200_D3_asqtad_mdagm_noalloc: (status, in . out)."""
+        dot = C.c_double()
+        rc = self.lib.QPHIX_B200_D3_asqtad_mdagm_noalloc(L, out, inp, mass, PARITY[parity], C.byref(dot))
+        return rc, dot.value
 
     def dslash_variant(self, prec_name):
         us = (C.c_double * 3)()

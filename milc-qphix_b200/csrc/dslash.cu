@@ -552,4 +552,21 @@ void dslash_mdagm_dot(Prec p, const Launch &L, VecBlock ttt, VecBlock tmp, const
     }
 }
 
+// FP64 Dslash and fused M^dag M launches with a fixed kernel variant (one
+// thread per site): no autotuning, hence no scratch allocation.  Used by the
+// allocation-free entry point.
+void dslash_fixed_d(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb)
+{
+    auto a = make_args<double>(L, out, in, ls, cb);
+    k_dslash<double><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, nullptr, -1);
+}
+
+void dslash_mdagm_fixed_d(const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls, VecBlock pv, double m4,
+                          int cb, SolverState *st, double *partials)
+{
+    auto a = make_args<double>(L, ttt, tmp, ls, cb);
+    k_dslash_mdagm<double><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, view<double>(pv, L.g->vh), m4, st,
+                                                                        partials, -1, 0);
+}
+
 }  // namespace qb

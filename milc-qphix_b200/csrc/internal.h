@@ -131,6 +131,13 @@ void dslash_mdagm_dot(Prec p, const Launch &L, VecBlock ttt, VecBlock tmp, const
 void dslash_gated(Prec p, const Launch &L, VecBlock out, VecBlock in, const LinkSet &links,
                   int cb, SolverState *st, int gate);
 
+// FP64 launches with a fixed variant and caller-provided scratch (no tuning,
+// no allocation): out[cb] = D in[1-cb]; ttt[cb] = D tmp[1-cb] + m4 pv, p.ttt
+// reduced into st->pkp through `partials`
+void dslash_fixed_d(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb);
+void dslash_mdagm_fixed_d(const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls, VecBlock pv, double m4,
+                          int cb, SolverState *st, double *partials);
+
 // variant chosen by the Dslash autotuner for precision p; us = its timings
 int dslash_variant(Prec p, float us[3]);
 
