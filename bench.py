@@ -174,12 +174,10 @@ def run_gpu(args):
         x, _, _, _ = solve("single")
         lib.destroy_V("D", x)
 
-    lib.set_kernel_timing(True)
     clocks = ClockSampler(local)
     barrier(pg)
     clocks.start()
     times, iters, rus, trues = [], [], [], []
-    dslash_ms = dslash_n = mdagm_ms = mdagm_n = 0.0
     xs_last = None
     for k in range(args.steps):
         x, ms, res, st = solve("single")
@@ -187,17 +185,25 @@ def run_gpu(args):
         iters.append(st.iterations)
         rus.append(st.reliable_updates)
         trues.append(res.final_rsq)
-        dslash_ms += st.dslash_ms
-        dslash_n += st.dslash_launches
-        mdagm_ms += st.mdagm_ms
-        mdagm_n += st.mdagm_launches
         if k == args.steps - 1:
             xs_last = lib.extract_V("D", x, "even")[: Vh * 6]
         lib.destroy_V("D", x)
     barrier(pg)
     clk = clocks.stop()
-    lib.set_kernel_timing(False)
     ms_step = max_over_ranks(pg, float(np.mean(times)))
+
+    # per-kernel CUDA-event durations from one more solve of the same input
+    # (events around every launch cost host time, so not inside the timed steps)
+    lib.set_kernel_timing(True)
+    x, ms_inst, _, st = solve("single")
+    lib.destroy_V("D", x)
+    lib.set_kernel_timing(False)
+    dslash_ms, dslash_n, mdagm_ms, mdagm_n = st.dslash_ms, st.dslash_launches, st.mdagm_ms, st.mdagm_launches
+
+    # 16-bit links with FP32 vectors (one solve, reported beside)
+    xl, msl, resl, stl = solve("half-links")
+    xsoll = lib.extract_V("D", xl, "even")[: Vh * 6]
+    lib.destroy_V("D", xl)
 
     # 16-bit inner variant (one solve, reported beside)
     xh, msh, resh, sth = solve("half")
@@ -242,7 +248,7 @@ def run_gpu(args):
     lib.destroy_V("D", vout)
     lib.destroy_V("D", b)
     lib.destroy_L("D", L)
-    tuning = {name: lib.dslash_variant(name) for name in ("single", "double", "half")}
+    tuning = {name: lib.dslash_variant(name) for name in ("single", "double", "half", "half-links")}
     lib.finalize()
 
     peak, peak_kind = peaks()
@@ -250,6 +256,7 @@ def run_gpu(args):
     achieved = DSLASH_BYTES_F32 * Vh / (k1_ms * 1e-3) / 1e9
     err_vs_fp64 = float(np.abs(xs_last - xsol64).max() / np.abs(xsol64).max())
     err_half = float(np.abs(xsolh - xsol64).max() / np.abs(xsol64).max())
+    err_hl = float(np.abs(xsoll - xsol64).max() / np.abs(xsol64).max())
     if rank != 0:
         if pg is not None:
             pg.destroy_process_group()
@@ -277,14 +284,20 @@ def run_gpu(args):
         "fp64_cg": {"s": ms64 / 1e3, "iterations": res64.final_iter, "true_rsq_rel": res64.final_rsq,
                     "speedup_mixed_vs_fp64": ms64 / ms_step},
         "half_inner_cg": {"s": msh / 1e3, "iterations": sth.iterations, "reliable_updates": sth.reliable_updates,
-                          "true_rsq_rel": resh.final_rsq, "err_vs_fp64_solution": err_half},
+                          "true_rsq_rel": resh.final_rsq, "err_vs_fp64_solution": err_half,
+                          "escalated_to_fp32": sth.escalated,
+                          "storage": "16-bit fixed-point vectors (per-site norm) and links"},
+        "half_links_cg": {"s": msl / 1e3, "iterations": stl.iterations, "reliable_updates": stl.reliable_updates,
+                          "true_rsq_rel": resl.final_rsq, "err_vs_fp64_solution": err_hl,
+                          "escalated_to_fp32": stl.escalated, "storage": "FP32 vectors, 16-bit fixed-point links"},
         "dslash": {"f32_us": ms_f32 * 1e3, "f32_gbs": DSLASH_BYTES_F32 * Vh / (ms_f32 * 1e-3) / 1e9,
                    "f64_us": ms_f64 * 1e3, "f64_gbs": DSLASH_BYTES_F64 * Vh / (ms_f64 * 1e-3) / 1e9,
                    "f32_gflops": DSLASH_FLOPS * Vh / (ms_f32 * 1e-3) / 1e9,
                    "bytes_per_site": {"f32": DSLASH_BYTES_F32, "f64": DSLASH_BYTES_F64},
                    "autotuner": {k: {"variant": ["resident-grid", "full-grid", "tma-pipeline"][v] if v >= 0 else None,
                                      "us": [round(x, 2) for x in us]} for k, (v, us) in tuning.items()}},
-        "roofline": {"kernel": "k_dslash<float> (K1) inside the timed solves", "bound": "hbm",
+        "roofline": {"kernel": "k_dslash<float> (K1) in a solve of the timed workload (CUDA events per launch)",
+                     "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind,
                      # ncu dram__bytes_read+write of k_dslash<float> at 24^3x32 (264.3 MB,

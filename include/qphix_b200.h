@@ -16,17 +16,22 @@ extern "C" {
 #endif
 
 /* Inner (sloppy) precision of QPHIX_D3_asqtad_invert / _invert_multi.
- * DOUBLE: FP64 throughout with the reference control flow (default).
- * SINGLE: FP32 inner CG with FP64 reliable updates; FP64 solution, FP64
- *         reductions; converges on the FP64 true residual.
- * HALF:   16-bit inner CG (per-site-normalised FP16 vectors, 16-bit fixed
- *         point links, FP32 arithmetic) with FP64 reliable updates.
- * The environment variable QPHIX_GPU_PRECISION=double|single|half sets the
- * initial value at QPHIX_init. */
+ * DOUBLE:     FP64 throughout with the reference control flow (default).
+ * SINGLE:     FP32 inner CG with FP64 reliable updates; FP64 solution, FP64
+ *             reductions; converges on the FP64 true residual.
+ * HALF:       16-bit inner CG: vectors as 16-bit fixed point with a per-site
+ *             norm, 16-bit fixed-point links, FP32 arithmetic; FP64
+ *             reliable updates.
+ * HALF_LINKS: FP32 vectors with 16-bit fixed-point links (half the link
+ *             bytes of SINGLE); FP64 reliable updates.
+ * A 16-bit inner solve that stops reducing the true residual continues
+ * with FP32 links and vectors.  QPHIX_GPU_PRECISION=double|single|half|
+ * half-links sets the initial value at QPHIX_init. */
 typedef enum {
   QPHIX_B200_PREC_HALF = 0,
   QPHIX_B200_PREC_SINGLE = 1,
-  QPHIX_B200_PREC_DOUBLE = 2
+  QPHIX_B200_PREC_DOUBLE = 2,
+  QPHIX_B200_PREC_HALF_LINKS = 3
 } QPHIX_B200_precision_t;
 
 QPHIX_status_t QPHIX_B200_set_inner_precision(QPHIX_B200_precision_t p);
@@ -70,7 +75,8 @@ QPHIX_status_t QPHIX_B200_D3_dslash_timed(void *links, void *out, void *in,
                                           QPHIX_evenodd_t parity, int reps,
                                           double *ms_per_call);
 
-/* Dslash kernel variant chosen by the library's autotuner for precision p:
+/* Dslash kernel variant chosen by the library's autotuner for precision p
+ * (HALF_LINKS: FP32 vectors with 16-bit links):
  * 0 register streaming over a resident grid, 1 register streaming with one
  * thread per site, 2 TMA bulk-copy pipeline.  The first Dslash of each
  * precision and lattice times all three on scratch vectors and keeps the

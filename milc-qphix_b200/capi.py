@@ -83,7 +83,7 @@ class Stats(C.Structure):
                 ("mdagm_ms", C.c_double), ("true_rsq", C.c_double), ("escalated", C.c_int)]
 
 
-PRECISION = {"half": 0, "single": 1, "double": 2}
+PRECISION = {"half": 0, "single": 1, "double": 2, "half-links": 3}
 
 
 class QphixLib:

@@ -38,13 +38,14 @@ void require_init()
     if (!ctx().initialized) throw Error("QPhiX library used before QPHIX_init");
 }
 
-Prec env_precision(Prec dflt)
+int env_precision(int dflt)
 {
     const char *e = std::getenv("QPHIX_GPU_PRECISION");
     if (!e) return dflt;
-    if (!strcmp(e, "double") || !strcmp(e, "fp64")) return Prec::Double;
-    if (!strcmp(e, "single") || !strcmp(e, "fp32") || !strcmp(e, "mixed")) return Prec::Single;
-    if (!strcmp(e, "half") || !strcmp(e, "fp16")) return Prec::Half;
+    if (!strcmp(e, "double") || !strcmp(e, "fp64")) return QPHIX_B200_PREC_DOUBLE;
+    if (!strcmp(e, "single") || !strcmp(e, "fp32") || !strcmp(e, "mixed")) return QPHIX_B200_PREC_SINGLE;
+    if (!strcmp(e, "half") || !strcmp(e, "fp16")) return QPHIX_B200_PREC_HALF;
+    if (!strcmp(e, "half-links")) return QPHIX_B200_PREC_HALF_LINKS;
     return dflt;
 }
 
@@ -99,7 +100,7 @@ void init_context(QPHIX_layout_t *layout)
         QB_CUDA(cudaEventCreate(&c.ev_solve[i]));
         QB_CUDA(cudaEventCreate(&c.ev_user[i]));
     }
-    c.inner = env_precision(Prec::Double);
+    c.inner_mode = env_precision(QPHIX_B200_PREC_DOUBLE);
     c.verbose = std::getenv("QPHIX_B200_VERBOSE") ? std::atoi(std::getenv("QPHIX_B200_VERBOSE")) : 0;
     c.initialized = true;
 }
@@ -317,7 +318,7 @@ QPHIX_status_t asqtad_dslash(typename Api<Real>::FL *H, typename Api<Real>::CV *
     });
 }
 
-// FP32 copy of a D3 link set, made on first use
+// FP32 and 16-bit copies of a D3 link set, made on first use
 const LinkSet &single_links(QPHIX_D3_FermionLinksAsqtad *H)
 {
     if (!H->sloppy_single.valid) {
@@ -325,6 +326,34 @@ const LinkSet &single_links(QPHIX_D3_FermionLinksAsqtad *H)
         links_convert(Prec::Single, H->sloppy_single, Prec::Double, H->links, ctx().launch());
     }
     return H->sloppy_single;
+}
+
+const LinkSet &half_links(QPHIX_D3_FermionLinksAsqtad *H)
+{
+    if (!H->sloppy_half.valid) {
+        H->sloppy_half = alloc_links(Prec::Half);
+        links_absmax(Prec::Double, H->links, H->sloppy_half, ctx().launch(), ctx().d_partials);
+        links_convert(Prec::Half, H->sloppy_half, Prec::Double, H->links, ctx().launch());
+    }
+    return H->sloppy_half;
+}
+
+// inner solve of a mixed-precision D3 call: vector precision, link set, and
+// the FP32 links a stalled 16-bit solve continues with
+struct SloppyCfg {
+    Prec vec;
+    const LinkSet *links;
+    const LinkSet *up;
+};
+
+SloppyCfg sloppy_cfg(QPHIX_D3_FermionLinksAsqtad *H, int mode)
+{
+    switch (mode) {
+    case QPHIX_B200_PREC_SINGLE: return {Prec::Single, &single_links(H), nullptr};
+    case QPHIX_B200_PREC_HALF: return {Prec::Half, &half_links(H), &single_links(H)};
+    case QPHIX_B200_PREC_HALF_LINKS: return {Prec::Single, &half_links(H), &single_links(H)};
+    default: throw Error("unknown inner precision");
+    }
 }
 
 template <typename Real>
@@ -343,35 +372,15 @@ int asqtad_invert(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_invert_ar
         c.stats = Stats();
         SolveArgs a{info, inv, res, (double)mass, {out->blk[0], out->blk[1]}, {in->blk[0], in->blk[1]}};
         QB_CUDA(cudaEventRecord(c.ev_solve[0], c.stream));
-        Prec inner = Api<Real>::prec;
-        if constexpr (std::is_same<Real, double>::value) inner = c.inner;
-        if (inner == Api<Real>::prec) {
-            iters = cg_reference(Api<Real>::prec, H->links, a);
-        } else {
-            const LinkSet &lss = [&]() -> const LinkSet & {
-                if constexpr (std::is_same<Real, double>::value) {
-                    if (inner == Prec::Single) {
-                        if (!H->sloppy_single.valid) {
-                            H->sloppy_single = alloc_links(Prec::Single);
-                            links_convert(Prec::Single, H->sloppy_single, Prec::Double, H->links, c.launch());
-                        }
-                        return H->sloppy_single;
-                    }
-                }
-                if (!H->sloppy_half.valid) {
-                    H->sloppy_half = alloc_links(Prec::Half);
-                    links_absmax(Api<Real>::prec, H->links, H->sloppy_half, c.launch(), c.d_partials);
-                    links_convert(Prec::Half, H->sloppy_half, Api<Real>::prec, H->links, c.launch());
-                }
-                return H->sloppy_half;
-            }();
-            if constexpr (std::is_same<Real, double>::value) {
-                const LinkSet *up = nullptr;
-                if (inner == Prec::Half) up = &single_links(H);
-                iters = cg_mixed(inner, H->links, lss, up, a);
+        if constexpr (std::is_same<Real, double>::value) {
+            if (c.inner_mode == QPHIX_B200_PREC_DOUBLE) {
+                iters = cg_reference(Prec::Double, H->links, a);
             } else {
-                throw Error("asqtad_invert: mixed precision is available through the D3 API");
+                const SloppyCfg s = sloppy_cfg(H, c.inner_mode);
+                iters = cg_mixed(s.vec, H->links, *s.links, s.up, a);
             }
+        } else {
+            iters = cg_reference(Prec::Single, H->links, a);
         }
         QB_CUDA(cudaEventRecord(c.ev_solve[1], c.stream));
         QB_CUDA(cudaEventSynchronize(c.ev_solve[1]));
@@ -415,30 +424,15 @@ int asqtad_invert_multi(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_inv
         a.in[0] = in->blk[0];
         a.in[1] = in->blk[1];
         QB_CUDA(cudaEventRecord(c.ev_solve[0], c.stream));
-        Prec inner = Api<Real>::prec;
-        if constexpr (std::is_same<Real, double>::value) inner = c.inner;
-        if (inner == Api<Real>::prec) {
-            iters = multishift_reference(Api<Real>::prec, H->links, a);
-        } else if constexpr (std::is_same<Real, double>::value) {
-            LinkSet *lss;
-            if (inner == Prec::Single) {
-                if (!H->sloppy_single.valid) {
-                    H->sloppy_single = alloc_links(Prec::Single);
-                    links_convert(Prec::Single, H->sloppy_single, Prec::Double, H->links, c.launch());
-                }
-                lss = &H->sloppy_single;
+        if constexpr (std::is_same<Real, double>::value) {
+            if (c.inner_mode == QPHIX_B200_PREC_DOUBLE) {
+                iters = multishift_reference(Prec::Double, H->links, a);
             } else {
-                if (!H->sloppy_half.valid) {
-                    H->sloppy_half = alloc_links(Prec::Half);
-                    links_absmax(Prec::Double, H->links, H->sloppy_half, c.launch(), c.d_partials);
-                    links_convert(Prec::Half, H->sloppy_half, Prec::Double, H->links, c.launch());
-                }
-                lss = &H->sloppy_half;
+                const SloppyCfg s = sloppy_cfg(H, c.inner_mode);
+                iters = multishift_mixed(s.vec, H->links, *s.links, s.up, a);
             }
-            const LinkSet *up = inner == Prec::Half ? &single_links(H) : nullptr;
-            iters = multishift_mixed(inner, H->links, *lss, up, a);
         } else {
-            throw Error("asqtad_invert_multi: mixed precision is available through the D3 API");
+            iters = multishift_reference(Prec::Single, H->links, a);
         }
         QB_CUDA(cudaEventRecord(c.ev_solve[1], c.stream));
         QB_CUDA(cudaEventSynchronize(c.ev_solve[1]));
@@ -592,12 +586,13 @@ void QPHIX_D3_symanzik_1loop_gauge_force(QPHIX_info_t *info, QPHIX_D3_GaugeField
 QPHIX_status_t QPHIX_B200_set_inner_precision(QPHIX_B200_precision_t p)
 {
     return guarded([&] {
-        if (p != QPHIX_B200_PREC_HALF && p != QPHIX_B200_PREC_SINGLE && p != QPHIX_B200_PREC_DOUBLE)
+        if (p != QPHIX_B200_PREC_HALF && p != QPHIX_B200_PREC_SINGLE && p != QPHIX_B200_PREC_DOUBLE &&
+            p != QPHIX_B200_PREC_HALF_LINKS)
             throw Error("set_inner_precision: unknown precision");
-        ctx().inner = static_cast<Prec>(p);
+        ctx().inner_mode = p;
     });
 }
-QPHIX_B200_precision_t QPHIX_B200_get_inner_precision(void) { return static_cast<QPHIX_B200_precision_t>(ctx().inner); }
+QPHIX_B200_precision_t QPHIX_B200_get_inner_precision(void) { return static_cast<QPHIX_B200_precision_t>(ctx().inner_mode); }
 QPHIX_status_t QPHIX_B200_set_reliable_delta(double delta)
 {
     return guarded([&] {
@@ -660,9 +655,16 @@ long QPHIX_B200_neighbor_index(const int L[4], int cb, long site, int k)
 }
 int QPHIX_B200_dslash_variant(QPHIX_B200_precision_t p, double us[3])
 {
-    if (p != QPHIX_B200_PREC_HALF && p != QPHIX_B200_PREC_SINGLE && p != QPHIX_B200_PREC_DOUBLE) return -1;
+    Prec pv, pl;
+    switch (p) {
+    case QPHIX_B200_PREC_HALF: pv = pl = Prec::Half; break;
+    case QPHIX_B200_PREC_SINGLE: pv = pl = Prec::Single; break;
+    case QPHIX_B200_PREC_DOUBLE: pv = pl = Prec::Double; break;
+    case QPHIX_B200_PREC_HALF_LINKS: pv = Prec::Single; pl = Prec::Half; break;
+    default: return -1;
+    }
     float t[3] = {0, 0, 0};
-    const int v = dslash_variant(static_cast<Prec>(p), t);
+    const int v = dslash_variant(pv, pl, t);
     if (us)
         for (int i = 0; i < 3; ++i) us[i] = t[i];
     return v;

@@ -61,6 +61,7 @@ LinkSet alloc_links(Prec p)
         ls.blk[cb] = dev_alloc(bytes);
         QB_CUDA(cudaMemsetAsync(ls.blk[cb], 0, bytes, c.stream));
     }
+    ls.prec = p;
     ls.valid = true;
     return ls;
 }

@@ -16,29 +16,32 @@
 // memory bound on HBM.
 #include <cstdlib>
 #include <cstring>
+#include <stdexcept>
 
 #include "device_common.cuh"
 
 namespace qb {
 
-template <typename S>
+// SV: storage type of the colour vectors, SL: storage type of the links
+// (double, float or the 16-bit formats tagged __half)
+template <typename SV, typename SL>
 struct DslashArgs {
-    VecView<S> out;
-    VecView<S> in;
-    LinkView<S> links;
+    VecView<SV> out;
+    VecView<SV> in;
+    LinkView<SL> links;
     Geom g;
     int cb;
 };
 
 // Neighbour k of output site s: one hop 2*d (backward) / 2*d+1 (forward),
 // three hops 8+2*d / 9+2*d (the reference's NeighTable order).
-template <typename S, typename A>
-__device__ __forceinline__ void dslash_site(const DslashArgs<S> &a, int j, A acc[6])
+template <typename SV, typename SL, typename A>
+__device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, A acc[6])
 {
     const SiteCoords s = decode(a.g, a.cb, j);
 #pragma unroll
     for (int i = 0; i < 6; ++i) acc[i] = A(0);
-    if constexpr (std::is_same<S, double>::value) {
+    if constexpr (std::is_same<SL, double>::value) {
         // FP64: one matrix and its neighbour per batch (192 bytes in flight)
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
@@ -52,7 +55,7 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<S> &a, int j, A acc
                 else mv_add(acc, u, v);
             }
         }
-    } else if constexpr (std::is_same<S, float>::value) {
+    } else if constexpr (std::is_same<SL, float>::value) {
         // FP32: forward/backward pair, 9 float4 + 2 neighbours per batch
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
@@ -133,31 +136,31 @@ __device__ __forceinline__ void mdagm_finalize(SolverState *st, double pkp, int 
     }
 }
 
-template <typename S>
-__global__ void __launch_bounds__(kBlock) k_dslash(DslashArgs<S> a, const SolverState *st, int gate)
+template <typename SV, typename SL>
+__global__ void __launch_bounds__(kBlock) k_dslash(DslashArgs<SV, SL> a, const SolverState *st, int gate)
 {
-    using A = typename Acc<S>::type;
+    using A = typename Acc<SV>::type;
     if (st && gated_off(st, gate)) return;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.g.vh; j += gridDim.x * blockDim.x) {
         A acc[6];
-        dslash_site<S, A>(a, j, acc);
+        dslash_site<SV, SL, A>(a, j, acc);
         a.out.store(j, acc);
     }
 }
 
 // ttt = D tmp + m4 * p ;  pkp = sum p . ttt  (calc_pkp, ks_d_congrad_fn.cpp:159-171;
 // ks_multicg_offset.cpp:107-122), then the scalar step of the solver.
-template <typename S>
+template <typename SV, typename SL>
 __global__ void __launch_bounds__(kBlock)
-k_dslash_mdagm(DslashArgs<S> a, VecView<S> pv, double m4, SolverState *st, double *partials,
+k_dslash_mdagm(DslashArgs<SV, SL> a, VecView<SV> pv, double m4, SolverState *st, double *partials,
                int gate, int mode)
 {
-    using A = typename Acc<S>::type;
+    using A = typename Acc<SV>::type;
     if (gated_off(st, gate)) return;
     double dot[1] = {0.0};
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.g.vh; j += gridDim.x * blockDim.x) {
         A acc[6], p[6];
-        dslash_site<S, A>(a, j, acc);
+        dslash_site<SV, SL, A>(a, j, acc);
         pv.load_cg(j, p);
         const A m = (A)m4;
 #pragma unroll
@@ -195,16 +198,16 @@ constexpr size_t tma_smem_bytes()
 
 // contribution of direction d from the staged chunks (chunk q of this
 // thread's site at ch[q*T])
-template <typename S, typename A>
-__device__ __forceinline__ void tma_direction(const DslashArgs<S> &a, const SiteCoords &s, int d,
+template <typename SV, typename SL, typename A>
+__device__ __forceinline__ void tma_direction(const DslashArgs<SV, SL> &a, const SiteCoords &s, int d,
                                               const uint4 *ch, A acc[6])
 {
-    constexpr int T = TmaCfg<S>::T;
+    constexpr int T = TmaCfg<SL>::T;
     A v[4][6];
 #pragma unroll
     for (int sl = 0; sl < 4; ++sl)
         a.in.load(neighbor(a.g, s, (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1)), v[sl]);
-    if constexpr (std::is_same<S, double>::value) {
+    if constexpr (std::is_same<SL, double>::value) {
         const double2 *c2 = reinterpret_cast<const double2 *>(ch);
 #pragma unroll
         for (int sl = 0; sl < 4; ++sl) {
@@ -217,7 +220,7 @@ __device__ __forceinline__ void tma_direction(const DslashArgs<S> &a, const Site
             if (sl & 1) mv_adj_sub(acc, u, v[sl]);
             else mv_add(acc, u, v[sl]);
         }
-    } else if constexpr (std::is_same<S, float>::value) {
+    } else if constexpr (std::is_same<SL, float>::value) {
         const float4 *c4 = reinterpret_cast<const float4 *>(ch);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
@@ -247,13 +250,13 @@ __device__ __forceinline__ void tma_direction(const DslashArgs<S> &a, const Site
 
 // MODE 0: out = D in.  MODE 1: out = D in + m4 p, p.out reduced, then the
 // solver's scalar step (mdagm_finalize).
-template <typename S, int MODE>
-__global__ void __launch_bounds__(TmaCfg<S>::T)
-k_dslash_tma(DslashArgs<S> a, const char *links, VecView<S> pv, double m4, SolverState *st, double *partials,
-             int gate, int mode, int *err)
+template <typename SV, typename SL, int MODE>
+__global__ void __launch_bounds__(TmaCfg<SL>::T)
+k_dslash_tma(DslashArgs<SV, SL> a, const char *links, VecView<SV> pv, double m4, SolverState *st,
+             double *partials, int gate, int mode, int *err)
 {
-    using A = typename Acc<S>::type;
-    constexpr int C = TmaCfg<S>::C, T = TmaCfg<S>::T, NS = TmaCfg<S>::NS;
+    using A = typename Acc<SV>::type;
+    constexpr int C = TmaCfg<SL>::C, T = TmaCfg<SL>::T, NS = TmaCfg<SL>::NS;
     if (st && gated_off(st, gate)) return;
     extern __shared__ __align__(128) unsigned char smem[];
     uint4 *buf = reinterpret_cast<uint4 *>(smem);
@@ -306,7 +309,7 @@ k_dslash_tma(DslashArgs<S> a, const char *links, VecView<S> pv, double m4, Solve
         if (!mbar_wait_bounded(&bars[b], (uint32_t)((g / NS) & 1))) s_fail = 1;
         if (j < vh) {
             const SiteCoords s = decode(a.g, a.cb, j);
-            tma_direction<S, A>(a, s, d, buf + (size_t)b * C * T + tid, acc);
+            tma_direction<SV, SL, A>(a, s, d, buf + (size_t)b * C * T + tid, acc);
             if (d == 3) {
                 if constexpr (MODE == 0) {
                     a.out.store(j, acc);
@@ -337,16 +340,16 @@ k_dslash_tma(DslashArgs<S> a, const char *links, VecView<S> pv, double m4, Solve
         grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) { mdagm_finalize(st, tot[0], mode); });
 }
 
-template <typename S>
-static DslashArgs<S> make_args(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb)
+template <typename SV, typename SL>
+static DslashArgs<SV, SL> make_args(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb)
 {
-    DslashArgs<S> a;
-    a.out = view<S>(out, L.g->vh);
-    a.in = view<S>(in, L.g->vh);
-    if constexpr (std::is_same<S, __half>::value) {
+    DslashArgs<SV, SL> a;
+    a.out = view<SV>(out, L.g->vh);
+    a.in = view<SV>(in, L.g->vh);
+    if constexpr (std::is_same<SL, __half>::value) {
         a.links = LinkView<__half>{static_cast<const int4 *>(ls.blk[cb]), L.g->vh,
                                    ls.link_max[0] / 32767.0f, ls.link_max[1] / 32767.0f};
-    } else if constexpr (std::is_same<S, float>::value) {
+    } else if constexpr (std::is_same<SL, float>::value) {
         a.links = LinkView<float>{static_cast<const float4 *>(ls.blk[cb]), L.g->vh};
     } else {
         a.links = LinkView<double>{static_cast<const double2 *>(ls.blk[cb]), L.g->vh};
@@ -375,7 +378,7 @@ static int resident_grid(K kernel, int vh)
 }
 
 // grid of the persistent TMA kernel: all CTAs resident
-template <typename S, int MODE>
+template <typename SV, typename SL, int MODE>
 static int tma_grid(int vh)
 {
     static int per_sm = -1, sms = 0;
@@ -383,13 +386,13 @@ static int tma_grid(int vh)
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(k_dslash_tma<S, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tma_smem_bytes<S>());
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dslash_tma<S, MODE>, TmaCfg<S>::T,
-                                                          tma_smem_bytes<S>()) != cudaSuccess || per_sm < 1)
+        cudaFuncSetAttribute(k_dslash_tma<SV, SL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tma_smem_bytes<SL>());
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dslash_tma<SV, SL, MODE>, TmaCfg<SL>::T,
+                                                          tma_smem_bytes<SL>()) != cudaSuccess || per_sm < 1)
             per_sm = 1;
     }
-    const int ntiles = (vh + TmaCfg<S>::T - 1) / TmaCfg<S>::T;
+    const int ntiles = (vh + TmaCfg<SL>::T - 1) / TmaCfg<SL>::T;
     return ntiles < per_sm * sms ? ntiles : per_sm * sms;
 }
 
@@ -422,53 +425,53 @@ struct TuneEntry {
     int variant = 0;
     float us[kVariants] = {0, 0, 0};
 };
-static TuneEntry g_tune[3];  // per Prec
+static TuneEntry g_tune[3][3];  // per (vector precision, link precision)
 
-template <typename S>
-static void launch_variant(int variant, const DslashArgs<S> &a, const LinkSet &ls, int cb, const Launch &L,
+template <typename SV, typename SL>
+static void launch_variant(int variant, const DslashArgs<SV, SL> &a, const LinkSet &ls, int cb, const Launch &L,
                            const SolverState *st, int gate)
 {
     if (variant == 2) {
-        k_dslash_tma<S, 0><<<tma_grid<S, 0>(L.g->vh), TmaCfg<S>::T, tma_smem_bytes<S>(), L.stream>>>(
+        k_dslash_tma<SV, SL, 0><<<tma_grid<SV, SL, 0>(L.g->vh), TmaCfg<SL>::T, tma_smem_bytes<SL>(), L.stream>>>(
             a, static_cast<const char *>(ls.blk[cb]), a.out, 0.0, const_cast<SolverState *>(st), nullptr, gate, 0,
             L.err);
     } else if (variant == 1) {
-        k_dslash<S><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, st, gate);
+        k_dslash<SV, SL><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, st, gate);
     } else {
-        k_dslash<S><<<resident_grid(k_dslash<S>, L.g->vh), kBlock, 0, L.stream>>>(a, st, gate);
+        k_dslash<SV, SL><<<resident_grid(k_dslash<SV, SL>, L.g->vh), kBlock, 0, L.stream>>>(a, st, gate);
     }
 }
 
-template <typename S>
-static int tuned_variant(Prec p, const Launch &L, const DslashArgs<S> &a, const LinkSet &ls, int cb)
+template <typename SV, typename SL>
+static int tuned_variant(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV, SL> &a, const LinkSet &ls, int cb)
 {
     const int f = forced_variant();
     if (f >= 0) return f;
-    TuneEntry &t = g_tune[(int)p];
+    TuneEntry &t = g_tune[(int)pv][(int)pl];
     if (t.vh == L.g->vh) return t.variant;
-    // scratch vectors: the caller's output may alias nothing we may clobber twice
-    const size_t cx = p == Prec::Double ? 16 : (p == Prec::Single ? 8 : 4);
+    // time the variants on scratch vectors so no caller data is touched twice
+    const size_t cx = pv == Prec::Double ? 16 : (pv == Prec::Single ? 8 : 4);
     void *vin = nullptr, *vout = nullptr;
     float *nin = nullptr, *nout = nullptr;
     cudaMallocAsync(&vin, 3 * cx * L.g->vh, L.stream);
     cudaMallocAsync(&vout, 3 * cx * L.g->vh, L.stream);
     cudaMemsetAsync(vin, 0, 3 * cx * L.g->vh, L.stream);
-    if (p == Prec::Half) {
+    if (pv == Prec::Half) {
         cudaMallocAsync(&nin, sizeof(float) * L.g->vh, L.stream);
         cudaMallocAsync(&nout, sizeof(float) * L.g->vh, L.stream);
         cudaMemsetAsync(nin, 0, sizeof(float) * L.g->vh, L.stream);
     }
-    DslashArgs<S> s = a;
-    s.in = view<S>(VecBlock{vin, nin}, L.g->vh);
-    s.out = view<S>(VecBlock{vout, nout}, L.g->vh);
+    DslashArgs<SV, SL> s = a;
+    s.in = view<SV>(VecBlock{vin, nin}, L.g->vh);
+    s.out = view<SV>(VecBlock{vout, nout}, L.g->vh);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int best = 0;
     for (int v = 0; v < kVariants; ++v) {
-        launch_variant<S>(v, s, ls, cb, L, nullptr, -1);  // warm
+        launch_variant<SV, SL>(v, s, ls, cb, L, nullptr, -1);  // warm
         cudaEventRecord(e0, L.stream);
-        for (int r = 0; r < 3; ++r) launch_variant<S>(v, s, ls, cb, L, nullptr, -1);
+        for (int r = 0; r < 3; ++r) launch_variant<SV, SL>(v, s, ls, cb, L, nullptr, -1);
         cudaEventRecord(e1, L.stream);
         cudaEventSynchronize(e1);
         float ms = 0;
@@ -487,57 +490,60 @@ static int tuned_variant(Prec p, const Launch &L, const DslashArgs<S> &a, const 
     return best;
 }
 
-template <typename S>
+template <typename SV, typename SL>
 static void launch_dslash(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb,
-                          const SolverState *st, int gate, Prec p)
+                          const SolverState *st, int gate, Prec pv)
 {
-    auto a = make_args<S>(L, out, in, ls, cb);
-    launch_variant<S>(tuned_variant<S>(p, L, a, ls, cb), a, ls, cb, L, st, gate);
+    auto a = make_args<SV, SL>(L, out, in, ls, cb);
+    launch_variant<SV, SL>(tuned_variant<SV, SL>(pv, ls.prec, L, a, ls, cb), a, ls, cb, L, st, gate);
 }
+
+// storage combinations served: vectors and links in the same precision, and
+// FP32 vectors with 16-bit links
+#define QB_DISPATCH_VL(pv, pl, F, ...)                                                           \
+    do {                                                                                        \
+        if ((pv) == Prec::Double && (pl) == Prec::Double) F<double, double>(__VA_ARGS__);       \
+        else if ((pv) == Prec::Single && (pl) == Prec::Single) F<float, float>(__VA_ARGS__);    \
+        else if ((pv) == Prec::Half && (pl) == Prec::Half) F<__half, __half>(__VA_ARGS__);     \
+        else if ((pv) == Prec::Single && (pl) == Prec::Half) F<float, __half>(__VA_ARGS__);     \
+        else throw std::runtime_error("Dslash: unsupported vector/link precision pair");       \
+    } while (0)
 
 void dslash(Prec p, const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb)
 {
-    switch (p) {
-    case Prec::Double: launch_dslash<double>(L, out, in, ls, cb, nullptr, -1, p); break;
-    case Prec::Single: launch_dslash<float>(L, out, in, ls, cb, nullptr, -1, p); break;
-    case Prec::Half: launch_dslash<__half>(L, out, in, ls, cb, nullptr, -1, p); break;
-    }
+    QB_DISPATCH_VL(p, ls.prec, launch_dslash, L, out, in, ls, cb, nullptr, -1, p);
 }
 
 void dslash_gated(Prec p, const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb,
                   SolverState *st, int gate)
 {
-    switch (p) {
-    case Prec::Double: launch_dslash<double>(L, out, in, ls, cb, st, gate, p); break;
-    case Prec::Single: launch_dslash<float>(L, out, in, ls, cb, st, gate, p); break;
-    case Prec::Half: launch_dslash<__half>(L, out, in, ls, cb, st, gate, p); break;
-    }
+    QB_DISPATCH_VL(p, ls.prec, launch_dslash, L, out, in, ls, cb, st, gate, p);
 }
 
-int dslash_variant(Prec p, float us[3])
+int dslash_variant(Prec pv, Prec pl, float us[3])
 {
-    const TuneEntry &t = g_tune[(int)p];
+    const TuneEntry &t = g_tune[(int)pv][(int)pl];
     for (int v = 0; v < kVariants; ++v) us[v] = t.us[v];
     if (forced_variant() >= 0) return forced_variant();
     return t.vh < 0 ? -1 : t.variant;
 }
 
-template <typename S>
+template <typename SV, typename SL>
 static void launch_mdagm(const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls,
                          VecBlock pv, double m4, int cb, SolverState *st, double *partials,
                          int gate, int mode, Prec p)
 {
-    auto a = make_args<S>(L, ttt, tmp, ls, cb);
-    const int variant = tuned_variant<S>(p, L, a, ls, cb);
+    auto a = make_args<SV, SL>(L, ttt, tmp, ls, cb);
+    const int variant = tuned_variant<SV, SL>(p, ls.prec, L, a, ls, cb);
     if (variant == 1) {
-        k_dslash_mdagm<S><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, view<S>(pv, L.g->vh), m4, st, partials,
-                                                                       gate, mode);
+        k_dslash_mdagm<SV, SL><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, view<SV>(pv, L.g->vh), m4, st,
+                                                                            partials, gate, mode);
     } else if (variant == 2) {
-        k_dslash_tma<S, 1><<<tma_grid<S, 1>(L.g->vh), TmaCfg<S>::T, tma_smem_bytes<S>(), L.stream>>>(
-            a, static_cast<const char *>(ls.blk[cb]), view<S>(pv, L.g->vh), m4, st, partials, gate, mode, L.err);
+        k_dslash_tma<SV, SL, 1><<<tma_grid<SV, SL, 1>(L.g->vh), TmaCfg<SL>::T, tma_smem_bytes<SL>(), L.stream>>>(
+            a, static_cast<const char *>(ls.blk[cb]), view<SV>(pv, L.g->vh), m4, st, partials, gate, mode, L.err);
     } else {
-        k_dslash_mdagm<S><<<resident_grid(k_dslash_mdagm<S>, L.g->vh), kBlock, 0, L.stream>>>(
-            a, view<S>(pv, L.g->vh), m4, st, partials, gate, mode);
+        k_dslash_mdagm<SV, SL><<<resident_grid(k_dslash_mdagm<SV, SL>, L.g->vh), kBlock, 0, L.stream>>>(
+            a, view<SV>(pv, L.g->vh), m4, st, partials, gate, mode);
     }
 }
 
@@ -545,11 +551,7 @@ void dslash_mdagm_dot(Prec p, const Launch &L, VecBlock ttt, VecBlock tmp, const
                       VecBlock pv, double m4, int cb, SolverState *st, double *partials, int gate,
                       int mode)
 {
-    switch (p) {
-    case Prec::Double: launch_mdagm<double>(L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode, p); break;
-    case Prec::Single: launch_mdagm<float>(L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode, p); break;
-    case Prec::Half: launch_mdagm<__half>(L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode, p); break;
-    }
+    QB_DISPATCH_VL(p, ls.prec, launch_mdagm, L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode, p);
 }
 
 // FP64 Dslash and fused M^dag M launches with a fixed kernel variant (one
@@ -557,16 +559,16 @@ void dslash_mdagm_dot(Prec p, const Launch &L, VecBlock ttt, VecBlock tmp, const
 // allocation-free entry point.
 void dslash_fixed_d(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb)
 {
-    auto a = make_args<double>(L, out, in, ls, cb);
-    k_dslash<double><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, nullptr, -1);
+    auto a = make_args<double, double>(L, out, in, ls, cb);
+    k_dslash<double, double><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, nullptr, -1);
 }
 
 void dslash_mdagm_fixed_d(const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls, VecBlock pv, double m4,
                           int cb, SolverState *st, double *partials)
 {
-    auto a = make_args<double>(L, ttt, tmp, ls, cb);
-    k_dslash_mdagm<double><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, view<double>(pv, L.g->vh), m4, st,
-                                                                        partials, -1, 0);
+    auto a = make_args<double, double>(L, ttt, tmp, ls, cb);
+    k_dslash_mdagm<double, double><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, view<double>(pv, L.g->vh), m4,
+                                                                                st, partials, -1, 0);
 }
 
 }  // namespace qb

@@ -69,6 +69,7 @@ struct VecBlock {
 struct LinkSet {
     void *blk[2] = {nullptr, nullptr};  // cx_t<R>[16*9*Vh] per parity (half: short2)
     float link_max[2] = {0.f, 0.f};     // half only: fixed-point range of fat / Naik links
+    Prec prec = Prec::Double;           // storage precision of the blocks
     bool valid = false;
 };
 
@@ -139,7 +140,7 @@ void dslash_mdagm_fixed_d(const Launch &L, VecBlock ttt, VecBlock tmp, const Lin
                           int cb, SolverState *st, double *partials);
 
 // variant chosen by the Dslash autotuner for precision p; us = its timings
-int dslash_variant(Prec p, float us[3]);
+int dslash_variant(Prec pv, Prec pl, float us[3]);
 
 // BLAS (blas.cu) ---------------------------------------------------------------
 // state->source_norm = |v|^2

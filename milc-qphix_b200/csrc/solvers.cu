@@ -376,9 +376,9 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
         // the corrections stop reducing the true residual.  Two reliable
         // updates in a row that fail to halve it switch the inner solve to FP32.
         stalled = (rsq > 0.25 * prev_true) ? stalled + 1 : 0;
-        if (stalled >= 2 && ps == Prec::Half && ls_up && ls_up->valid) {
+        if (stalled >= 2 && (ps == Prec::Half || ls_cur->prec == Prec::Half) && ls_up && ls_up->valid) {
             VecBlock p32 = ws.get(Prec::Single);
-            vec_copy(Prec::Single, p32, Prec::Half, pv, L);
+            vec_copy(Prec::Single, p32, ps, pv, L);
             pv = p32;
             xs = ws.get(Prec::Single);
             rs = ws.get(Prec::Single);

@@ -110,7 +110,7 @@ def test_cg_parity_mismatch_is_an_error(gpu):
     lib.destroy_L("D", L)
 
 
-@pytest.mark.parametrize("inner", ["single", "half"])
+@pytest.mark.parametrize("inner", ["single", "half", "half-links"])
 def test_cg_mixed_reaches_fp64_tolerance(gpu, inner):
     dims = (8, 8, 8, 8)
     lib = gpu.use(dims)

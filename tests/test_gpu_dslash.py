@@ -150,3 +150,28 @@ def test_dslash_timed_runs(gpu):
     for h in (vin, vout):
         lib.destroy_V("F", h)
     lib.destroy_L("F", L)
+
+
+def test_dslash_fp32_vectors_16bit_links(gpu):
+    """The HALF_LINKS inner operator (FP32 vectors with 16-bit fixed-point
+    links) drives a mixed solve to the FP64 tolerance, and the autotuner
+    has timed that vector/link pair."""
+    dims = (8, 8, 8, 8)
+    lib = gpu.use(dims)
+    links = fields(dims, seed=11)
+    src = synthetic.gaussian_source(dims, seed=22, parity="evenodd")
+    L = lib.create_L("D", links)
+    b = lib.create_V("D", src, "even")
+    x = lib.create_V("D", np.zeros_like(src), "even")
+    lib.set_inner_precision("half-links")
+    try:
+        it, info, res = lib.invert("D", L, x, b, 0.05, parity="even", max_iter=2000, nrestart=5, resid=1e-20)
+        st = lib.last_stats()
+    finally:
+        lib.set_inner_precision("double")
+    assert info.status == 0 and res.final_rsq < 1e-20
+    v, us = lib.dslash_variant("half-links")
+    assert v in (0, 1, 2) and min(us) > 0
+    for h in (b, x):
+        lib.destroy_V("D", h)
+    lib.destroy_L("D", L)

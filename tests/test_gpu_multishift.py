@@ -78,7 +78,7 @@ def test_multishift_fp32_close(gpu):
         assert rel_err(a, b) < 2e-5
 
 
-@pytest.mark.parametrize("inner", ["single", "half"])
+@pytest.mark.parametrize("inner", ["single", "half", "half-links"])
 def test_multishift_mixed_every_shift_converges(gpu, inner):
     dims = (8, 8, 8, 8)
     lib = gpu.use(dims)
