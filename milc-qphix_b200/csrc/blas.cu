@@ -136,7 +136,7 @@ k_cg_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverSta
         st->b = round_to(round_to(rsq, single) / oldrsq, single);
         const bool conv = (st->rsqmin <= 0 || st->rsqmin > st->size_r) &&
                           (st->relrsqmin <= 0 || st->relrsqmin > st->size_relr);
-        if ((st->iteration % st->niter == 0) || conv) st->stop_at = gate;
+        if ((st->iteration % st->niter == 0) || conv || run_guard(st)) stop_run(st, gate);
     });
 }
 
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_axpy(VecView<S> r, VecView<S> pv,
 {
     using A = typename Acc<S>::type;
     if (gated_off(st, gate)) return;
-    if (gate >= 0 && st->axpy_skip_at == gate) return;  // p update redone by the host (mixed RU)
+    if (st->skip_axpy) return;  // p update redone by the host after a reliable update
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= r.vh) return;
     A rv[6], p[6];
@@ -188,7 +188,7 @@ k_ms_residual(VecView<S> r, VecView<S> ttt, SolverState *st, double *partials, i
         st->rsq = rsq;
         if (rsq <= st->rsqstop) {
             st->converged = 1;
-            st->stop_at = gate;
+            stop_run(st, gate);
             return;
         }
         const int jl = st->j_low;
@@ -201,7 +201,7 @@ k_ms_residual(VecView<S> r, VecView<S> ttt, SolverState *st, double *partials, i
                                                  st->beta_i[k], single) / zb, single);
             else { st->alpha[k] = 0.0; st->finished[k] = 1; }
         }
-        if (st->iteration >= st->max_cg) st->stop_at = gate;
+        if (st->iteration >= st->max_cg || run_guard(st)) stop_run(st, gate);
     });
 }
 
@@ -289,10 +289,10 @@ k_mx_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverSta
         st->rsq = rsq;
         st->b = rsq / oldrsq;
         const bool ru = (rsq < delta2 * st->rsq_ru) || (rsq <= st->rsqstop) ||
-                        (st->iteration >= st->max_cg) || !(rsq == rsq);
+                        (st->iteration >= st->max_cg) || !(rsq == rsq) || run_guard(st);
         if (ru) {
-            st->stop_at = gate;
-            st->axpy_skip_at = gate;  // this iteration's p update waits for the true residual
+            st->skip_axpy = 1;  // this iteration's p update waits for the true residual
+            stop_run(st, gate);
         }
     });
 }

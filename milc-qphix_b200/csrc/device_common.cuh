@@ -268,6 +268,21 @@ __device__ __forceinline__ bool gated_off(const SolverState *st, int gate)
 
 inline int grid_for(int n) { return (n + kBlock - 1) / kBlock; }
 
+// Ends the device run of a solver phase: records the stopping iteration for
+// the chunked launcher and, inside a CUDA-graph while loop, clears the loop
+// condition.  Called by one thread.
+__device__ __forceinline__ void stop_run(SolverState *st, int gate)
+{
+    st->stop_at = gate;
+    if (st->use_cond) cudaGraphSetConditional(st->cond, 0);
+}
+
+// hard limits of one device run: the iteration cap and a failed kernel wait
+__device__ __forceinline__ bool run_guard(const SolverState *st)
+{
+    return st->iteration >= st->iter_cap || (st->err && *(volatile int *)st->err);
+}
+
 // ------------------------------------------------- TMA bulk copies (sm_100a) --
 // 1-D bulk copy global -> shared completing on an mbarrier (no multicast).
 __device__ __forceinline__ uint32_t smem_u32(const void *p)

@@ -529,6 +529,23 @@ int dslash_variant(Prec pv, Prec pl, float us[3])
 }
 
 template <typename SV, typename SL>
+static void prepare_impl(Prec pv, const LinkSet &ls, const Launch &L)
+{
+    VecBlock none{};
+    auto a = make_args<SV, SL>(L, none, none, ls, 0);
+    (void)tuned_variant<SV, SL>(pv, ls.prec, L, a, ls, 0);
+    (void)resident_grid(k_dslash<SV, SL>, L.g->vh);
+    (void)resident_grid(k_dslash_mdagm<SV, SL>, L.g->vh);
+    (void)tma_grid<SV, SL, 0>(L.g->vh);
+    (void)tma_grid<SV, SL, 1>(L.g->vh);
+}
+
+void dslash_prepare(Prec pv, const LinkSet &ls, const Launch &L)
+{
+    QB_DISPATCH_VL(pv, ls.prec, prepare_impl, pv, ls, L);
+}
+
+template <typename SV, typename SL>
 static void launch_mdagm(const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls,
                          VecBlock pv, double m4, int cb, SolverState *st, double *partials,
                          int gate, int mode, Prec p)

@@ -99,7 +99,12 @@ struct SolverState {
     int j_low;
     int n_shifts;
     int first_iter;
-    int axpy_skip_at;        // mixed CG: chunk iteration whose p update the host redoes
+    int axpy_skip_at;        // (unused) kept for layout stability
+    int skip_axpy;           // mixed CG: the stopping iteration's p update waits for the host
+    int use_cond;            // iterations run inside a CUDA-graph while loop
+    int iter_cap;            // hard cap on st->iteration for one device run
+    unsigned long long cond; // cudaGraphConditionalHandle of that loop
+    int *err;                // kernel failure word (bounded waits); stops the loop
     int max_cg;              // multi-shift: iteration cap (max * nrestart)
     int error;
     unsigned int counter;    // last-block counter of the grid reductions
@@ -138,6 +143,10 @@ void dslash_gated(Prec p, const Launch &L, VecBlock out, VecBlock in, const Link
 void dslash_fixed_d(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb);
 void dslash_mdagm_fixed_d(const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls, VecBlock pv, double m4,
                           int cb, SolverState *st, double *partials);
+
+// run the autotuner and one-time launch set-up for this vector/link pair now
+// (required before a stream capture, which must not synchronise)
+void dslash_prepare(Prec pv, const LinkSet &ls, const Launch &L);
 
 // variant chosen by the Dslash autotuner for precision p; us = its timings
 int dslash_variant(Prec pv, Prec pl, float us[3]);

@@ -109,6 +109,111 @@ int next_chunk(int current, double size_prev, double size_now, int done, double 
     return chunk;
 }
 
+// Runs the device iterations of one solver phase until the device stops.
+// `enqueue(gate)` enqueues one iteration; `next(chunk, it0)` sizes the next
+// chunk from the host mirror S.
+//  * Graph mode: the iteration is captured once (per phase configuration)
+//    into the body of a CUDA-graph while loop; the update kernel's last
+//    block clears the loop condition when the stop test fires, so a whole
+//    phase runs with no host round trip.  A hard iteration cap and the
+//    kernel failure word also end the loop.
+//  * Chunk mode (kernel timing on, or QPHIX_B200_GRAPHS=0): chunks of gated
+//    iterations, one state read per chunk.
+class IterLoop {
+public:
+    IterLoop() = default;
+    IterLoop(const IterLoop &) = delete;
+    IterLoop &operator=(const IterLoop &) = delete;
+    ~IterLoop() { release(); }
+    void invalidate() { release(); }
+
+    template <typename Enq, typename Next>
+    void run(Enq enqueue, Next next, TimedLaunches &tl, int cap, int first_chunk = 8)
+    {
+        Context &c = ctx();
+        SolverState &S = *c.h_state;
+        S.stop_at = INT_MAX;
+        S.skip_axpy = 0;
+        S.err = c.d_err;
+        S.counter = S.counter2 = 0;
+        if (graphs_enabled() && !tl.on) {
+            if (!exec_) build(enqueue);
+            S.use_cond = 1;
+            S.cond = handle_;
+            S.iter_cap = S.iteration + (cap > 0 ? cap : 1);
+            upload_state();
+            QB_CUDA(cudaGraphLaunch(exec_, c.stream));
+            download_state();
+            S.use_cond = 0;
+            if (S.stop_at == INT_MAX) throw Error("solver: device loop ended without a stop");
+            return;
+        }
+        S.use_cond = 0;
+        S.iter_cap = INT_MAX;
+        upload_state();
+        int chunk = first_chunk;
+        for (;;) {
+            for (int k = 0; k < chunk; ++k) enqueue(k);
+            const int it0 = S.iteration;
+            QB_CUDA(cudaGetLastError());
+            download_state();
+            tl.collect(S.stop_at);
+            if (S.stop_at != INT_MAX) break;
+            if (S.iteration == it0) throw Error("solver: device iterations made no progress");
+            chunk = next(chunk, it0);
+        }
+    }
+
+private:
+    static bool graphs_enabled()
+    {
+        static int v = -1;
+        if (v < 0) {
+            const char *e = std::getenv("QPHIX_B200_GRAPHS");
+            v = (e && e[0] == '0') ? 0 : 1;
+        }
+        return v == 1;
+    }
+
+    template <typename Enq> void build(Enq enqueue)
+    {
+        Context &c = ctx();
+        QB_CUDA(cudaGraphCreate(&graph_, 0));
+        QB_CUDA(cudaGraphConditionalHandleCreate(&handle_, graph_, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams p = {};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = handle_;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        cudaGraphNode_t node;
+        QB_CUDA(cudaGraphAddNode(&node, graph_, nullptr, 0, &p));
+        cudaGraph_t body = p.conditional.phGraph_out[0];
+        QB_CUDA(cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueue(-1);
+        } catch (...) {
+            cudaGraph_t dummy;
+            cudaStreamEndCapture(c.stream, &dummy);
+            throw;
+        }
+        QB_CUDA(cudaStreamEndCapture(c.stream, &body));
+        QB_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+    }
+
+    void release()
+    {
+        if (exec_) cudaGraphExecDestroy(exec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        exec_ = nullptr;
+        graph_ = nullptr;
+        handle_ = 0;
+    }
+
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+    cudaGraphConditionalHandle handle_ = 0;
+};
+
 }  // namespace
 
 // ===========================================================================
@@ -177,6 +282,8 @@ int cg_reference(Prec P, const LinkSet &ls, SolveArgs &A)
             return iteration;
         }
         bool switch_parity = false;
+        dslash_prepare(P, ls, L);
+        IterLoop loop;  // rebuilt per parity pass: the vectors differ
         for (;;) {
             if ((iteration % niter == 0) || conv(res->size_r, res->size_relr)) {
                 // (re)initialisation with the true residual (:365-448)
@@ -217,34 +324,26 @@ int cg_reference(Prec P, const LinkSet &ls, SolveArgs &A)
             S.msq_x4 = msq_x4;
             S.iteration = iteration;
             S.niter = niter;
-            S.stop_at = INT_MAX;
-            S.axpy_skip_at = -1;
             S.prec_single = single;
             S.size_r = res->size_r;
             S.size_relr = res->size_relr;
-            S.counter = S.counter2 = 0;
-            upload_state();
-            int chunk = 8;
             double size_prev = res->size_r > 0 ? res->size_r : 1.0;
-            for (;;) {
-                const int cap = niter - (S.iteration % niter);
-                for (int k = 0; k < chunk; ++k) {
+            loop.run(
+                [&](int k) {
                     tl.run(0, k, [&] { dslash_gated(P, L, tmp, cg_p, ls, otherparity, c.d_state, k); });
                     tl.run(1, k, [&] {
                         dslash_mdagm_dot(P, L, ttt, tmp, ls, cg_p, -msq_x4, parity, c.d_state, c.d_partials, k, 0);
                     });
                     cg_update(P, L, t_dest, cg_p, resid, ttt, c.d_state, c.d_partials, k, relres);
                     cg_axpy(P, L, resid, cg_p, c.d_state, k);
-                }
-                const int it0 = S.iteration;
-                QB_CUDA(cudaGetLastError());
-                download_state();
-                tl.collect(S.stop_at);
-                if (S.stop_at != INT_MAX) break;
-                if (S.iteration == it0) throw Error("invert: device iterations made no progress");
-                chunk = next_chunk(chunk, size_prev, S.size_r, S.iteration - it0, rsqmin, cap);
-                size_prev = S.size_r;
-            }
+                },
+                [&](int chunk, int it0) {
+                    const int cap = niter - (S.iteration % niter);
+                    const int n = next_chunk(chunk, size_prev, S.size_r, S.iteration - it0, rsqmin, cap);
+                    size_prev = S.size_r;
+                    return n;
+                },
+                tl, niter - (iteration % niter) + 1);
             iteration = S.iteration;
             rsq = S.rsq;
             relrsq = S.relrsq;
@@ -329,34 +428,28 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
     S.msq_x4 = m4;
     S.iteration = 0;
     S.max_cg = max_cg;
-    S.stop_at = INT_MAX;
-    S.axpy_skip_at = -1;
     S.prec_single = 0;
-    S.counter = S.counter2 = 0;
-    upload_state();
-    int chunk = 8;
     int stalled = 0;
+    dslash_prepare(ps, *ls_cur, L);
+    IterLoop loop;
     for (;;) {
         double size_prev = S.rsq;
-        for (;;) {
-            for (int k = 0; k < chunk; ++k) {
+        loop.run(
+            [&](int k) {
                 tl.run(0, k, [&] { dslash_gated(ps, L, tmps, pv, *ls_cur, other, c.d_state, k); });
                 tl.run(1, k, [&] {
                     dslash_mdagm_dot(ps, L, ttts, tmps, *ls_cur, pv, -m4, parity, c.d_state, c.d_partials, k, 0);
                 });
                 mx_update(ps, L, xs, pv, rs, ttts, c.d_state, c.d_partials, k, delta2);
                 cg_axpy(ps, L, rs, pv, c.d_state, k);
-            }
-            const int it0 = S.iteration;
-            QB_CUDA(cudaGetLastError());
-            download_state();
-            tl.collect(S.stop_at);
-            if (S.stop_at != INT_MAX) break;
-            if (S.iteration == it0) throw Error("invert: device iterations made no progress");
-            const double target = std::max(S.rsqstop, delta2 * S.rsq_ru);
-            chunk = next_chunk(chunk, size_prev, S.rsq, S.iteration - it0, target, 0);
-            size_prev = S.rsq;
-        }
+            },
+            [&](int chunk, int it0) {
+                const double target = std::max(S.rsqstop, delta2 * S.rsq_ru);
+                const int n = next_chunk(chunk, size_prev, S.rsq, S.iteration - it0, target, 0);
+                size_prev = S.rsq;
+                return n;
+            },
+            tl, max_cg - S.iteration + 1);
         out.iterations = S.iteration;
         const double oldrsq = S.oldrsq;
         const double sloppy_rsq = S.rsq;
@@ -388,13 +481,14 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
             ls_cur = ls_up;
             stalled = 0;
             out.escalated = 1;
+            loop.invalidate();
+            dslash_prepare(ps, *ls_cur, L);
         }
         vec_copy(ps, rs, Prec::Double, r64, L);
         S.b = rsq / oldrsq;
         S.rsq = rsq;
         S.rsq_ru = rsq;
-        S.stop_at = INT_MAX;
-        S.axpy_skip_at = -1;
+        S.skip_axpy = 0;
         S.counter = S.counter2 = 0;
         upload_state();
         cg_axpy(ps, L, rs, pv, c.d_state, -1);  // p = r + beta p with the true residual
@@ -501,31 +595,26 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
     S.max_cg = max_cg;
     S.first_iter = 1;
     S.converged = 0;
-    S.stop_at = INT_MAX;
     S.prec_single = single;
-    S.counter = S.counter2 = 0;
-    upload_state();
     const double m4 = round_prec(-1.0 * offset_low, single);
-    int chunk = 8;
     double size_prev = out.rsq;
-    for (;;) {
-        for (int k = 0; k < chunk; ++k) {
+    dslash_prepare(p, ls, L);
+    IterLoop loop;
+    loop.run(
+        [&](int k) {
             tl.run(0, k, [&] { dslash_gated(p, L, tmp, pm[j_low], ls, other, c.d_state, k); });
             tl.run(1, k, [&] {
                 dslash_mdagm_dot(p, L, ttt, tmp, ls, pm[j_low], m4, parity, c.d_state, c.d_partials, k, 1);
             });
             ms_residual(p, L, resid, ttt, c.d_state, c.d_partials, k);
             ms_update(p, L, xp, d_x, d_p, resid, n, c.d_state, k);
-        }
-        const int it0 = S.iteration;
-        QB_CUDA(cudaGetLastError());
-        download_state();
-        tl.collect(S.stop_at);
-        if (S.stop_at != INT_MAX) break;
-        if (S.iteration == it0) throw Error("invert_multi: device iterations made no progress");
-        chunk = next_chunk(chunk, size_prev, S.rsq, S.iteration - it0, S.rsqstop, max_cg - S.iteration);
-        size_prev = S.rsq;
-    }
+        },
+        [&](int chunk, int it0) {
+            const int m = next_chunk(chunk, size_prev, S.rsq, S.iteration - it0, S.rsqstop, max_cg - S.iteration);
+            size_prev = S.rsq;
+            return m;
+        },
+        tl, max_cg + 1);
     out.iteration = S.iteration;
     out.converged = S.converged != 0;
     out.rsq = S.rsq;
