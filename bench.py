@@ -397,7 +397,7 @@ FP64_ITERATIONS = 808
 def run_profile_dslash(args):
     """--mode dslash: one FP32 and one FP64 Dslash launch after a warm-up
     (small-lattice capture target for ncu)."""
-    dims = tuple(int(v) for v in args.lattice.split("x"))
+    dims = tuple(int(v) for v in (args.lattice or "16x16x16x32").split("x"))
     links = synthetic.asqtad_links(dims, seed=LINK_SEED)
     V = int(np.prod(dims))
     lib = capi.QphixLib(LIB_PATH)
@@ -415,7 +415,7 @@ def run_profile_dslash(args):
         lib.destroy_V(prec, vout)
         lib.destroy_L(prec, L)
     lib.finalize()
-    print(json.dumps({"mode": "dslash", "lattice": args.lattice, "reps": args.reps, **out}))
+    print(json.dumps({"mode": "dslash", "lattice": "x".join(map(str, dims)), "reps": args.reps, **out}))
 
 
 def run_profile_mixed(args):
@@ -443,11 +443,263 @@ def run_profile_mixed(args):
     print(json.dumps({"mode": "mixed", "inner": args.inner, "solves": res_all}))
 
 
+MS_DIMS = (32, 32, 32, 64)
+MS_MASS = 0.0012
+MS_SIGMAS = np.logspace(-5, 0, 12)  # RHMC-style shifts sigma_j
+MS_WORKLOAD = ("asqtad CG and 12-shift multi-shift CG 32^3x64, HISQ-shaped links (smeared eps=0.2 fat, "
+               "eps=0.3 Naik), m=0.0012, shifts log-spaced 1e-5..1, tol 1e-10")
+
+
+def _true_rel_rsq(lib, L, x_raw, src, mass, V):
+    """|b - (4m^2 - D_eo D_oe) x|^2 / |b|^2 on the even sites, with the FP64
+    operator applied through QPHIX_D3_asqtad_dslash (independent of the
+    solver's own residual)."""
+    e = slice(0, V * 3)
+    full = np.zeros(V * 6)
+    full[e] = x_raw[e]
+    hin = lib.create_V("D", full)
+    tmp = lib.create_V("D", np.zeros(V * 6))
+    out = lib.create_V("D", np.zeros(V * 6))
+    lib.dslash("D", L, tmp, hin, "odd")
+    lib.dslash("D", L, out, tmp, "even")
+    dd = lib.extract_V("D", out)[e]
+    for h in (hin, tmp, out):
+        lib.destroy_V("D", h)
+    r = src[e] - (4 * mass * mass * x_raw[e] - dd)
+    return float(np.dot(r, r) / np.dot(src[e], src[e]))
+
+
+def run_multishift(args):
+    """--mode multishift: the 32^3x64 workload.  Times, on one GPU and on the
+    same input: the FP64 CG (reference control flow), the mixed CG with FP32
+    and with 16-bit-link inner solves, the FP64 multi-shift CG with 12 shifts
+    and the mixed multi-shift CG; checks every solution's FP64 true residual
+    through the FP64 Dslash and its error against the FP64 solution.  Prints
+    one JSON line."""
+    import torch
+
+    dims = tuple(int(v) for v in args.lattice.split("x")) if args.lattice else MS_DIMS
+    V = int(np.prod(dims))
+    dev = "cuda" if torch.cuda.is_available() else None
+    t0 = time.perf_counter()
+    links = synthetic.asqtad_links(dims, seed=LINK_SEED, eps_fat=0.2, eps_long=0.3, fat_scale=0.9,
+                                   smear=True, device=dev)
+    src = synthetic.gaussian_source(dims, seed=SRC_SEED, parity="even")
+    gen_s = time.perf_counter() - t0
+    torch.cuda.empty_cache()
+    masses = np.sqrt(MS_MASS ** 2 + MS_SIGMAS / 4)
+    lib = capi.QphixLib(LIB_PATH)
+    assert lib.init(dims) == 0, lib.last_error()
+    L = lib.create_L("D", links)
+    b = lib.create_V("D", src, "even")
+    assert L and b, lib.last_error()
+    zeros = np.zeros_like(src)
+    out = {"mode": "multishift", "workload": MS_WORKLOAD, "lattice": "x".join(map(str, dims)),
+           "mass": MS_MASS, "sigmas": [float(s) for s in MS_SIGMAS], "resid_sq": RESID,
+           "seeds": {"links": LINK_SEED, "source": SRC_SEED}, "field_generation_s": gen_s}
+    which = set(args.solves.split(",")) if args.solves else None
+
+    def want(name):
+        return which is None or name in which
+
+    def cg(inner, reps):
+        lib.set_inner_precision(inner)
+        for k in range(reps):
+            x = lib.create_V("D", zeros, "even")
+            lib.timer_start()
+            it, info, res = lib.invert("D", L, x, b, MS_MASS, parity="even", max_iter=MAX_ITER,
+                                       nrestart=NRESTART, resid=RESID)
+            ms = lib.timer_stop()
+            st = lib.last_stats()
+            assert info.status == 0, lib.last_error()
+            sol = lib.extract_V("D", x, "even")
+            lib.destroy_V("D", x)
+        return ms, st, res, sol
+
+    def multi(inner, reps):
+        lib.set_inner_precision(inner)
+        for k in range(reps):
+            xs = [lib.create_V("D", zeros, "even") for _ in masses]
+            lib.timer_start()
+            it, info, res = lib.invert_multi("D", L, xs, b, masses, parity="even", max_iter=MAX_ITER,
+                                             nrestart=NRESTART, resid=RESID)
+            ms = lib.timer_stop()
+            st = lib.last_stats()
+            assert info.status == 0, lib.last_error()
+            sols = [lib.extract_V("D", x, "even") for x in xs]
+            for x in xs:
+                lib.destroy_V("D", x)
+        return ms, st, res, sols
+
+    def rel(a, ref):
+        e = slice(0, V * 3)
+        return float(np.abs(a[e] - ref[e]).max() / np.abs(ref[e]).max())
+
+    def note(name):
+        print(json.dumps({name: out[name]}), file=sys.stderr, flush=True)
+
+    note("field_generation_s")
+    reps = 1 + max(0, min(args.steps, 2) - 1)  # the last of `reps` solves is reported
+    x64 = xs64 = None
+    ms64 = ms64m = None
+    if want("fp64_cg"):
+        ms64, st64, res64, x64 = cg("double", reps)
+        out["fp64_cg"] = {"s": ms64 / 1e3, "iterations": res64.final_iter,
+                          "true_rsq_rel": _true_rel_rsq(lib, L, x64, src, MS_MASS, V)}
+        note("fp64_cg")
+    for inner in ("single", "half-links"):
+        if not want(f"mixed_cg_{inner}"):
+            continue
+        ms, st, res, x = cg(inner, reps)
+        d = {"s": ms / 1e3, "iterations": st.iterations, "reliable_updates": st.reliable_updates,
+             "escalated": st.escalated, "true_rsq_rel": _true_rel_rsq(lib, L, x, src, MS_MASS, V)}
+        if x64 is not None:
+            d["err_vs_fp64"] = rel(x, x64)
+            d["speedup_vs_fp64_cg"] = ms64 / ms
+        if inner == "single":
+            # per-kernel CUDA-event durations from one more solve (not timed)
+            lib.set_kernel_timing(True)
+            _, sti, _, _ = cg(inner, 1)
+            lib.set_kernel_timing(False)
+            d["k1_us"] = sti.dslash_ms / max(sti.dslash_launches, 1) * 1e3
+            d["k2_us"] = sti.mdagm_ms / max(sti.mdagm_launches, 1) * 1e3
+            d["k1_launches"] = sti.dslash_launches
+        out[f"mixed_cg_{inner}"] = d
+        note(f"mixed_cg_{inner}")
+    if want("fp64_multishift"):
+        ms64m, st64m, res64m, xs64 = multi("double", reps)
+        out["fp64_multishift"] = {"s": ms64m / 1e3, "iterations": st64m.iterations,
+                                  "true_rsq_rel": [_true_rel_rsq(lib, L, x, src, m, V)
+                                                   for x, m in zip(xs64, masses)]}
+        note("fp64_multishift")
+    for inner in ("single", "half-links"):
+        if not want(f"mixed_multishift_{inner}"):
+            continue
+        ms, st, res, xs = multi(inner, reps)
+        d = {"s": ms / 1e3, "iterations": st.iterations, "reliable_updates": st.reliable_updates,
+             "true_rsq_rel": [_true_rel_rsq(lib, L, x, src, m, V) for x, m in zip(xs, masses)]}
+        if xs64 is not None:
+            d["err_vs_fp64"] = [rel(x, y) for x, y in zip(xs, xs64)]
+            d["speedup_vs_fp64_multishift"] = ms64m / ms
+        if ms64 is not None:
+            d["speedup_vs_fp64_cg"] = ms64 / ms
+        out[f"mixed_multishift_{inner}"] = d
+        note(f"mixed_multishift_{inner}")
+    lib.destroy_V("D", b)
+    lib.destroy_L("D", L)
+    out["autotuner"] = {k: lib.dslash_variant(k) for k in ("single", "double", "half-links")}
+    lib.finalize()
+    print(json.dumps(out))
+
+
+BATCH_BIG = (24, 24, 24, 48)
+BATCH_NRHS = 16
+BATCH_SMALL = [(8, 8, 8, 8), (12, 12, 12, 12), (16, 16, 16, 32), (20, 20, 20, 40)]
+BATCH_MASS = 0.02
+BATCH_WORKLOAD = ("batched mixed CG: 16 Gaussian RHS on 24^3x48 + 8 lattices (8^4, 12^4, 16^3x32, 20^3x40, "
+                  "two of each, one RHS each), m=0.02, tol 1e-10, one device run")
+
+
+def run_batch(args):
+    """--mode batch: 24 systems on 9 lattices in one QPHIX_B200_D3_batch_invert
+    call (host buffers in and out), against the same systems solved one at a
+    time through QPHIX_D3_asqtad_invert with the FP32 inner solve.  Every
+    solution's FP64 true residual is checked through the FP64 Dslash."""
+    import torch
+
+    dev = "cuda" if torch.cuda.is_available() else None
+    t0 = time.perf_counter()
+    lats = [BATCH_BIG] + [d for d in BATCH_SMALL for _ in range(2)]
+    links = [synthetic.asqtad_links(d, seed=LINK_SEED + i, device=dev) for i, d in enumerate(lats)]
+    systems = [(0, BATCH_MASS, synthetic.gaussian_source(BATCH_BIG, seed=SRC_SEED + r, parity="even"))
+               for r in range(BATCH_NRHS)]
+    systems += [(l, BATCH_MASS, synthetic.gaussian_source(lats[l], seed=SRC_SEED + 100 + l, parity="even"))
+                for l in range(1, len(lats))]
+    gen_s = time.perf_counter() - t0
+    print(json.dumps({"field_generation_s": gen_s}), file=sys.stderr, flush=True)
+    if dev:
+        torch.cuda.empty_cache()
+    lib = capi.QphixLib(LIB_PATH)
+    assert lib.init(BATCH_BIG) == 0, lib.last_error()
+    B = lib.batch_create_L(list(zip(lats, links)))
+    assert B, lib.last_error()
+    outs = [torch.zeros(s[2].shape, dtype=torch.float64).pin_memory().numpy() for s in systems]
+    pinned_src = [torch.from_numpy(s[2]).pin_memory().numpy() for s in systems]
+    psys = [(l, m, p) for (l, m, _), p in zip(systems, pinned_src)]
+
+    def batch_solve():
+        for o in outs:
+            o[:] = 0.0
+        lib.timer_start()
+        w0 = time.perf_counter()
+        it, info, res, xs = lib.batch_invert(B, psys, max_iter=MAX_ITER, nrestart=NRESTART, resid=RESID,
+                                             outs=outs)
+        wall = time.perf_counter() - w0
+        ms = lib.timer_stop()
+        assert info.status == 0, lib.last_error()
+        return max(ms / 1e3, wall), res, [x.copy() for x in xs]
+
+    for _ in range(max(1, args.warmup)):
+        batch_solve()
+    times = []
+    for _ in range(max(1, args.steps)):
+        s, res, xs = batch_solve()
+        times.append(s)
+    s_batch = float(np.median(times))
+    print(json.dumps({"batch_s": s_batch, "iterations": [r.final_iter for r in res]}), file=sys.stderr, flush=True)
+    lib.batch_destroy_L(B)
+
+    # the same systems one at a time (FP32 inner, FP64 reliable updates)
+    seq = 0.0
+    seq_iters = []
+    trues = []
+    lib.finalize()
+    for l, dims in enumerate(lats):
+        mine = [k for k, s in enumerate(systems) if s[0] == l]
+        assert lib.init(dims) == 0, lib.last_error()
+        L = lib.create_L("D", links[l])
+        lib.set_inner_precision("single")
+        V = int(np.prod(dims))
+        for rep in range(2):  # the first pass warms the autotuner and the graphs
+            for k in mine:
+                b = lib.create_V("D", systems[k][2], "even")
+                x = lib.create_V("D", np.zeros_like(systems[k][2]), "even")
+                lib.timer_start()
+                it, info, r1 = lib.invert("D", L, x, b, BATCH_MASS, parity="even", max_iter=MAX_ITER,
+                                          nrestart=NRESTART, resid=RESID)
+                ms = lib.timer_stop()
+                if rep == 1:
+                    seq += ms / 1e3
+                    seq_iters.append(lib.last_stats().iterations)
+                lib.destroy_V("D", b)
+                lib.destroy_V("D", x)
+        for k in mine:
+            trues.append(_true_rel_rsq(lib, L, xs[k], systems[k][2], BATCH_MASS, V))
+        lib.destroy_L("D", L)
+        lib.finalize()
+    print(json.dumps({
+        "mode": "batch", "workload": BATCH_WORKLOAD, "systems": len(systems), "lattices": len(lats),
+        "field_generation_s": gen_s, "batch_s": s_batch, "batch_all_s": times,
+        "sequential_s": seq, "speedup_vs_sequential": seq / s_batch,
+        "batch_iterations": [r.final_iter for r in res], "batch_reliable_updates": [r.final_restart for r in res],
+        "sequential_iterations": seq_iters,
+        "true_rsq_rel_max": max(trues), "true_rsq_rel": trues,
+        "timing": "batch: one C-ABI call from pinned host buffers (H2D of sources and guesses, D2H of "
+                  "solutions inside); sequential: device time of each QPHIX_D3_asqtad_invert on resident vectors",
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", default="bench", choices=["bench", "dslash", "mixed"],
-                    help="bench: the benchmark line; dslash/mixed: small profiling targets")
-    ap.add_argument("--lattice", default="16x16x16x32")
+    ap.add_argument("--mode", default="bench", choices=["bench", "dslash", "mixed", "multishift", "batch"],
+                    help="bench: the benchmark line; dslash/mixed: small profiling targets; "
+                         "multishift: the 32^3x64 CG and 12-shift multi-shift workload; "
+                         "batch: 24 systems on 9 lattices in one batched solve")
+    ap.add_argument("--lattice", default=None)
+    ap.add_argument("--solves", default=None,
+                    help="multishift mode: comma-separated subset of fp64_cg, mixed_cg_single, "
+                         "mixed_cg_half-links, fp64_multishift, mixed_multishift_single, "
+                         "mixed_multishift_half-links")
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--inner", default="single", choices=["single", "half", "double"])
     ap.add_argument("--gpus", type=int, default=1)
@@ -462,6 +714,12 @@ def main():
         return
     if args.mode == "mixed":
         run_profile_mixed(args)
+        return
+    if args.mode == "multishift":
+        run_multishift(args)
+        return
+    if args.mode == "batch":
+        run_batch(args)
         return
     if args.impl == "reference":
         run_reference(args)

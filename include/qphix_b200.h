@@ -9,6 +9,7 @@
 #define _QPHIX_B200_H
 
 #include <qphix_int.h>
+#include <qphix_f3.h>
 #include <qphix_d3.h>
 
 #ifdef __cplusplus
@@ -100,6 +101,56 @@ int QPHIX_B200_dslash_variant(QPHIX_B200_precision_t p, double us[3]);
 QPHIX_status_t QPHIX_B200_D3_asqtad_mdagm_noalloc(QPHIX_D3_FermionLinksAsqtad *L, QPHIX_D3_ColorVector *out,
                                                  QPHIX_D3_ColorVector *in, QPHIX_D_Real mass,
                                                  QPHIX_evenodd_t parity, double *in_dot_out);
+
+/* ---- Batched solves (no counterpart in the reference) ----------------------
+ * The reference solves one system per QPHIX_D3_asqtad_invert call
+ * (ks_d_congrad_fn.cpp:221) on the lattice fixed by QPHIX_init.  A batch
+ * holds the gauge fields of nlat <= 16 lattices, each of any size QPHIX_init
+ * accepts and independent of the QPHIX_init lattice (which must exist), and
+ * solves many systems on them in one device run.
+ *
+ * QPHIX_B200_D3_batch_create_L: lattice l has extents latsize[4l..4l+3]
+ * = {Nx,Ny,Nz,Nt} and raw MILC links fat[l], lng[l], fatback[l],
+ * lngback[l] (the layout of QPHIX_D3_asqtad_create_L_from_raw, both
+ * parities).  Returns NULL on failure (QPHIX_B200_last_error). */
+typedef struct QPHIX_B200_Batch_struct QPHIX_B200_Batch;
+QPHIX_B200_Batch *QPHIX_B200_D3_batch_create_L(int nlat, const int *latsize, double *const *fat,
+                                               double *const *lng, double *const *fatback,
+                                               double *const *lngback);
+void QPHIX_B200_D3_batch_destroy_L(QPHIX_B200_Batch *B);
+
+/* Solves (4 mass[k]^2 - D_eo D_oe) x_k = in_k for k = 0..nsys-1 (nsys <= 64)
+ * on the sites of parity inv_arg->parity (QPHIX_EVEN or QPHIX_ODD), system
+ * k on lattice lat[k].  in[k] and out[k] are raw MILC colour vectors of that
+ * lattice (6 reals per site, even sites first); out[k] holds the initial
+ * guess and receives the solution on the solve parity.  Inner CG in FP32
+ * with FP64 reliable updates (QPHIX_B200_set_reliable_delta); each system
+ * stops when its FP64 true residual satisfies |r|^2 <= res_arg[k]->resid
+ * |b|^2.  Systems on one lattice share every link load.  At most
+ * inv_arg->max * inv_arg->nrestart iterations.  res_arg[k] receives
+ * final_rsq (relative, squared), final_iter and final_restart (reliable
+ * updates); returns the largest iteration count. */
+int QPHIX_B200_D3_batch_invert(QPHIX_info_t *info, QPHIX_B200_Batch *B, QPHIX_invert_arg_t *inv_arg,
+                               QPHIX_resid_arg_t **res_arg, int nsys, const int *lat,
+                               const double *mass, double *const *out, double *const *in);
+
+/* ---- Fermion force (no counterpart in the reference) -----------------------
+ * Gradient of S = sum_k coef[k] phi_k^dag (4 m_k^2 - D_pq D_qp)^{-1} phi_k
+ * with respect to the fat and Naik links, given the solutions
+ * x[k] = (4 m_k^2 - D_pq D_qp)^{-1} phi_k on parity p = `parity` (EVEN or
+ * ODD; e.g. from QPHIX_*_asqtad_invert or the shifts of _invert_multi).
+ * The backward links are taken to be the caller's shifted forward links
+ * (fatback(x) = fat(x - mu), lngback(x) = lng(x - 3 mu)), so the gradient
+ * covers both uses of each link.  grad_fat and grad_lng have the layout of
+ * the raw fat and lng arrays (72 reals per site, both parities): entry
+ * (site, mu, a, b, re/im) = dS / d(Re or Im of U_mu(site)_ab).  D x is
+ * recomputed on the device; the call allocates two raw-layout buffers. */
+QPHIX_status_t QPHIX_B200_D3_asqtad_force(QPHIX_D3_FermionLinksAsqtad *L, int n, const double *coef,
+                                          QPHIX_D3_ColorVector **x, QPHIX_evenodd_t parity,
+                                          double *grad_fat, double *grad_lng);
+QPHIX_status_t QPHIX_B200_F3_asqtad_force(QPHIX_F3_FermionLinksAsqtad *L, int n, const float *coef,
+                                          QPHIX_F3_ColorVector **x, QPHIX_evenodd_t parity,
+                                          float *grad_fat, float *grad_lng);
 
 /* Host-side neighbour arithmetic used by the Dslash kernels (no GPU
  * needed): block index, in the opposite parity, of neighbour k of site

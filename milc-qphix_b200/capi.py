@@ -140,10 +140,83 @@ class QphixLib:
                                                              C.c_int, C.POINTER(C.c_double)]
             L.QPHIX_B200_dslash_variant.restype = C.c_int
             L.QPHIX_B200_dslash_variant.argtypes = [C.c_int, C.POINTER(C.c_double)]
+            dpp = C.POINTER(C.POINTER(C.c_double))
+            L.QPHIX_B200_D3_batch_create_L.restype = C.c_void_p
+            L.QPHIX_B200_D3_batch_create_L.argtypes = [C.c_int, C.POINTER(C.c_int), dpp, dpp, dpp, dpp]
+            L.QPHIX_B200_D3_batch_destroy_L.restype = None
+            L.QPHIX_B200_D3_batch_destroy_L.argtypes = [C.c_void_p]
+            L.QPHIX_B200_D3_batch_invert.restype = C.c_int
+            L.QPHIX_B200_D3_batch_invert.argtypes = [C.POINTER(Info), C.c_void_p, C.POINTER(InvertArg),
+                                                     C.POINTER(C.POINTER(ResidArg)), C.c_int,
+                                                     C.POINTER(C.c_int), C.POINTER(C.c_double), dpp, dpp]
+            for P, real in (("F", C.c_float), ("D", C.c_double)):
+                f = getattr(L, f"QPHIX_B200_{P}3_asqtad_force")
+                f.restype = C.c_int
+                f.argtypes = [C.c_void_p, C.c_int, C.POINTER(real), C.POINTER(C.c_void_p), C.c_int,
+                              C.POINTER(real), C.POINTER(real)]
             L.QPHIX_B200_neighbor_index.restype = C.c_long
             L.QPHIX_B200_neighbor_index.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_long, C.c_int]
 
     # -- QPHIX_B200_* ------------------------------------------------------
+    @staticmethod
+    def _dptrs(arrays):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in arrays]
+        ptrs = (C.POINTER(C.c_double) * len(arrs))(*[a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs])
+        return ptrs, arrs
+
+    def batch_create_L(self, lattices):
+        """``lattices``: list of (dims, links), links a dict of raw FP64
+        ``fat, lng, fatback, lngback``.  Returns the batch handle (or None)."""
+        n = len(lattices)
+        sizes = (C.c_int * (4 * n))(*[int(v) for dims, _ in lattices for v in dims])
+        keep, ptrs = [], []
+        for key in ("fat", "lng", "fatback", "lngback"):
+            p, a = self._dptrs([links[key] for _, links in lattices])
+            ptrs.append(p)
+            keep.append(a)
+        return self.lib.QPHIX_B200_D3_batch_create_L(n, sizes, *ptrs)
+
+    def batch_destroy_L(self, B):
+        self.lib.QPHIX_B200_D3_batch_destroy_L(B)
+
+    def batch_invert(self, B, systems, parity="even", max_iter=1000, nrestart=5, resid=1e-20, outs=None):
+        """``systems``: list of (lattice index, mass, source raw vector[,
+        initial guess]).  ``outs`` (optional): the raw arrays that receive
+        the solutions.  Returns (iterations, info, [ResidArg], [solutions])."""
+        n = len(systems)
+        info = Info()
+        inv = InvertArg(PARITY[parity], max_iter, max_iter, nrestart, QPHIX_EVENODD)
+        res = [ResidArg(resid, 0, 0, 0, 0, 0, 0, 0) for _ in range(n)]
+        res_ptrs = (C.POINTER(ResidArg) * n)(*[C.pointer(r) for r in res])
+        lat = (C.c_int * n)(*[int(s[0]) for s in systems])
+        mass = (C.c_double * n)(*[float(s[1]) for s in systems])
+        srcs = [np.ascontiguousarray(s[2], dtype=np.float64) for s in systems]
+        if outs is None:
+            outs = [np.array(s[3], dtype=np.float64) if len(s) > 3 else np.zeros_like(srcs[k])
+                    for k, s in enumerate(systems)]
+        pin, _ = self._dptrs(srcs)
+        pout = (C.POINTER(C.c_double) * n)(*[o.ctypes.data_as(C.POINTER(C.c_double)) for o in outs])
+        it = self.lib.QPHIX_B200_D3_batch_invert(C.byref(info), B, C.byref(inv), res_ptrs, n, lat, mass, pout, pin)
+        return it, info, res, outs
+
+    def force(self, prec, L, xs, coef, parity="even"):
+        """Gradient of sum_k coef[k] phi_k^dag M^-1 phi_k with respect to the
+        raw fat and Naik links, from the solutions ``xs`` (handles).  Returns
+        (grad_fat, grad_lng) in the raw link layout."""
+        ct, nt = self._real(prec)
+        n = len(xs)
+        V = int(np.prod(self.dims))
+        gf = np.zeros(V * 72, dtype=nt)
+        gl = np.zeros(V * 72, dtype=nt)
+        c = np.ascontiguousarray(coef, dtype=nt)
+        arr = (C.c_void_p * n)(*xs)
+        rc = getattr(self.lib, f"QPHIX_B200_{prec}3_asqtad_force")(
+            L, n, c.ctypes.data_as(C.POINTER(ct)), arr, PARITY[parity],
+            gf.ctypes.data_as(C.POINTER(ct)), gl.ctypes.data_as(C.POINTER(ct)))
+        if rc != 0:
+            raise RuntimeError("asqtad_force failed: " + self.last_error())
+        return gf, gl
+
     def last_error(self):
         if not self.has_b200:
             return ""

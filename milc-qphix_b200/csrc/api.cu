@@ -60,15 +60,7 @@ void init_context(QPHIX_layout_t *layout)
     for (int i = 0; i < layout->machdim; ++i) nranks *= layout->machsize ? layout->machsize[i] : 1;
     if (nranks != 1) throw Error("QPHIX_init: one lattice per GPU; machsize must be all ones");
     const int *L = layout->latsize;
-    for (int i = 0; i < 4; ++i)
-        if (L[i] <= 0) throw Error("QPHIX_init: non-positive lattice extent");
-    if (L[0] % 2) throw Error("QPHIX_init: Nx must be even");
-    if ((L[0] / 2) % 2 != 0) throw Error("QPHIX_init: Nx/2 must be even");
-    if (L[1] % 4 || L[2] % 4 || L[3] % 4) throw Error("QPHIX_init: Ny, Nz and Nt must be multiples of 4");
-    const long long V = (long long)L[0] * L[1] * L[2] * L[3];
-    if (V / 2 > (1LL << 30)) throw Error("QPHIX_init: lattice too large for 32-bit site indices");
-    if (2LL * ((V / 2 + kBlock - 1) / kBlock) > 4LL * kMaxPartials)
-        throw Error("QPHIX_init: lattice too large for one GPU's reduction scratch");
+    check_lattice(L, "QPHIX_init");
     if (layout->node_number) {
         const int orig[4] = {0, 0, 0, 0};
         (void)layout->node_number(orig);  // the reference calls it (qphix_misc.cpp:489)

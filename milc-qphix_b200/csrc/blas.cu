@@ -288,7 +288,15 @@ k_mx_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverSta
         st->oldrsq = oldrsq;
         st->rsq = rsq;
         st->b = rsq / oldrsq;
-        const bool ru = (rsq < delta2 * st->rsq_ru) || (rsq <= st->rsqstop) ||
+        bool stalled = false;
+        if (rsq < st->ru_best) {
+            st->ru_best = rsq;
+            st->ru_best_iter = st->iteration;
+        } else if (st->ru_stall_window > 0 && st->iteration - st->ru_best_iter >= st->ru_stall_window) {
+            stalled = true;
+            st->ru_stalled = 1;
+        }
+        const bool ru = (rsq < delta2 * st->rsq_ru) || (rsq <= st->rsqstop) || stalled ||
                         (st->iteration >= st->max_cg) || !(rsq == rsq) || run_guard(st);
         if (ru) {
             st->skip_axpy = 1;  // this iteration's p update waits for the true residual

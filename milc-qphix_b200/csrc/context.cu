@@ -1,5 +1,6 @@
 // Context, device memory and state transfer helpers.
 #include "context.h"
+#include "device_common.cuh"
 
 namespace qb {
 
@@ -28,6 +29,20 @@ void dev_free(void *p)
     if (p) cudaFreeAsync(p, ctx().stream);
 }
 
+void check_lattice(const int L[4], const char *who)
+{
+    const std::string w(who);
+    for (int i = 0; i < 4; ++i)
+        if (L[i] <= 0) throw Error(w + ": non-positive lattice extent");
+    if (L[0] % 2) throw Error(w + ": Nx must be even");
+    if ((L[0] / 2) % 2 != 0) throw Error(w + ": Nx/2 must be even");
+    if (L[1] % 4 || L[2] % 4 || L[3] % 4) throw Error(w + ": Ny, Nz and Nt must be multiples of 4");
+    const long long V = (long long)L[0] * L[1] * L[2] * L[3];
+    if (V / 2 > (1LL << 30)) throw Error(w + ": lattice too large for 32-bit site indices");
+    if (2LL * ((V / 2 + kBlock - 1) / kBlock) > 4LL * kMaxPartials)
+        throw Error(w + ": lattice too large for one GPU's reduction scratch");
+}
+
 static size_t cx_bytes(Prec p) { return p == Prec::Double ? 16 : (p == Prec::Single ? 8 : 4); }
 
 VecBlock alloc_vec(Prec p)
@@ -52,11 +67,13 @@ void free_vec(VecBlock &b)
     b.norm = nullptr;
 }
 
-LinkSet alloc_links(Prec p)
+LinkSet alloc_links(Prec p) { return alloc_links(p, ctx().g.vh); }
+
+LinkSet alloc_links(Prec p, int vh)
 {
     Context &c = ctx();
     LinkSet ls;
-    const size_t bytes = (size_t)kMats * 9 * c.g.vh * cx_bytes(p);
+    const size_t bytes = (size_t)kMats * 9 * vh * cx_bytes(p);
     for (int cb = 0; cb < 2; ++cb) {
         ls.blk[cb] = dev_alloc(bytes);
         QB_CUDA(cudaMemsetAsync(ls.blk[cb], 0, bytes, c.stream));

@@ -101,7 +101,8 @@ void dev_free(void *p);
 
 VecBlock alloc_vec(Prec p);
 void free_vec(VecBlock &b);
-LinkSet alloc_links(Prec p);
+LinkSet alloc_links(Prec p);          // for the QPHIX_init lattice
+LinkSet alloc_links(Prec p, int vh);  // for a lattice of vh sites per parity
 void free_links(LinkSet &ls);
 
 void upload_state();    // h_state -> d_state (async)
@@ -109,6 +110,10 @@ void download_state();  // d_state -> h_state, waits
 void sync_check();      // waits for the stream; throws if a kernel reported a failed wait
 
 double wall_seconds();
+
+// lattice extents the library accepts (the reference's asserts,
+// qphix_misc.cpp:455-469,494-497); throws Error("<who>: ...") otherwise
+void check_lattice(const int L[4], const char *who);
 
 }  // namespace qb
 

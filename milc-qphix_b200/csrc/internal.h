@@ -106,6 +106,14 @@ struct SolverState {
     unsigned long long cond; // cudaGraphConditionalHandle of that loop
     int *err;                // kernel failure word (bounded waits); stops the loop
     int max_cg;              // multi-shift: iteration cap (max * nrestart)
+    // mixed CG: stagnation of the inner solve.  The smallest inner |r|^2
+    // since the last reliable update and the iteration it was seen; no new
+    // minimum for ru_stall_window iterations forces a reliable update and
+    // sets ru_stalled.
+    double ru_best;
+    int ru_best_iter;
+    int ru_stall_window;
+    int ru_stalled;
     int error;
     unsigned int counter;    // last-block counter of the grid reductions
     unsigned int counter2;

@@ -372,6 +372,10 @@ int cg_reference(Prec P, const LinkSet &ls, SolveArgs &A)
 // ===========================================================================
 namespace {
 
+// iterations without a new smallest inner residual after which the mixed CG
+// takes a reliable update and restarts its search direction
+constexpr int kInnerStallWindow = 256;
+
 struct MixedResult {
     double true_rsq_rel = 0;
     int iterations = 0;
@@ -429,6 +433,10 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
     S.iteration = 0;
     S.max_cg = max_cg;
     S.prec_single = 0;
+    S.ru_best = rsq;
+    S.ru_best_iter = 0;
+    S.ru_stall_window = kInnerStallWindow;
+    S.ru_stalled = 0;
     int stalled = 0;
     dslash_prepare(ps, *ls_cur, L);
     IterLoop loop;
@@ -466,9 +474,12 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
         if (out.true_rsq_rel < tol || S.iteration >= max_cg || !std::isfinite(rsq)) break;
         // A 16-bit inner solve perturbs the operator by ~1e-4 relative; once
         // the residual lives in the lowest modes of an ill-conditioned system
-        // the corrections stop reducing the true residual.  Two reliable
-        // updates in a row that fail to halve it switch the inner solve to FP32.
-        stalled = (rsq > 0.25 * prev_true) ? stalled + 1 : 0;
+        // the corrections stop reducing the true residual, or the inner CG
+        // itself stops reducing its residual.  Two reliable updates in a row
+        // that fail to halve the true residual, or that an inner stagnation
+        // forced, switch the inner solve to FP32.
+        const bool inner_stall = S.ru_stalled != 0;
+        stalled = (rsq > 0.25 * prev_true || inner_stall) ? stalled + 1 : 0;
         if (stalled >= 2 && (ps == Prec::Half || ls_cur->prec == Prec::Half) && ls_up && ls_up->valid) {
             VecBlock p32 = ws.get(Prec::Single);
             vec_copy(Prec::Single, p32, ps, pv, L);
@@ -485,9 +496,13 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
             dslash_prepare(ps, *ls_cur, L);
         }
         vec_copy(ps, rs, Prec::Double, r64, L);
-        S.b = rsq / oldrsq;
+        // after an inner stagnation the search direction is restarted (p = r)
+        S.b = inner_stall ? 0.0 : rsq / oldrsq;
         S.rsq = rsq;
         S.rsq_ru = rsq;
+        S.ru_best = rsq;
+        S.ru_best_iter = S.iteration;
+        S.ru_stalled = 0;
         S.skip_axpy = 0;
         S.counter = S.counter2 = 0;
         upload_state();

@@ -88,20 +88,27 @@ def _torch_device(device):
 
 
 def random_su3(n, eps, rng, device=None):
-    """``n`` SU(3) matrices ``exp(i*eps*H)`` as complex128 numpy (n,3,3)."""
+    """``n`` SU(3) matrices ``exp(i*eps*H)`` as complex128 numpy (n,3,3).
+
+    On the CPU the exponential is formed from the eigendecomposition of H; on
+    a GPU with ``torch.linalg.matrix_exp`` (both exact to FP64 rounding), then
+    re-unitarised.  The Gaussian draws are the same either way."""
     torch, dev = _torch_device(device)
     a = rng.standard_normal((n, 3, 3)) + 1j * rng.standard_normal((n, 3, 3))
     out = np.empty((n, 3, 3), dtype=np.complex128)
-    # batched eigh: the GPU solver takes at most ~1e5 matrices per call
-    chunk = 1 << 16 if str(dev).startswith("cuda") else 1 << 21
+    on_gpu = str(dev).startswith("cuda")
+    chunk = 1 << 20 if on_gpu else 1 << 21
     for s in range(0, n, chunk):
         A = torch.from_numpy(a[s:s + chunk]).to(dev)
         H = 0.5 * (A + A.mH)
         tr = torch.diagonal(H, dim1=-2, dim2=-1).sum(-1) / 3.0
         H = H - tr[:, None, None] * torch.eye(3, dtype=H.dtype, device=dev)
-        w, Q = torch.linalg.eigh(H)
-        ph = torch.exp(1j * eps * w.to(torch.complex128))
-        U = (Q * ph[:, None, :]) @ Q.mH
+        if on_gpu:
+            U = torch.linalg.matrix_exp(1j * eps * H)
+        else:
+            w, Q = torch.linalg.eigh(H)
+            ph = torch.exp(1j * eps * w.to(torch.complex128))
+            U = (Q * ph[:, None, :]) @ Q.mH
         out[s:s + chunk] = _reunitarize(torch, U).cpu().numpy()
     return out
 
@@ -159,6 +166,28 @@ def _smear3(lat, U):
     return out
 
 
+def _smear3_torch(U, dev):
+    """_smear3 on a torch device (same arithmetic; used for large lattices)."""
+    import torch
+    T = torch.from_numpy(U).to(dev)
+    ax = lambda mu: 3 - mu  # noqa: E731  (axis of direction mu in (T,Z,Y,X))
+    sh = lambda a, mu, k: torch.roll(a, -k, dims=ax(mu))  # noqa: E731
+    adj = lambda a: a.mH  # noqa: E731
+    out = T.clone()
+    for mu in range(4):
+        Umu = T[..., mu, :, :]
+        acc = torch.zeros_like(Umu)
+        for nu in range(4):
+            if nu == mu:
+                continue
+            Unu = T[..., nu, :, :]
+            acc += Unu @ sh(Umu, nu, 1) @ adj(sh(Unu, mu, 1))
+            Unu_mnu = sh(Unu, nu, -1)
+            acc += adj(Unu_mnu) @ sh(Umu, nu, -1) @ sh(Unu_mnu, mu, 1)
+        out[..., mu, :, :] = Umu + acc / 8.0
+    return out.cpu().numpy()
+
+
 def _to_raw_links(lat, Ulex):
     """(T,Z,Y,X,4,3,3) complex -> raw float64 (V*72,)."""
     lex = lat.lex_of_raw()
@@ -177,6 +206,22 @@ def _backlinks(lat, Ulex, hop):
     return out
 
 
+def links_raw_to_lex(dims, raw):
+    """Raw MILC link array (V*72 reals) -> complex (T,Z,Y,X,4,3,3)."""
+    lat = Lattice(dims)
+    a = np.asarray(raw, dtype=np.float64).reshape(lat.V, 4, 3, 3, 2)
+    U = np.empty((lat.V, 4, 3, 3), dtype=np.complex128)
+    U[lat.lex_of_raw()] = a[..., 0] + 1j * a[..., 1]
+    return U.reshape(lat.nt, lat.nz, lat.ny, lat.nx, 4, 3, 3)
+
+
+def backlinks_raw(dims, raw, hop):
+    """The backward-link array MILC passes beside a forward one: the forward
+    link of x - hop*mu placed at x (no adjoint), raw layout."""
+    lat = Lattice(dims)
+    return _to_raw_links(lat, _backlinks(lat, links_raw_to_lex(dims, raw), hop))
+
+
 def asqtad_links(dims, seed=1001, eps_fat=0.3, eps_long=0.3, fat_scale=0.9,
                  smear=False, device=None):
     """Random asqtad/HISQ-shaped links in raw layout.
@@ -192,7 +237,8 @@ def asqtad_links(dims, seed=1001, eps_fat=0.3, eps_long=0.3, fat_scale=0.9,
     Uf = random_su3(lat.V * 4, eps_fat, rng, device).reshape(shape)
     Ul = random_su3(lat.V * 4, eps_long, rng, device).reshape(shape)
     if smear:
-        Uf = _smear3(lat, Uf)
+        torch, dev = _torch_device(device)
+        Uf = _smear3_torch(Uf, dev) if str(dev).startswith("cuda") else _smear3(lat, Uf)
         norm = np.mean(np.sqrt(np.sum(np.abs(Uf) ** 2, axis=(-1, -2)) / 3.0))
         Uf = Uf * (fat_scale / norm)
     else:
