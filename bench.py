@@ -577,6 +577,7 @@ def run_multishift(args):
             continue
         ms, st, res, xs = multi(inner, reps)
         d = {"s": ms / 1e3, "iterations": st.iterations, "reliable_updates": st.reliable_updates,
+             "final_iter_per_shift": [r.final_iter for r in res],
              "true_rsq_rel": [_true_rel_rsq(lib, L, x, src, m, V) for x, m in zip(xs, masses)]}
         if xs64 is not None:
             d["err_vs_fp64"] = [rel(x, y) for x, y in zip(xs, xs64)]
@@ -689,12 +690,104 @@ def run_batch(args):
     }))
 
 
+FORCE_DIMS = (16, 16, 16, 32)
+FORCE_MASS = 0.05
+FORCE_WORKLOAD = ("fermion force d/dU of phi^dag (4m^2 - D_eo D_oe)^-1 phi, 16^3x32, m=0.05, eps=0.3 links; "
+                  "central finite differences h=1e-5 along 32 random su(3) directions dU = i T U")
+
+
+def run_force(args):
+    """--mode force: the fermion force on 16^3x32 through the C ABI.  Checks
+    the FP64 force against central finite differences of S along 32 random
+    su(3) perturbations of all fat and Naik links (every S from an FP64 solve),
+    the FP32 force against the FP64 one, and times both."""
+    dims = FORCE_DIMS
+    V = int(np.prod(dims))
+    lat = synthetic.Lattice(dims)
+    links = synthetic.asqtad_links(dims, seed=LINK_SEED)
+    phi = synthetic.gaussian_source(dims, seed=SRC_SEED, parity="even")
+    lib = capi.QphixLib(LIB_PATH)
+    assert lib.init(dims) == 0, lib.last_error()
+    lib.set_inner_precision("double")
+
+    def action(fat, lng, want_force=False):
+        lk = {"fat": fat, "lng": lng, "fatback": synthetic.backlinks_raw(dims, fat, 1),
+              "lngback": synthetic.backlinks_raw(dims, lng, 3)}
+        L = lib.create_L("D", lk)
+        b = lib.create_V("D", phi, "even")
+        x = lib.create_V("D", np.zeros_like(phi), "even")
+        it, info, res = lib.invert("D", L, x, b, FORCE_MASS, parity="even", max_iter=MAX_ITER,
+                                   nrestart=NRESTART, resid=1e-26)
+        assert info.status == 0, lib.last_error()
+        xr = lib.extract_V("D", x, "even")
+        S = float(np.dot(phi[: 3 * V], xr[: 3 * V]))
+        out = (S,)
+        if want_force:
+            lib.force("D", L, [x], [1.0], "even")  # warm
+            lib.timer_start()
+            gf, gl = lib.force("D", L, [x], [1.0], "even")
+            ms64 = lib.timer_stop()
+            k64 = lib.last_stats().solve_ms
+            Lf = lib.create_L("F", lk)
+            xf = lib.create_V("F", xr, "even")
+            lib.force("F", Lf, [xf], [1.0], "even")
+            lib.timer_start()
+            ff, fl = lib.force("F", Lf, [xf], [1.0], "even")
+            ms32 = lib.timer_stop()
+            k32 = lib.last_stats().solve_ms
+            lib.destroy_V("F", xf)
+            lib.destroy_L("F", Lf)
+            out = (S, gf, gl, ff, fl, ms64, ms32, it, k64, k32)
+        for h in (b, x):
+            lib.destroy_V("D", h)
+        lib.destroy_L("D", L)
+        return out
+
+    S0, gf, gl, ff, fl, ms64, ms32, iters, k64, k32 = action(links["fat"], links["lng"], True)
+    gnorm = float(np.sqrt(gf @ gf + gl @ gl))
+    rng = np.random.default_rng(3003)
+    h = 1e-5
+    errs, nerrs = [], []
+    t0 = time.perf_counter()
+    for _ in range(32):
+        dirs = []
+        for key in ("fat", "lng"):
+            U = synthetic.links_raw_to_lex(dims, links[key])
+            a = rng.standard_normal(U.shape) + 1j * rng.standard_normal(U.shape)
+            T = 0.5 * (a + np.conj(np.swapaxes(a, -1, -2)))
+            T = T - (np.trace(T, axis1=-2, axis2=-1) / 3.0)[..., None, None] * np.eye(3)
+            dirs.append(synthetic._to_raw_links(lat, 1j * T @ U))
+        Sp = action(links["fat"] + h * dirs[0], links["lng"] + h * dirs[1])[0]
+        Sm = action(links["fat"] - h * dirs[0], links["lng"] - h * dirs[1])[0]
+        fd = (Sp - Sm) / (2 * h)
+        an = float(gf @ dirs[0] + gl @ dirs[1])
+        errs.append(abs(fd - an) / abs(an))
+        nerrs.append(abs(fd - an) / (gnorm * float(np.sqrt(dirs[0] @ dirs[0] + dirs[1] @ dirs[1]))))
+    fd_s = time.perf_counter() - t0
+    scale = max(np.abs(gf).max(), np.abs(gl).max())
+    lib.finalize()
+    bytes64 = 2 * V * 72 * 8
+    print(json.dumps({
+        "mode": "force", "workload": FORCE_WORKLOAD, "lattice": "x".join(map(str, dims)), "mass": FORCE_MASS,
+        "action": S0, "solve_iterations": iters, "fd_perturbations": len(errs), "fd_h": h,
+        "fd_rel_err_max": max(errs), "fd_rel_err_median": float(np.median(errs)), "fd_wall_s": fd_s,
+        "fp32_vs_fp64_max_rel": float(max(np.abs(ff - gf).max(), np.abs(fl - gl).max()) / scale),
+        "fd_err_over_grad_times_dir_norm_max": max(nerrs),
+        "force_call_ms": {"f64": ms64, "f32": ms32},
+        "force_kernels_ms": {"f64": k64, "f32": k32},
+        "force_kernels_gbs_f64": (bytes64 + DSLASH_BYTES_F64 * V // 2 + 2 * V * 48) / (k64 * 1e-3) / 1e9,
+        "force_call_note": "one C-ABI call: D x, the outer-product kernel and the D2H copy of both "
+                           f"gradient arrays ({bytes64 / 1e6:.0f} MB FP64)",
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", default="bench", choices=["bench", "dslash", "mixed", "multishift", "batch"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "dslash", "mixed", "multishift", "batch", "force"],
                     help="bench: the benchmark line; dslash/mixed: small profiling targets; "
                          "multishift: the 32^3x64 CG and 12-shift multi-shift workload; "
-                         "batch: 24 systems on 9 lattices in one batched solve")
+                         "batch: 24 systems on 9 lattices in one batched solve; "
+                         "force: the 16^3x32 fermion force against finite differences")
     ap.add_argument("--lattice", default=None)
     ap.add_argument("--solves", default=None,
                     help="multishift mode: comma-separated subset of fp64_cg, mixed_cg_single, "
@@ -720,6 +813,9 @@ def main():
         return
     if args.mode == "batch":
         run_batch(args)
+        return
+    if args.mode == "force":
+        run_force(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -144,7 +144,9 @@ int QPHIX_B200_D3_batch_invert(QPHIX_info_t *info, QPHIX_B200_Batch *B, QPHIX_in
  * covers both uses of each link.  grad_fat and grad_lng have the layout of
  * the raw fat and lng arrays (72 reals per site, both parities): entry
  * (site, mu, a, b, re/im) = dS / d(Re or Im of U_mu(site)_ab).  D x is
- * recomputed on the device; the call allocates two raw-layout buffers. */
+ * recomputed on the device; the call allocates two raw-layout buffers.
+ * Afterwards QPHIX_B200_get_last_stats reports in solve_ms the device time
+ * of the force kernels (D x and the outer products, not the copies). */
 QPHIX_status_t QPHIX_B200_D3_asqtad_force(QPHIX_D3_FermionLinksAsqtad *L, int n, const double *coef,
                                           QPHIX_D3_ColorVector **x, QPHIX_evenodd_t parity,
                                           double *grad_fat, double *grad_lng);

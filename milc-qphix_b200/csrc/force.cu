@@ -25,38 +25,55 @@
 
 namespace qb {
 
-template <typename R>
+// One block covers 64 consecutive raw sites x 4 directions, whose gradient
+// entries are one contiguous run of 256 x 18 reals per link family.  The
+// outer products go through shared memory so that the block writes that run
+// with coalesced stores (a thread's own 18 reals are 144 bytes apart from its
+// neighbour's).  ACC = false: the first solution writes the gradient; true:
+// later ones add to it.
+template <typename R, bool ACC>
 __global__ void __launch_bounds__(kBlock) k_force(R *gfat, R *glng, VecView<R> x, VecView<R> y, Geom g, int P,
                                                   R coef)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // (raw site i, mu)
-    if (t >= 8LL * g.vh) return;
-    const int mu = (int)(t & 3);
-    const int i = (int)(t >> 2);
-    const int p = i >= g.vh ? 1 : 0;
-    const int j = i - p * g.vh;
-    const SiteCoords s = decode(g, p, j);
-    const VecView<R> &here = (p == P) ? x : y;
-    const VecView<R> &there = (p == P) ? y : x;
+    __shared__ R stage[kBlock * 18];
+    const long long n = 8LL * g.vh;  // (raw site, direction) pairs
+    const long long t0 = (long long)blockIdx.x * kBlock;
+    const long long t = t0 + threadIdx.x;
     R w[6], wn[2][6];
-    here.load(j, w);
-    there.load(neighbor(g, s, 2 * mu + 1), wn[0]);
-    there.load(neighbor(g, s, 8 + 2 * mu + 1), wn[1]);
-    const R sc = (p == P ? R(2) : R(-2)) * coef;
-    R *out[2] = {gfat + ((size_t)i * 4 + mu) * 18, glng + ((size_t)i * 4 + mu) * 18};
+    R sc = 0;
+    if (t < n) {
+        const int i = (int)(t >> 2), mu = (int)(t & 3);
+        const int p = i >= g.vh ? 1 : 0;
+        const int j = i - p * g.vh;
+        const SiteCoords s = decode(g, p, j);
+        const VecView<R> &here = (p == P) ? x : y;
+        const VecView<R> &there = (p == P) ? y : x;
+        here.load(j, w);
+        there.load(neighbor(g, s, 2 * mu + 1), wn[0]);
+        there.load(neighbor(g, s, 8 + 2 * mu + 1), wn[1]);
+        sc = (p == P ? R(2) : R(-2)) * coef;
+    }
+    const long long nout = (n - t0 < kBlock ? n - t0 : kBlock) * 18;  // reals this block writes
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
+        if (t < n) {
+            R *o = stage + threadIdx.x * 18;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
+            for (int a = 0; a < 3; ++a) {
 #pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                const R re = w[2 * a] * wn[h][2 * b] + w[2 * a + 1] * wn[h][2 * b + 1];
-                const R im = w[2 * a] * wn[h][2 * b + 1] - w[2 * a + 1] * wn[h][2 * b];
-                R *o = out[h] + 6 * a + 2 * b;
-                o[0] += sc * re;
-                o[1] -= sc * im;
+                for (int b = 0; b < 3; ++b) {
+                    o[6 * a + 2 * b] = sc * (w[2 * a] * wn[h][2 * b] + w[2 * a + 1] * wn[h][2 * b + 1]);
+                    o[6 * a + 2 * b + 1] = -sc * (w[2 * a] * wn[h][2 * b + 1] - w[2 * a + 1] * wn[h][2 * b]);
+                }
             }
         }
+        __syncthreads();
+        R *dst = (h == 0 ? gfat : glng) + t0 * 18;
+        for (int e = threadIdx.x; e < nout; e += kBlock) {
+            if (ACC) dst[e] += stage[e];
+            else dst[e] = stage[e];
+        }
+        __syncthreads();
     }
 }
 
@@ -89,18 +106,24 @@ static void force_impl(typename ForceApi<Real>::FL *H, int n, const Real *coef, 
     Real *g = static_cast<Real *>(dev_alloc(2 * nraw * sizeof(Real)));
     VecBlock y = alloc_vec(ForceApi<Real>::prec);
     try {
-        QB_CUDA(cudaMemsetAsync(g, 0, 2 * nraw * sizeof(Real), c.stream));
+        QB_CUDA(cudaEventRecord(c.ev_solve[0], c.stream));
         const int grid = (int)((8LL * c.g.vh + kBlock - 1) / kBlock);
         for (int k = 0; k < n; ++k) {
             const VecBlock xb = x[k]->blk[P];
             dslash(ForceApi<Real>::prec, L, y, xb, H->links, 1 - P);  // y = D_qp x
-            k_force<Real><<<grid, kBlock, 0, c.stream>>>(g, g + nraw, view<Real>(xb, c.g.vh), view<Real>(y, c.g.vh),
-                                                         c.g, P, coef[k]);
+            const VecView<Real> xv = view<Real>(xb, c.g.vh), yv = view<Real>(y, c.g.vh);
+            if (k == 0) k_force<Real, false><<<grid, kBlock, 0, c.stream>>>(g, g + nraw, xv, yv, c.g, P, coef[k]);
+            else k_force<Real, true><<<grid, kBlock, 0, c.stream>>>(g, g + nraw, xv, yv, c.g, P, coef[k]);
         }
         QB_CUDA(cudaGetLastError());
+        QB_CUDA(cudaEventRecord(c.ev_solve[1], c.stream));
         QB_CUDA(cudaMemcpyAsync(grad_fat, g, nraw * sizeof(Real), cudaMemcpyDeviceToHost, c.stream));
         QB_CUDA(cudaMemcpyAsync(grad_lng, g + nraw, nraw * sizeof(Real), cudaMemcpyDeviceToHost, c.stream));
         sync_check();
+        float ms = 0.f;
+        QB_CUDA(cudaEventElapsedTime(&ms, c.ev_solve[0], c.ev_solve[1]));
+        c.stats = Stats{};
+        c.stats.solve_ms = ms;
     } catch (...) {
         free_vec(y);
         dev_free(g);
