@@ -43,6 +43,7 @@ MASS = 0.01
 RESID = 1e-20          # squared: |r|/|b| < 1e-10
 MAX_ITER, NRESTART = 20000, 5
 LINK_SEED, SRC_SEED = 1001, 2002
+RU_DELTA = 0.1         # reliable update at every 0.1 drop of |r| (24^3x48 workload)
 DSLASH_BYTES_F32 = 1200  # algorithmic bytes per output site, FP32, 18-real links
 DSLASH_BYTES_F64 = 2400
 DSLASH_FLOPS = 1146
@@ -149,6 +150,7 @@ def run_gpu(args):
     Vh = V // 2
     lib = capi.QphixLib(LIB_PATH)
     assert lib.init(DIMS) == 0, lib.last_error()
+    lib.set_reliable_delta(RU_DELTA)  # the workload's reliable-update threshold
     L = lib.create_L("D", links)
     b = lib.create_V("D", src, "even")
     assert L and b, lib.last_error()
@@ -283,6 +285,7 @@ def run_gpu(args):
         "dtype": "f32 inner / f64 reliable updates",
         "data": "synthetic (seeded random SU(3) links, Gaussian source)",
         "config": {"workload": WORKLOAD, "lattice": "24x24x24x48", "mass": MASS, "resid_sq": RESID,
+                   "reliable_delta": RU_DELTA,
                    "seeds": {"links": LINK_SEED, "source": SRC_SEED}, "parallelism": f"replicas{world}",
                    "l2": "working set (links 0.76 GB FP32, 1.5 GB FP64) exceeds the 126 MB L2"},
         "solve": {"iterations": int(np.median(iters)), "reliable_updates": int(np.median(rus)),
@@ -423,6 +426,7 @@ def run_profile_mixed(args):
     links, src = make_inputs()
     lib = capi.QphixLib(LIB_PATH)
     assert lib.init(DIMS) == 0, lib.last_error()
+    lib.set_reliable_delta(RU_DELTA)
     L = lib.create_L("D", links)
     b = lib.create_V("D", src, "even")
     lib.set_inner_precision(args.inner)
@@ -490,12 +494,14 @@ def run_multishift(args):
     masses = np.sqrt(MS_MASS ** 2 + MS_SIGMAS / 4)
     lib = capi.QphixLib(LIB_PATH)
     assert lib.init(dims) == 0, lib.last_error()
+    lib.set_reliable_delta(0.2)
     L = lib.create_L("D", links)
     b = lib.create_V("D", src, "even")
     assert L and b, lib.last_error()
     zeros = np.zeros_like(src)
     out = {"mode": "multishift", "workload": MS_WORKLOAD, "lattice": "x".join(map(str, dims)),
            "mass": MS_MASS, "sigmas": [float(s) for s in MS_SIGMAS], "resid_sq": RESID,
+           "reliable_delta": 0.2,
            "seeds": {"links": LINK_SEED, "source": SRC_SEED}, "field_generation_s": gen_s}
     which = set(args.solves.split(",")) if args.solves else None
 
@@ -610,9 +616,11 @@ def run_batch(args):
 
     dev = "cuda" if torch.cuda.is_available() else None
     t0 = time.perf_counter()
-    lats = [BATCH_BIG] + [d for d in BATCH_SMALL for _ in range(2)]
+    # --lattice: the 16 right-hand sides on that lattice alone (profiling target)
+    big = tuple(int(v) for v in args.lattice.split("x")) if args.lattice else BATCH_BIG
+    lats = [big] + ([] if args.lattice else [d for d in BATCH_SMALL for _ in range(2)])
     links = [synthetic.asqtad_links(d, seed=LINK_SEED + i, device=dev) for i, d in enumerate(lats)]
-    systems = [(0, BATCH_MASS, synthetic.gaussian_source(BATCH_BIG, seed=SRC_SEED + r, parity="even"))
+    systems = [(0, BATCH_MASS, synthetic.gaussian_source(big, seed=SRC_SEED + r, parity="even"))
                for r in range(BATCH_NRHS)]
     systems += [(l, BATCH_MASS, synthetic.gaussian_source(lats[l], seed=SRC_SEED + 100 + l, parity="even"))
                 for l in range(1, len(lats))]
@@ -621,7 +629,7 @@ def run_batch(args):
     if dev:
         torch.cuda.empty_cache()
     lib = capi.QphixLib(LIB_PATH)
-    assert lib.init(BATCH_BIG) == 0, lib.last_error()
+    assert lib.init(big) == 0, lib.last_error()
     B = lib.batch_create_L(list(zip(lats, links)))
     assert B, lib.last_error()
     outs = [torch.zeros(s[2].shape, dtype=torch.float64).pin_memory().numpy() for s in systems]
@@ -649,6 +657,11 @@ def run_batch(args):
     s_batch = float(np.median(times))
     print(json.dumps({"batch_s": s_batch, "iterations": [r.final_iter for r in res]}), file=sys.stderr, flush=True)
     lib.batch_destroy_L(B)
+    if args.no_sequential:
+        lib.finalize()
+        print(json.dumps({"mode": "batch", "workload": BATCH_WORKLOAD, "batch_s": s_batch,
+                          "batch_iterations": [r.final_iter for r in res]}))
+        return
 
     # the same systems one at a time (FP32 inner, FP64 reliable updates)
     seq = 0.0
@@ -749,7 +762,7 @@ def run_force(args):
     h = 1e-5
     errs, nerrs = [], []
     t0 = time.perf_counter()
-    for _ in range(32):
+    for _ in range(args.fd_dirs):
         dirs = []
         for key in ("fat", "lng"):
             U = synthetic.links_raw_to_lex(dims, links[key])
@@ -770,9 +783,10 @@ def run_force(args):
     print(json.dumps({
         "mode": "force", "workload": FORCE_WORKLOAD, "lattice": "x".join(map(str, dims)), "mass": FORCE_MASS,
         "action": S0, "solve_iterations": iters, "fd_perturbations": len(errs), "fd_h": h,
-        "fd_rel_err_max": max(errs), "fd_rel_err_median": float(np.median(errs)), "fd_wall_s": fd_s,
+        "fd_rel_err_max": max(errs) if errs else None,
+        "fd_rel_err_median": float(np.median(errs)) if errs else None, "fd_wall_s": fd_s,
         "fp32_vs_fp64_max_rel": float(max(np.abs(ff - gf).max(), np.abs(fl - gl).max()) / scale),
-        "fd_err_over_grad_times_dir_norm_max": max(nerrs),
+        "fd_err_over_grad_times_dir_norm_max": max(nerrs) if nerrs else None,
         "force_call_ms": {"f64": ms64, "f32": ms32},
         "force_kernels_ms": {"f64": k64, "f32": k32},
         "force_kernels_gbs_f64": (bytes64 + DSLASH_BYTES_F64 * V // 2 + 2 * V * 48) / (k64 * 1e-3) / 1e9,
@@ -801,6 +815,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fd-dirs", type=int, default=32,
+                    help="force mode: finite-difference directions (0: force only)")
+    ap.add_argument("--no-sequential", action="store_true",
+                    help="batch mode: skip the one-at-a-time comparison (profiling target)")
     args = ap.parse_args()
     if args.mode == "dslash":
         run_profile_dslash(args)

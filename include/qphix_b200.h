@@ -40,7 +40,7 @@ QPHIX_B200_precision_t QPHIX_B200_get_inner_precision(void);
 
 /* Reliable-update threshold of the mixed-precision solvers: the FP64 true
  * residual is recomputed when the sloppy residual norm has dropped by this
- * factor since the last update (default 0.1). */
+ * factor since the last update (default 0.2). */
 QPHIX_status_t QPHIX_B200_set_reliable_delta(double delta);
 
 /* Diagnostics of the most recent invert / invert_multi call. */

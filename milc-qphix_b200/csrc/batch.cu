@@ -5,12 +5,12 @@
 // batch holds the gauge fields of several lattices of different sizes and
 // solves (4 m_k^2 - D_eo D_oe) x_k = b_k for up to kBMaxSys systems at once:
 //
-//  * Systems on the same lattice form segments of nrhs = 1, 2, 4, ..., 32
-//    right-hand sides.  A segment's colour vectors are stored site-major
-//    with the right-hand side fastest, c2[(c*Vh + j)*nrhs + r], so one
-//    thread applies every link it loads to G right-hand sides (G = 4 FP32,
-//    2 FP64): the link stream -- 1152 of the 1200 bytes per site of a
-//    single-RHS FP32 Dslash -- is shared by the whole segment.
+//  * Systems on the same lattice form segments of nrhs = G * 2^k <= 32
+//    right-hand sides (G = 1..4).  A segment's colour vectors are stored
+//    site-major with the right-hand side fastest, c2[(c*Vh + j)*nrhs + r], so
+//    one thread applies every link it loads to G right-hand sides: the link
+//    stream -- 1152 of the 1200 bytes per site of a single-RHS FP32 Dslash --
+//    is shared by the whole segment.
 //  * Every kernel runs over all segments of all lattices: a resident grid
 //    walks a table of 256-item tiles; per-system reductions are kept in
 //    registers per segment, combined per block in shared memory and
@@ -38,7 +38,6 @@ namespace qb {
 
 constexpr int kBMaxSys = 64;  // systems per batched solve (64-bit masks)
 constexpr int kBMaxSeg = 64;
-constexpr int kBMaxRhs = 32;  // right-hand sides per segment
 constexpr int kBMaxLat = 16;
 
 // One segment under one kernel's thread mapping: items are (site, group of
@@ -46,9 +45,9 @@ constexpr int kBMaxLat = 16;
 // the vector kernels.
 struct BSeg {
     Geom g;
-    int nrhs;         // right-hand sides (power of two)
+    int nrhs;         // right-hand sides (G * 2^k)
     int G;            // right-hand sides per thread
-    int lg_ngrp;      // log2(items per site): nrhs / G for the Dslash, nrhs for vectors
+    int lg_ngrp;      // log2(groups of G right-hand sides)
     int sys0;         // first batch system of the segment
     int tile0;        // first tile of the segment
     int items;
@@ -229,9 +228,12 @@ __device__ __forceinline__ void bload(const float2 *f, int vh, int nrhs, int j, 
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const float2 *p = f + ((size_t)(c * vh + j) * nrhs + q * G);
-        if constexpr (G == 1) {
-            const float2 z = __ldg(p);
-            v[0][2 * c] = z.x; v[0][2 * c + 1] = z.y;
+        if constexpr (G % 2 == 1) {
+#pragma unroll
+            for (int e = 0; e < G; ++e) {
+                const float2 z = __ldg(p + e);
+                v[e][2 * c] = z.x; v[e][2 * c + 1] = z.y;
+            }
         } else {
 #pragma unroll
             for (int e = 0; e < G; e += 2) {
@@ -249,8 +251,9 @@ __device__ __forceinline__ void bstore(float2 *f, int vh, int nrhs, int j, int q
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float2 *p = f + ((size_t)(c * vh + j) * nrhs + q * G);
-        if constexpr (G == 1) {
-            *p = make_float2(v[0][2 * c], v[0][2 * c + 1]);
+        if constexpr (G % 2 == 1) {
+#pragma unroll
+            for (int e = 0; e < G; ++e) p[e] = make_float2(v[e][2 * c], v[e][2 * c + 1]);
         } else {
 #pragma unroll
             for (int e = 0; e < G; e += 2)
@@ -400,6 +403,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bdslash_s(const BTable *tab, BSta
         if (item < sh.seg.items) {
             switch (sh.seg.G) {
             case 4: bdslash_s_item<4, MDAGM>(item, cb, out, in, pv, sh, acc); break;
+            case 3: bdslash_s_item<3, MDAGM>(item, cb, out, in, pv, sh, acc); break;
             case 2: bdslash_s_item<2, MDAGM>(item, cb, out, in, pv, sh, acc); break;
             default: bdslash_s_item<1, MDAGM>(item, cb, out, in, pv, sh, acc); break;
             }
@@ -482,8 +486,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_bdslash_d(const BTable *tab, BSta
         }
         const int item = (t - sh.seg.tile0) * kBlock + threadIdx.x;
         if (item < sh.seg.items) {
-            if (sh.seg.G == 2) bdslash_d_item<2, RESID>(item, cb, out, in, f, sh, acc);
-            else bdslash_d_item<1, RESID>(item, cb, out, in, f, sh, acc);
+            switch (sh.seg.G) {
+            case 3: bdslash_d_item<3, RESID>(item, cb, out, in, f, sh, acc); break;
+            case 2: bdslash_d_item<2, RESID>(item, cb, out, in, f, sh, acc); break;
+            default: bdslash_d_item<1, RESID>(item, cb, out, in, f, sh, acc); break;
+            }
         }
     }
     if constexpr (RESID) {
@@ -518,7 +525,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_bdslash_d(const BTable *tab, BSta
 }
 
 // ------------------------------------------------------ vector kernels --
-// Items are complex numbers of a segment; system = sys0 + (item & (nrhs-1)).
+// Items are (complex number of a segment's (component, site) space, group
+// of G right-hand sides); system = sys0 + q*G + e.
 enum BOp : int {
     kBNormB = 0,    // |b|^2 -> bnorm, rsqstop, flags of the first reliable update
     kBUpdate = 1,   // x_s += a p, r -= a Ap, |r|^2 -> b, reliable-update flags
@@ -563,35 +571,43 @@ __global__ void __launch_bounds__(kBlock) k_bvec(const BTable *tab, BState *st, 
         const BSeg &sg = sh.seg;
         const int item = (t - sg.tile0) * kBlock + threadIdx.x;
         if (item >= sg.items) continue;
-        const int k = sg.sys0 + (item & (sg.nrhs - 1));
-        if (!(mask >> k & 1ull)) continue;
-        const size_t i = sg.voff + item;
-        if constexpr (OP == kBNormB) {
-            const double2 z = f.b[i];
-            acc[0][0] += z.x * z.x + z.y * z.y;
-        } else if constexpr (OP == kBUpdate) {
-            const float a = (float)sh.coef[0][k];
-            const float2 p = f.p[i], ap = f.ap[i];
-            float2 x = f.xs[i], r = f.r[i];
-            x.x += a * p.x; x.y += a * p.y;
-            r.x -= a * ap.x; r.y -= a * ap.y;
-            f.xs[i] = x;
-            f.r[i] = r;
-            acc[0][0] += (double)(r.x * r.x + r.y * r.y);
-        } else if constexpr (OP == kBAxpy || OP == kBAxpyRu) {
-            const float b = (float)sh.coef[1][k];
-            const float2 r = f.r[i];
-            float2 p = f.p[i];
-            p.x = r.x + b * p.x;
-            p.y = r.y + b * p.y;
-            f.p[i] = p;
-        } else {
-            const float2 xs = f.xs[i];
-            double2 x = f.x[i];
-            x.x += (double)xs.x;
-            x.y += (double)xs.y;
-            f.x[i] = x;
-            f.xs[i] = make_float2(0.f, 0.f);
+        // item = (complex number of the (component, site) space, group q);
+        // the thread handles the G right-hand sides of its group
+        const int q = item & ((1 << sg.lg_ngrp) - 1);
+        const size_t base = sg.voff + (size_t)(item >> sg.lg_ngrp) * sg.nrhs + q * sg.G;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            if (e >= sg.G) break;
+            const int k = sg.sys0 + q * sg.G + e;
+            if (!(mask >> k & 1ull)) continue;
+            const size_t i = base + e;
+            if constexpr (OP == kBNormB) {
+                const double2 z = f.b[i];
+                acc[0][e] += z.x * z.x + z.y * z.y;
+            } else if constexpr (OP == kBUpdate) {
+                const float a = (float)sh.coef[0][k];
+                const float2 p = f.p[i], ap = f.ap[i];
+                float2 x = f.xs[i], r = f.r[i];
+                x.x += a * p.x; x.y += a * p.y;
+                r.x -= a * ap.x; r.y -= a * ap.y;
+                f.xs[i] = x;
+                f.r[i] = r;
+                acc[0][e] += (double)(r.x * r.x + r.y * r.y);
+            } else if constexpr (OP == kBAxpy || OP == kBAxpyRu) {
+                const float b = (float)sh.coef[1][k];
+                const float2 r = f.r[i];
+                float2 p = f.p[i];
+                p.x = r.x + b * p.x;
+                p.y = r.y + b * p.y;
+                f.p[i] = p;
+            } else {
+                const float2 xs = f.xs[i];
+                double2 x = f.x[i];
+                x.x += (double)xs.x;
+                x.y += (double)xs.y;
+                f.x[i] = x;
+                f.xs[i] = make_float2(0.f, 0.f);
+            }
         }
     }
     if constexpr (NV > 0) {
@@ -694,6 +710,12 @@ int resident_blocks(K kernel)
     return std::max(1, per_sm) * sms;
 }
 
+// one lattice of a batched solve: geometry and its FP64 / FP32 link blocks
+struct LatRef {
+    const Geom *g;
+    const LinkSet *l64, *l32;
+};
+
 struct SegPlan {
     int lat, nrhs, sys0;
     std::vector<int> user;  // caller's system index of each slot
@@ -706,8 +728,42 @@ int log2i(int n)
     return l;
 }
 
-// kind 0: FP32 Dslash (G <= 4), 1: FP64 Dslash (G <= 2), 2: vector kernels
-BTable make_table(const std::vector<SegPlan> &plan, const QPHIX_B200_Batch &B, int kind)
+// Segment sizes: G * 2^k with G = 1..4 right-hand sides per thread, so that
+// every kernel's groups per site are a power of two (warp-shuffle sums).
+constexpr int kSegSizes[] = {32, 24, 16, 12, 8, 6, 4, 3, 2, 1};
+
+// Systems of each lattice in segments of the largest allowed size first;
+// slot_of[k] = batch slot of caller system k.
+std::vector<SegPlan> plan_segments(int nlat, int nsys, const int *lat, std::vector<int> &slot_of)
+{
+    std::vector<SegPlan> plan;
+    slot_of.assign(nsys, 0);
+    int sys = 0;
+    for (int l = 0; l < nlat; ++l) {
+        std::vector<int> mine;
+        for (int k = 0; k < nsys; ++k)
+            if (lat[k] == l) mine.push_back(k);
+        size_t pos = 0;
+        while (pos < mine.size()) {
+            int n = 1;
+            for (int sz : kSegSizes)
+                if (sz <= (int)(mine.size() - pos)) { n = sz; break; }
+            SegPlan p{l, n, sys, {}};
+            for (int r = 0; r < n; ++r) {
+                p.user.push_back(mine[pos + r]);
+                slot_of[mine[pos + r]] = sys + r;
+            }
+            sys += n;
+            pos += n;
+            plan.push_back(p);
+        }
+    }
+    if ((int)plan.size() > kBMaxSeg) throw Error("batch: too many segments");
+    return plan;
+}
+
+// kind 0: FP32 Dslash (G <= 4), 1: FP64 Dslash (G <= 3), 2: vector kernels
+BTable make_table(const std::vector<SegPlan> &plan, const std::vector<LatRef> &lats, int kind)
 {
     BTable t{};
     t.nseg = (int)plan.size();
@@ -715,22 +771,25 @@ BTable make_table(const std::vector<SegPlan> &plan, const QPHIX_B200_Batch &B, i
     int tile = 0;
     for (int s = 0; s < t.nseg; ++s) {
         const SegPlan &p = plan[s];
-        const auto &L = B.lats[p.lat];
+        const LatRef &L = lats[p.lat];
+        const int n = p.nrhs;
         BSeg &g = t.seg[s];
-        g.g = L.g;
-        g.nrhs = p.nrhs;
+        g.g = *L.g;
+        g.nrhs = n;
         g.sys0 = p.sys0;
         g.voff = voff;
-        voff += 3LL * L.g.vh * p.nrhs;
+        voff += 3LL * L.g->vh * n;
         if (kind == 2) {
-            g.G = 1;
-            g.lg_ngrp = log2i(p.nrhs);
-            g.items = 3 * L.g.vh * p.nrhs;
+            int ngrp = 1;
+            while (ngrp < 32 && n % (2 * ngrp) == 0) ngrp *= 2;
+            g.G = n / ngrp;
+            g.lg_ngrp = log2i(ngrp);
+            g.items = 3 * L.g->vh * ngrp;
         } else {
-            g.G = std::min(p.nrhs, kind == 0 ? 4 : 2);
-            g.lg_ngrp = log2i(p.nrhs / g.G);
-            g.items = L.g.vh * (p.nrhs / g.G);
-            const LinkSet &ls = kind == 0 ? L.l32 : L.l64;
+            g.G = (n % 3 == 0) ? 3 : std::min(n, kind == 0 ? 4 : 2);
+            g.lg_ngrp = log2i(n / g.G);
+            g.items = L.g->vh * (n / g.G);
+            const LinkSet &ls = kind == 0 ? *L.l32 : *L.l64;
             g.links[0] = ls.blk[0];
             g.links[1] = ls.blk[1];
         }
@@ -858,6 +917,129 @@ struct BatchMem {
     }
 };
 
+
+// One batched solve.  load(f, vtab) fills f.b and f.x (sources and initial
+// guesses, vector-table layout); store(f, vtab, h) reads the solutions and
+// the per-system results after the run.  m4[s] and resid[s] are per batch
+// slot.
+template <typename Load, typename Store>
+void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan, int nsys, const double *m4,
+               const double *resid, int cb, int iter_cap, Load load, Store store)
+{
+    Context &c = ctx();
+    const BTable tabs[3] = {make_table(plan, lats, 0), make_table(plan, lats, 1), make_table(plan, lats, 2)};
+    long long ncx = 0;
+    for (const auto &p : plan) ncx += 3LL * lats[p.lat].g->vh * p.nrhs;
+
+    BatchMem mem;
+    BTable *d_tabs = static_cast<BTable *>(mem.get(sizeof(tabs)));
+    BState *d_st = static_cast<BState *>(mem.get(sizeof(BState)));
+    BFields f{};
+    void *mem64 = mem.get((size_t)ncx * 16 * 3);
+    void *mem32 = mem.get((size_t)ncx * 8 * 5);
+    f.x = static_cast<double2 *>(mem64);
+    f.b = f.x + ncx;
+    f.t64 = f.b + ncx;
+    f.xs = static_cast<float2 *>(mem32);
+    f.r = f.xs + ncx;
+    f.p = f.r + ncx;
+    f.ap = f.p + ncx;
+    f.t32 = f.ap + ncx;
+    QB_CUDA(cudaMemsetAsync(mem64, 0, (size_t)ncx * 16 * 3, c.stream));
+    QB_CUDA(cudaMemsetAsync(mem32, 0, (size_t)ncx * 8 * 5, c.stream));
+    QB_CUDA(cudaMemcpyAsync(d_tabs, tabs, sizeof(tabs), cudaMemcpyHostToDevice, c.stream));
+
+    static int rb_s0 = 0, rb_s1, rb_d0, rb_d1, rb_v[5];
+    if (!rb_s0) {
+        rb_s1 = resident_blocks(k_bdslash_s<true>);
+        rb_d0 = resident_blocks(k_bdslash_d<false>);
+        rb_d1 = resident_blocks(k_bdslash_d<true>);
+        rb_v[0] = resident_blocks(k_bvec<0>);
+        rb_v[1] = resident_blocks(k_bvec<1>);
+        rb_v[2] = resident_blocks(k_bvec<2>);
+        rb_v[3] = resident_blocks(k_bvec<3>);
+        rb_v[4] = resident_blocks(k_bvec<4>);
+        rb_s0 = resident_blocks(k_bdslash_s<false>);
+    }
+    auto grid = [](int res_blocks, int ntiles) { return std::max(1, std::min(res_blocks, ntiles)); };
+    BatchRun R{};
+    R.tab_s = d_tabs;
+    R.tab_d = d_tabs + 1;
+    R.tab_v = d_tabs + 2;
+    R.grid_s0 = grid(rb_s0, tabs[0].ntiles);
+    R.grid_s1 = grid(rb_s1, tabs[0].ntiles);
+    R.grid_d0 = grid(rb_d0, tabs[1].ntiles);
+    R.grid_d1 = grid(rb_d1, tabs[1].ntiles);
+    for (int i = 0; i < 5; ++i) R.grid_v[i] = grid(rb_v[i], tabs[2].ntiles);
+    const int gmax = std::max({R.grid_s1, R.grid_d1, R.grid_v[0], R.grid_v[1]});
+    R.partials = static_cast<double *>(mem.get(sizeof(double) * kBMaxSys * gmax));
+    R.st = d_st;
+    R.f = f;
+    R.cb = cb;
+    R.other = 1 - cb;
+    R.stream = c.stream;
+
+    load(f, tabs[2], mem);
+
+    BState *h = pinned_state();
+    std::memset(h, 0, sizeof(BState));
+    h->nsys = nsys;
+    h->delta2 = c.reliable_delta * c.reliable_delta;
+    h->iter_cap = std::max(1, iter_cap);
+    for (int s = 0; s < nsys; ++s) {
+        h->sys[s].m4 = m4[s];
+        h->sys[s].resid = resid[s];
+    }
+    upload(d_st, h, c.stream);
+    k_bvec<kBNormB><<<R.grid_v[kBNormB], kBlock, 0, c.stream>>>(R.tab_v, d_st, f, R.partials);
+    QB_CUDA(cudaGetLastError());
+    download(h, d_st, c.stream);
+
+    if (!h->stop) {
+        if (batch_graphs_enabled()) {
+            BatchGraph G;
+            G.build(R);
+            h->use_cond = 1;
+            h->cond_loop = G.hloop;
+            h->cond_ru = G.hru;
+            upload(d_st, h, c.stream);
+            QB_CUDA(cudaGraphLaunch(G.exec, c.stream));
+            download(h, d_st, c.stream);
+        } else {
+            h->use_cond = 0;
+            upload(d_st, h, c.stream);
+            int chunk = 16;
+            for (;;) {
+                for (int i = 0; i < chunk; ++i) {
+                    R.reliable_update();
+                    R.iteration();
+                }
+                QB_CUDA(cudaGetLastError());
+                download(h, d_st, c.stream);
+                if (h->stop && !h->any_flag) break;
+                chunk = std::min(chunk * 2, 256);
+            }
+        }
+        // systems stopped by the iteration cap: one last reliable update
+        // folds x_s into x and measures their true residual
+        if (h->active_mask && !h->nonfinite) {
+            h->flag_mask = h->active_mask;
+            for (int k = 0; k < h->nsys; ++k) h->sys[k].flag = h->sys[k].active;
+            h->any_flag = 1;
+            h->use_cond = 0;
+            upload(d_st, h, c.stream);
+            R.reliable_update();
+            download(h, d_st, c.stream);
+        }
+    }
+    if (h->nonfinite) throw Error("batch: non-finite residual");
+    store(f, tabs[2], h, mem);
+    sync_check();
+    c.stats = Stats{};
+    c.stats.iterations = h->iteration;
+    for (int k = 0; k < h->nsys; ++k) c.stats.reliable_updates += h->sys[k].reliable_updates;
+}
+
 void free_batch_links(QPHIX_B200_Batch &B)
 {
     for (auto &L : B.lats) {
@@ -932,182 +1114,63 @@ static int batch_invert(QPHIX_info_t *info, QPHIX_B200_Batch *B, QPHIX_invert_ar
     }
     info->final_sec = wall_seconds();
     const int cb = inv->parity == QPHIX_EVEN ? 0 : 1;
-
-    // segments: the systems of each lattice in chunks of 32, 16, ..., 1
-    std::vector<SegPlan> plan;
-    std::vector<int> slot_of(nsys);
-    int sys = 0;
-    for (int l = 0; l < (int)B->lats.size(); ++l) {
-        std::vector<int> mine;
-        for (int k = 0; k < nsys; ++k)
-            if (lat[k] == l) mine.push_back(k);
-        size_t pos = 0;
-        while (pos < mine.size()) {
-            int n = kBMaxRhs;
-            while (n > (int)(mine.size() - pos)) n >>= 1;
-            SegPlan p{l, n, sys, {}};
-            for (int r = 0; r < n; ++r) {
-                p.user.push_back(mine[pos + r]);
-                slot_of[mine[pos + r]] = sys + r;
-            }
-            sys += n;
-            pos += n;
-            plan.push_back(p);
-        }
-    }
-
-    const BTable tabs[3] = {make_table(plan, *B, 0), make_table(plan, *B, 1), make_table(plan, *B, 2)};
-    long long ncx = 0;
-    for (const auto &p : plan) ncx += 3LL * B->lats[p.lat].g.vh * p.nrhs;
-
-    BatchMem mem;
-    BTable *d_tabs = static_cast<BTable *>(mem.get(sizeof(tabs)));
-    BState *d_st = static_cast<BState *>(mem.get(sizeof(BState)));
-    BFields f{};
-    void *mem64 = mem.get((size_t)ncx * 16 * 3);
-    void *mem32 = mem.get((size_t)ncx * 8 * 5);
-    f.x = static_cast<double2 *>(mem64);
-    f.b = f.x + ncx;
-    f.t64 = f.b + ncx;
-    f.xs = static_cast<float2 *>(mem32);
-    f.r = f.xs + ncx;
-    f.p = f.r + ncx;
-    f.ap = f.p + ncx;
-    f.t32 = f.ap + ncx;
-    QB_CUDA(cudaMemsetAsync(mem64, 0, (size_t)ncx * 16 * 3, c.stream));
-    QB_CUDA(cudaMemsetAsync(mem32, 0, (size_t)ncx * 8 * 5, c.stream));
-    QB_CUDA(cudaMemcpyAsync(d_tabs, tabs, sizeof(tabs), cudaMemcpyHostToDevice, c.stream));
-
-    static int rb_s0 = 0, rb_s1, rb_d0, rb_d1, rb_v[5];
-    if (!rb_s0) {
-        rb_s1 = resident_blocks(k_bdslash_s<true>);
-        rb_d0 = resident_blocks(k_bdslash_d<false>);
-        rb_d1 = resident_blocks(k_bdslash_d<true>);
-        rb_v[0] = resident_blocks(k_bvec<0>);
-        rb_v[1] = resident_blocks(k_bvec<1>);
-        rb_v[2] = resident_blocks(k_bvec<2>);
-        rb_v[3] = resident_blocks(k_bvec<3>);
-        rb_v[4] = resident_blocks(k_bvec<4>);
-        rb_s0 = resident_blocks(k_bdslash_s<false>);
-    }
-    auto grid = [](int res_blocks, int ntiles) { return std::max(1, std::min(res_blocks, ntiles)); };
-    BatchRun R{};
-    R.tab_s = d_tabs;
-    R.tab_d = d_tabs + 1;
-    R.tab_v = d_tabs + 2;
-    R.grid_s0 = grid(rb_s0, tabs[0].ntiles);
-    R.grid_s1 = grid(rb_s1, tabs[0].ntiles);
-    R.grid_d0 = grid(rb_d0, tabs[1].ntiles);
-    R.grid_d1 = grid(rb_d1, tabs[1].ntiles);
-    for (int i = 0; i < 5; ++i) R.grid_v[i] = grid(rb_v[i], tabs[2].ntiles);
-    const int gmax = std::max({R.grid_s1, R.grid_d1, R.grid_v[0], R.grid_v[1]});
-    R.partials = static_cast<double *>(mem.get(sizeof(double) * kBMaxSys * gmax));
-    R.st = d_st;
-    R.f = f;
-    R.cb = cb;
-    R.other = 1 - cb;
-    R.stream = c.stream;
-
-    // sources and initial guesses (parity cb of the raw vectors)
-    for (size_t s = 0; s < plan.size(); ++s) {
-        const SegPlan &p = plan[s];
-        const Geom &g = B->lats[p.lat].g;
-        const size_t n = (size_t)6 * g.vh;
-        double *sb = static_cast<double *>(mem.get(sizeof(double) * n * 2 * p.nrhs));
-        for (int r = 0; r < p.nrhs; ++r) {
-            const int k = p.user[r];
-            double *bk = sb + 2 * n * r, *xk = bk + n;
-            QB_CUDA(cudaMemcpyAsync(bk, in[k] + cb * n, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
-            QB_CUDA(cudaMemcpyAsync(xk, out[k] + cb * n, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
-            k_b_from_raw<<<grid_for(g.vh), kBlock, 0, c.stream>>>(f.b, tabs[2].seg[s].voff, g.vh, p.nrhs, r, bk);
-            k_b_from_raw<<<grid_for(g.vh), kBlock, 0, c.stream>>>(f.x, tabs[2].seg[s].voff, g.vh, p.nrhs, r, xk);
-        }
-    }
-
-    BState *h = pinned_state();
-    std::memset(h, 0, sizeof(BState));
-    h->nsys = sys;
-    h->delta2 = c.reliable_delta * c.reliable_delta;
-    h->iter_cap = std::max(1, inv->max * inv->nrestart);
+    std::vector<int> slot_of;
+    const std::vector<SegPlan> plan = plan_segments((int)B->lats.size(), nsys, lat, slot_of);
+    std::vector<LatRef> lats;
+    for (const auto &L : B->lats) lats.push_back(LatRef{&L.g, &L.l64, &L.l32});
+    std::vector<double> m4(nsys), rs(nsys);
     for (int k = 0; k < nsys; ++k) {
-        BSys &y = h->sys[slot_of[k]];
-        y.m4 = 4.0 * mass[k] * mass[k];
-        y.resid = res[k]->resid;
+        m4[slot_of[k]] = 4.0 * mass[k] * mass[k];
+        rs[slot_of[k]] = res[k]->resid;
     }
-    upload(d_st, h, c.stream);
-    k_bvec<kBNormB><<<R.grid_v[kBNormB], kBlock, 0, c.stream>>>(R.tab_v, d_st, f, R.partials);
-    QB_CUDA(cudaGetLastError());
-    download(h, d_st, c.stream);
-
-    if (!h->stop) {
-        if (batch_graphs_enabled()) {
-            BatchGraph G;
-            G.build(R);
-            h->use_cond = 1;
-            h->cond_loop = G.hloop;
-            h->cond_ru = G.hru;
-            upload(d_st, h, c.stream);
-            QB_CUDA(cudaGraphLaunch(G.exec, c.stream));
-            download(h, d_st, c.stream);
-        } else {
-            h->use_cond = 0;
-            upload(d_st, h, c.stream);
-            int chunk = 16;
-            for (;;) {
-                for (int i = 0; i < chunk; ++i) {
-                    R.reliable_update();
-                    R.iteration();
-                }
-                QB_CUDA(cudaGetLastError());
-                download(h, d_st, c.stream);
-                if (h->stop && !h->any_flag) break;
-                chunk = std::min(chunk * 2, 256);
-            }
-        }
-        // systems stopped by the iteration cap: one last reliable update
-        // folds x_s into x and measures their true residual
-        if (h->active_mask && !h->nonfinite) {
-            h->flag_mask = h->active_mask;
-            for (int k = 0; k < h->nsys; ++k) h->sys[k].flag = h->sys[k].active;
-            h->any_flag = 1;
-            h->use_cond = 0;
-            upload(d_st, h, c.stream);
-            R.reliable_update();
-            download(h, d_st, c.stream);
-        }
-    }
-    if (h->nonfinite) throw Error("batch_invert: non-finite residual");
-
-    // solutions back into the callers' raw arrays
     int max_iter = 0;
     double flops = 0;
-    for (size_t s = 0; s < plan.size(); ++s) {
-        const SegPlan &p = plan[s];
-        const Geom &g = B->lats[p.lat].g;
-        const size_t n = (size_t)6 * g.vh;
-        double *stage = static_cast<double *>(mem.get(sizeof(double) * n));
-        for (int r = 0; r < p.nrhs; ++r) {
-            const int k = p.user[r];
-            const BSys &y = h->sys[p.sys0 + r];
-            k_b_to_raw<<<grid_for(g.vh), kBlock, 0, c.stream>>>(stage, f.x, tabs[2].seg[s].voff, g.vh, p.nrhs, r);
-            QB_CUDA(cudaMemcpyAsync(out[k] + cb * n, stage, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
-            sync_check();
-            res[k]->final_rsq = y.bnorm > 0 ? y.true_rsq / y.bnorm : 0.0;
-            res[k]->size_r = res[k]->final_rsq;
-            res[k]->final_rel = 0;
-            res[k]->size_relr = 0;
-            res[k]->final_iter = y.iterations;
-            res[k]->final_restart = y.reliable_updates;
-            max_iter = std::max(max_iter, y.iterations);
-            flops += 1187.0 * y.iterations * 2.0 * g.vh;
-        }
-    }
+    run_batch(
+        lats, plan, nsys, m4.data(), rs.data(), cb, inv->max * inv->nrestart,
+        [&](const BFields &f, const BTable &vt, BatchMem &mem) {
+            // sources and initial guesses: parity cb of the callers' raw vectors
+            for (size_t s = 0; s < plan.size(); ++s) {
+                const SegPlan &p = plan[s];
+                const Geom &g = *lats[p.lat].g;
+                const size_t n = (size_t)6 * g.vh;
+                double *sb = static_cast<double *>(mem.get(sizeof(double) * n * 2 * p.nrhs));
+                for (int r = 0; r < p.nrhs; ++r) {
+                    const int k = p.user[r];
+                    double *bk = sb + 2 * n * r, *xk = bk + n;
+                    QB_CUDA(cudaMemcpyAsync(bk, in[k] + cb * n, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+                    QB_CUDA(cudaMemcpyAsync(xk, out[k] + cb * n, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+                    k_b_from_raw<<<grid_for(g.vh), kBlock, 0, c.stream>>>(f.b, vt.seg[s].voff, g.vh, p.nrhs, r, bk);
+                    k_b_from_raw<<<grid_for(g.vh), kBlock, 0, c.stream>>>(f.x, vt.seg[s].voff, g.vh, p.nrhs, r, xk);
+                }
+            }
+        },
+        [&](const BFields &f, const BTable &vt, const BState *h, BatchMem &mem) {
+            for (size_t s = 0; s < plan.size(); ++s) {
+                const SegPlan &p = plan[s];
+                const Geom &g = *lats[p.lat].g;
+                const size_t n = (size_t)6 * g.vh;
+                double *stage = static_cast<double *>(mem.get(sizeof(double) * n));
+                for (int r = 0; r < p.nrhs; ++r) {
+                    const int k = p.user[r];
+                    const BSys &y = h->sys[p.sys0 + r];
+                    k_b_to_raw<<<grid_for(g.vh), kBlock, 0, c.stream>>>(stage, f.x, vt.seg[s].voff, g.vh, p.nrhs, r);
+                    QB_CUDA(cudaMemcpyAsync(out[k] + cb * n, stage, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                            c.stream));
+                    sync_check();
+                    res[k]->final_rsq = y.bnorm > 0 ? y.true_rsq / y.bnorm : 0.0;
+                    res[k]->size_r = res[k]->final_rsq;
+                    res[k]->final_rel = 0;
+                    res[k]->size_relr = 0;
+                    res[k]->final_iter = y.iterations;
+                    res[k]->final_restart = y.reliable_updates;
+                    max_iter = std::max(max_iter, y.iterations);
+                    flops += 1187.0 * y.iterations * 2.0 * g.vh;
+                }
+            }
+        });
     info->final_sec = wall_seconds() - info->final_sec;
     info->final_flop = flops;
     info->status = QPHIX_SUCCESS;
-    c.stats = Stats{};
-    c.stats.iterations = h->iteration;
-    for (int k = 0; k < h->nsys; ++k) c.stats.reliable_updates += h->sys[k].reliable_updates;
     return max_iter;
 }
 

@@ -80,7 +80,7 @@ struct Context {
     cudaEvent_t ev_user[2] = {nullptr, nullptr};
     // settings (qphix_b200.h)
     int inner_mode = QPHIX_B200_PREC_DOUBLE;  // QPHIX_B200_precision_t of D3 solves
-    double reliable_delta = 0.1;
+    double reliable_delta = 0.2;
     int kernel_timing = 0;
     int max_chunk = 64;
     int verbose = 0;
