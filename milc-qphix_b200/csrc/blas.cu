@@ -8,6 +8,8 @@
 // in its fptype; here every reduction accumulates in FP64 and the step sizes
 // are rounded to the solve precision exactly where the reference assigns
 // them to an fptype variable.
+#include <climits>
+
 #include "device_common.cuh"
 
 namespace qb {
@@ -201,6 +203,13 @@ k_ms_residual(VecView<S> r, VecView<S> ttt, SolverState *st, double *partials, i
                                                  st->beta_i[k], single) / zb, single);
             else { st->alpha[k] = 0.0; st->finished[k] = 1; }
         }
+        if (st->shift_stop > 0.0) {
+            for (int k = 0; k < st->num_now; ++k) {
+                if (k == jl || st->shift_done_at[k] != INT_MAX) continue;
+                const double z = st->zeta_ip1[k];
+                if (z * z * rsq <= st->shift_stop) st->shift_done_at[k] = st->iteration;
+            }
+        }
         if (st->iteration >= st->max_cg || run_guard(st)) stop_run(st, gate);
     });
 }
@@ -215,12 +224,15 @@ k_ms_update(VecBlock *xs, VecBlock *ps, VecView<S> r, int n, SolverState *st, in
     using AX = typename Acc<X>::type;
     if (gated_off(st, gate)) return;
     __shared__ double sb[kMaxShifts], sz[kMaxShifts], sa[kMaxShifts];
+    __shared__ int sd[kMaxShifts];
     const int nn = st->num_now;
     const bool conv = st->converged;
+    const int it = st->iteration;
     for (int k = threadIdx.x; k < nn; k += blockDim.x) {
         sb[k] = st->beta_i[k];
         sz[k] = st->zeta_ip1[k];
         sa[k] = st->alpha[k];
+        sd[k] = st->shift_done_at[k];
     }
     __syncthreads();
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -228,6 +240,9 @@ k_ms_update(VecBlock *xs, VecBlock *ps, VecView<S> r, int n, SolverState *st, in
     A rv[6];
     if (!conv) r.load_cg(j, rv);
     for (int k = 0; k < nn; ++k) {
+        // a shift that reached its sloppy tolerance gets its last x update in
+        // that iteration and is left alone afterwards
+        if (sd[k] < it) continue;
         VecView<S> pk = view<S>(ps[k], r.vh);
         VecView<X> xk = view<X>(xs[k], r.vh);
         A p[6];
@@ -238,7 +253,7 @@ k_ms_update(VecBlock *xs, VecBlock *ps, VecView<S> r, int n, SolverState *st, in
 #pragma unroll
         for (int i = 0; i < 6; ++i) xv[i] = xv[i] + bk * (AX)p[i];
         xk.store(j, xv);
-        if (!conv) {
+        if (!conv && sd[k] != it) {
             const A ak = (A)sa[k];
             const double zk = sz[k];
 #pragma unroll

@@ -122,6 +122,11 @@ struct SolverState {
     double zeta_i[kMaxShifts], zeta_im1[kMaxShifts], zeta_ip1[kMaxShifts];
     double beta_i[kMaxShifts], beta_im1[kMaxShifts], alpha[kMaxShifts];
     int finished[kMaxShifts];
+    // mixed multi-shift (sloppy phase): shift k stops being updated after the
+    // iteration shift_done_at[k] at which its residual zeta_k^2 |r|^2 fell to
+    // shift_stop (0: never; the reference recurrence updates every shift)
+    double shift_stop;
+    int shift_done_at[kMaxShifts];
 };
 
 // ----------------------------------------------------------------------------
