@@ -300,18 +300,31 @@ __device__ __forceinline__ void bsite(const BSeg &sg, int cb, int j, int q, cons
     for (int e = 0; e < G; ++e)
 #pragma unroll
         for (int i = 0; i < 6; ++i) acc[e][i] = 0.f;
+    // A forward/backward pair is 9 float4 chunks (18 complex); the forward
+    // matrix is in chunks 0-4 and the backward one in chunks 4-8 (chunk 4
+    // holds the last forward and the first backward complex).  Loading five
+    // chunks per matrix keeps 20 link floats live instead of 36, which leaves
+    // registers for the G right-hand sides.
 #pragma unroll
     for (int d = 0; d < 4; ++d) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            float u[36], v[G][6];
-            lv.load_pair(d, h, j, u);
-            bload<G>(in, sg.g.vh, sg.nrhs, neighbor(sg.g, s, 8 * h + 2 * d + 1), q, v);
+            const float4 *pair = lv.p + ((size_t)d * 18 + 9 * h) * lv.vh + j;
 #pragma unroll
-            for (int e = 0; e < G; ++e) mv_add(acc[e], u, v[e]);
-            bload<G>(in, sg.g.vh, sg.nrhs, neighbor(sg.g, s, 8 * h + 2 * d), q, v);
+            for (int half = 0; half < 2; ++half) {
+                float w[20], v[G][6];
 #pragma unroll
-            for (int e = 0; e < G; ++e) mv_adj_sub(acc[e], u + 18, v[e]);
+                for (int c = 0; c < 5; ++c) {
+                    const float4 z = __ldcs(pair + (size_t)(4 * half + c) * lv.vh);
+                    w[4 * c] = z.x; w[4 * c + 1] = z.y; w[4 * c + 2] = z.z; w[4 * c + 3] = z.w;
+                }
+                bload<G>(in, sg.g.vh, sg.nrhs, neighbor(sg.g, s, 8 * h + 2 * d + (half ? 0 : 1)), q, v);
+#pragma unroll
+                for (int e = 0; e < G; ++e) {
+                    if (half) mv_adj_sub(acc[e], w + 2, v[e]);
+                    else mv_add(acc[e], w, v[e]);
+                }
+            }
         }
     }
 }
@@ -375,8 +388,10 @@ __device__ __forceinline__ void bdslash_s_item(int item, int cb, float2 *out, co
     bstore<G>(out + sg.voff, sg.g.vh, sg.nrhs, j, q, a);
 }
 
-template <bool MDAGM>
-__global__ void __launch_bounds__(kBlock, 2) k_bdslash_s(const BTable *tab, BState *st, float2 *out,
+// GMAX: largest G of the table's segments.  With G <= 2 the kernel fits in
+// 80 registers (3 blocks of 256 per SM); G = 3, 4 need 128 (2 blocks).
+template <bool MDAGM, int GMAX>
+__global__ void __launch_bounds__(kBlock, GMAX <= 2 ? 3 : 2) k_bdslash_s(const BTable *tab, BState *st, float2 *out,
                                                          const float2 *in, const float2 *pv, int cb,
                                                          double *partials)
 {
@@ -401,12 +416,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_bdslash_s(const BTable *tab, BSta
         }
         const int item = (t - sh.seg.tile0) * kBlock + threadIdx.x;
         if (item < sh.seg.items) {
-            switch (sh.seg.G) {
-            case 4: bdslash_s_item<4, MDAGM>(item, cb, out, in, pv, sh, acc); break;
-            case 3: bdslash_s_item<3, MDAGM>(item, cb, out, in, pv, sh, acc); break;
-            case 2: bdslash_s_item<2, MDAGM>(item, cb, out, in, pv, sh, acc); break;
-            default: bdslash_s_item<1, MDAGM>(item, cb, out, in, pv, sh, acc); break;
+            if constexpr (GMAX > 2) {
+                if (sh.seg.G == 4) bdslash_s_item<4, MDAGM>(item, cb, out, in, pv, sh, acc);
+                else if (sh.seg.G == 3) bdslash_s_item<3, MDAGM>(item, cb, out, in, pv, sh, acc);
             }
+            if (sh.seg.G == 2) bdslash_s_item<2, MDAGM>(item, cb, out, in, pv, sh, acc);
+            else if (sh.seg.G == 1) bdslash_s_item<1, MDAGM>(item, cb, out, in, pv, sh, acc);
         }
     }
     if constexpr (MDAGM) {
@@ -762,7 +777,9 @@ std::vector<SegPlan> plan_segments(int nlat, int nsys, const int *lat, std::vect
     return plan;
 }
 
-// kind 0: FP32 Dslash (G <= 4), 1: FP64 Dslash (G <= 3), 2: vector kernels
+// kind 0: FP32 Dslash (G = 3 for multiples of 3, else <= 4; measured: G = 4
+// at 2 blocks/SM beats G = 2 at 3 blocks/SM by 4-5 %), 1: FP64 Dslash (G = 3
+// for multiples of 3, else <= 2), 2: vector kernels
 BTable make_table(const std::vector<SegPlan> &plan, const std::vector<LatRef> &lats, int kind)
 {
     BTable t{};
@@ -816,6 +833,7 @@ bool batch_graphs_enabled()
 struct BatchRun {
     const BTable *tab_s, *tab_d, *tab_v;
     int grid_s0, grid_s1, grid_d0, grid_d1, grid_v[5];
+    int gmax_s;  // largest right-hand sides per thread of the FP32 Dslash table
     BState *st;
     BFields f;
     double *partials;
@@ -833,8 +851,13 @@ struct BatchRun {
     // K1..K4: one FP32 CG iteration of every active system
     void iteration() const
     {
-        k_bdslash_s<false><<<grid_s0, kBlock, 0, stream>>>(tab_s, st, f.t32, f.p, f.p, other, partials);
-        k_bdslash_s<true><<<grid_s1, kBlock, 0, stream>>>(tab_s, st, f.ap, f.t32, f.p, cb, partials);
+        if (gmax_s > 2) {
+            k_bdslash_s<false, 4><<<grid_s0, kBlock, 0, stream>>>(tab_s, st, f.t32, f.p, f.p, other, partials);
+            k_bdslash_s<true, 4><<<grid_s1, kBlock, 0, stream>>>(tab_s, st, f.ap, f.t32, f.p, cb, partials);
+        } else {
+            k_bdslash_s<false, 2><<<grid_s0, kBlock, 0, stream>>>(tab_s, st, f.t32, f.p, f.p, other, partials);
+            k_bdslash_s<true, 2><<<grid_s1, kBlock, 0, stream>>>(tab_s, st, f.ap, f.t32, f.p, cb, partials);
+        }
         k_bvec<kBUpdate><<<grid_v[kBUpdate], kBlock, 0, stream>>>(tab_v, st, f, partials);
         k_bvec<kBAxpy><<<grid_v[kBAxpy], kBlock, 0, stream>>>(tab_v, st, f, partials);
     }
@@ -949,9 +972,13 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
     QB_CUDA(cudaMemsetAsync(mem32, 0, (size_t)ncx * 8 * 5, c.stream));
     QB_CUDA(cudaMemcpyAsync(d_tabs, tabs, sizeof(tabs), cudaMemcpyHostToDevice, c.stream));
 
-    static int rb_s0 = 0, rb_s1, rb_d0, rb_d1, rb_v[5];
+    int gmax_s = 1;
+    for (int s = 0; s < tabs[0].nseg; ++s) gmax_s = std::max(gmax_s, tabs[0].seg[s].G);
+    static int rb_s0 = 0, rb_s1, rb_s0w, rb_s1w, rb_d0, rb_d1, rb_v[5];
     if (!rb_s0) {
-        rb_s1 = resident_blocks(k_bdslash_s<true>);
+        rb_s1 = resident_blocks(k_bdslash_s<true, 2>);
+        rb_s0w = resident_blocks(k_bdslash_s<false, 4>);
+        rb_s1w = resident_blocks(k_bdslash_s<true, 4>);
         rb_d0 = resident_blocks(k_bdslash_d<false>);
         rb_d1 = resident_blocks(k_bdslash_d<true>);
         rb_v[0] = resident_blocks(k_bvec<0>);
@@ -959,15 +986,16 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
         rb_v[2] = resident_blocks(k_bvec<2>);
         rb_v[3] = resident_blocks(k_bvec<3>);
         rb_v[4] = resident_blocks(k_bvec<4>);
-        rb_s0 = resident_blocks(k_bdslash_s<false>);
+        rb_s0 = resident_blocks(k_bdslash_s<false, 2>);
     }
     auto grid = [](int res_blocks, int ntiles) { return std::max(1, std::min(res_blocks, ntiles)); };
     BatchRun R{};
     R.tab_s = d_tabs;
     R.tab_d = d_tabs + 1;
     R.tab_v = d_tabs + 2;
-    R.grid_s0 = grid(rb_s0, tabs[0].ntiles);
-    R.grid_s1 = grid(rb_s1, tabs[0].ntiles);
+    R.gmax_s = gmax_s;
+    R.grid_s0 = grid(gmax_s > 2 ? rb_s0w : rb_s0, tabs[0].ntiles);
+    R.grid_s1 = grid(gmax_s > 2 ? rb_s1w : rb_s1, tabs[0].ntiles);
     R.grid_d0 = grid(rb_d0, tabs[1].ntiles);
     R.grid_d1 = grid(rb_d1, tabs[1].ntiles);
     for (int i = 0; i < 5; ++i) R.grid_v[i] = grid(rb_v[i], tabs[2].ntiles);

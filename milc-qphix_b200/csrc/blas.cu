@@ -9,6 +9,7 @@
 // are rounded to the solve precision exactly where the reference assigns
 // them to an fptype variable.
 #include <climits>
+#include <type_traits>
 
 #include "device_common.cuh"
 
@@ -160,6 +161,111 @@ __global__ void __launch_bounds__(kBlock) k_cg_axpy(VecView<S> r, VecView<S> pv,
     pv.store(j, p);
 }
 
+// end of an inner iteration of the mixed CG (one thread): b, and whether
+// to stop for a reliable update
+__device__ __forceinline__ void mx_finish(SolverState *st, double rsq, int gate, double delta2)
+{
+    const double oldrsq = st->rsq;
+    st->oldrsq = oldrsq;
+    st->rsq = rsq;
+    st->b = rsq / oldrsq;
+    bool stalled = false;
+    if (rsq < st->ru_best) {
+        st->ru_best = rsq;
+        st->ru_best_iter = st->iteration;
+    } else if (st->ru_stall_window > 0 && st->iteration - st->ru_best_iter >= st->ru_stall_window) {
+        stalled = true;
+        st->ru_stalled = 1;
+    }
+    const bool ru = (rsq < delta2 * st->rsq_ru) || (rsq <= st->rsqstop) || stalled ||
+                    (st->iteration >= st->max_cg) || !(rsq == rsq) || run_guard(st);
+    if (ru) {
+        st->skip_axpy = 1;  // this iteration's p update waits for the true residual
+        stop_run(st, gate);
+    }
+}
+
+// ------------------------------------------- flat vectorised p / x, r updates --
+// In FP32 and FP64 a parity block is one contiguous array of 6 Vh reals
+// (component-major), so the element-wise updates of the inner CG need no
+// site structure: each thread moves two 16-byte words per vector, half the
+// array apart (both halves coalesced), which doubles the bytes in flight of
+// the per-site kernels above.  Same arithmetic, element by element.
+template <typename R> struct Wide;
+template <> struct Wide<float> { using type = float4; static constexpr int n = 4; };
+template <> struct Wide<double> { using type = double2; static constexpr int n = 2; };
+
+template <typename R>
+__device__ __forceinline__ void wide_get(const typename Wide<R>::type &w, R v[Wide<R>::n]);
+template <> __device__ __forceinline__ void wide_get<float>(const float4 &w, float v[4])
+{
+    v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
+}
+template <> __device__ __forceinline__ void wide_get<double>(const double2 &w, double v[2])
+{
+    v[0] = w.x; v[1] = w.y;
+}
+__device__ __forceinline__ float4 wide_make(const float v[4]) { return make_float4(v[0], v[1], v[2], v[3]); }
+__device__ __forceinline__ double2 wide_make(const double v[2]) { return make_double2(v[0], v[1]); }
+
+// p = r + b p
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_axpy_flat(const typename Wide<R>::type *r, typename Wide<R>::type *p,
+                                                      long long n, SolverState *st, int gate)
+{
+    if (gated_off(st, gate)) return;
+    if (st->skip_axpy) return;  // p update redone by the host after a reliable update
+    constexpr int W = Wide<R>::n;
+    const long long half = (n + 1) / 2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const R b = (R)st->b;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const long long i = t + k * half;
+        if (t >= half || i >= n) continue;
+        R rv[W], pv[W];
+        wide_get<R>(__ldcg(r + i), rv);
+        wide_get<R>(__ldcg(p + i), pv);
+#pragma unroll
+        for (int e = 0; e < W; ++e) pv[e] = rv[e] + b * pv[e];
+        p[i] = wide_make(pv);
+    }
+}
+
+// x += a p; r += a ttt; |r|^2 -> the reliable-update decision of k_mx_update
+template <typename R>
+__global__ void __launch_bounds__(kBlock)
+k_mx_update_flat(typename Wide<R>::type *x, const typename Wide<R>::type *p, typename Wide<R>::type *r,
+                 const typename Wide<R>::type *ttt, long long n, SolverState *st, double *partials, int gate,
+                 double delta2)
+{
+    if (gated_off(st, gate)) return;
+    constexpr int W = Wide<R>::n;
+    const long long half = (n + 1) / 2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const R a = (R)st->a;
+    double s[1] = {0.0};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const long long i = t + k * half;
+        if (t >= half || i >= n) continue;
+        R xv[W], pv[W], rv[W], tv[W];
+        wide_get<R>(__ldcg(x + i), xv);
+        wide_get<R>(__ldcg(p + i), pv);
+        wide_get<R>(__ldcg(r + i), rv);
+        wide_get<R>(__ldcg(ttt + i), tv);
+#pragma unroll
+        for (int e = 0; e < W; ++e) {
+            xv[e] = xv[e] + a * pv[e];
+            rv[e] = rv[e] + a * tv[e];
+            s[0] += (double)(rv[e] * rv[e]);
+        }
+        x[i] = wide_make(xv);
+        r[i] = wide_make(rv);
+    }
+    grid_reduce<1>(s, partials, &st->counter, [&](const double *tot) { mx_finish(st, tot[0], gate, delta2); });
+}
+
 // ------------------------------------------------------------ multi-shift --
 // calc_rsq2 (ks_multicg_offset.cpp:124-140) + the convergence test (:520)
 // + the alpha recurrences (:587-598), evaluated on the device.
@@ -271,6 +377,7 @@ k_ms_update(VecBlock *xs, VecBlock *ps, VecView<S> r, int n, SolverState *st, in
 // reliable update when |r_s|^2 < delta^2 |r_RU|^2 or the sloppy residual
 // passes the target.  The request cancels this iteration's p update, which the
 // host redoes with the true residual.
+
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
 k_mx_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverState *st,
@@ -297,27 +404,7 @@ k_mx_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverSta
 #pragma unroll
         for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
     }
-    grid_reduce<1>(s, partials, &st->counter, [&](const double *t) {
-        const double oldrsq = st->rsq;
-        const double rsq = t[0];
-        st->oldrsq = oldrsq;
-        st->rsq = rsq;
-        st->b = rsq / oldrsq;
-        bool stalled = false;
-        if (rsq < st->ru_best) {
-            st->ru_best = rsq;
-            st->ru_best_iter = st->iteration;
-        } else if (st->ru_stall_window > 0 && st->iteration - st->ru_best_iter >= st->ru_stall_window) {
-            stalled = true;
-            st->ru_stalled = 1;
-        }
-        const bool ru = (rsq < delta2 * st->rsq_ru) || (rsq <= st->rsqstop) || stalled ||
-                        (st->iteration >= st->max_cg) || !(rsq == rsq) || run_guard(st);
-        if (ru) {
-            st->skip_axpy = 1;  // this iteration's p update waits for the true residual
-            stop_run(st, gate);
-        }
-    });
+    grid_reduce<1>(s, partials, &st->counter, [&](const double *t) { mx_finish(st, t[0], gate, delta2); });
 }
 
 // -------------------------------------------------------------- elementwise --
@@ -408,7 +495,15 @@ template <typename S>
 static void axpy_impl(const Launch &L, VecBlock r, VecBlock pv, SolverState *st, int gate)
 {
     const int vh = L.g->vh;
-    k_cg_axpy<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(r, vh), view<S>(pv, vh), st, gate);
+    if constexpr (std::is_same<S, __half>::value) {
+        k_cg_axpy<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(r, vh), view<S>(pv, vh), st, gate);
+    } else {
+        using V = typename Wide<S>::type;
+        const long long n = 6LL * vh / Wide<S>::n;
+        const int grid = (int)(((n + 1) / 2 + kBlock - 1) / kBlock);
+        k_axpy_flat<S><<<grid, kBlock, 0, L.stream>>>(static_cast<const V *>(r.data), static_cast<V *>(pv.data), n,
+                                                      st, gate);
+    }
 }
 
 void cg_axpy(Prec p, const Launch &L, VecBlock r, VecBlock pv, SolverState *st, int gate)
@@ -450,8 +545,17 @@ static void mx_impl(const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlo
                     double *partials, int gate, double delta2)
 {
     const int vh = L.g->vh;
-    k_mx_update<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(x, vh), view<S>(pv, vh), view<S>(r, vh),
-                                                          view<S>(ttt, vh), st, partials, gate, delta2);
+    if constexpr (std::is_same<S, __half>::value) {
+        k_mx_update<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(x, vh), view<S>(pv, vh), view<S>(r, vh),
+                                                              view<S>(ttt, vh), st, partials, gate, delta2);
+    } else {
+        using V = typename Wide<S>::type;
+        const long long n = 6LL * vh / Wide<S>::n;
+        const int grid = (int)(((n + 1) / 2 + kBlock - 1) / kBlock);
+        k_mx_update_flat<S><<<grid, kBlock, 0, L.stream>>>(static_cast<V *>(x.data), static_cast<const V *>(pv.data),
+                                                           static_cast<V *>(r.data), static_cast<const V *>(ttt.data),
+                                                           n, st, partials, gate, delta2);
+    }
 }
 
 void mx_update(Prec p, const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlock ttt,

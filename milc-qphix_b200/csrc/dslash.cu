@@ -528,12 +528,101 @@ int dslash_variant(Prec pv, Prec pl, float us[3])
     return t.vh < 0 ? -1 : t.variant;
 }
 
+
+template <typename SV, typename SL>
+static void launch_mdagm_variant(int variant, const DslashArgs<SV, SL> &a, const LinkSet &ls, VecView<SV> pv,
+                                 double m4, int cb, SolverState *st, double *partials, int gate, int mode,
+                                 const Launch &L)
+{
+    if (variant == 1) {
+        k_dslash_mdagm<SV, SL><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, pv, m4, st, partials, gate, mode);
+    } else if (variant == 2) {
+        k_dslash_tma<SV, SL, 1><<<tma_grid<SV, SL, 1>(L.g->vh), TmaCfg<SL>::T, tma_smem_bytes<SL>(), L.stream>>>(
+            a, static_cast<const char *>(ls.blk[cb]), pv, m4, st, partials, gate, mode, L.err);
+    } else {
+        k_dslash_mdagm<SV, SL><<<resident_grid(k_dslash_mdagm<SV, SL>, L.g->vh), kBlock, 0, L.stream>>>(
+            a, pv, m4, st, partials, gate, mode);
+    }
+}
+
+// The fused M^dag M kernel (K2) is tuned on its own: its grid-wide reduction
+// favours fewer, longer-lived blocks more than the plain Dslash does.
+static TuneEntry g_tune_mdagm[3][3];
+
+template <typename SV, typename SL>
+static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV, SL> &a, const LinkSet &ls,
+                               int cb)
+{
+    const int f = forced_variant();
+    if (f >= 0) return f;
+    TuneEntry &t = g_tune_mdagm[(int)pv][(int)pl];
+    if (t.vh == L.g->vh) return t.variant;
+    // scratch vectors, solver state and partials: no caller data is touched
+    const size_t cx = pv == Prec::Double ? 16 : (pv == Prec::Single ? 8 : 4);
+    void *vin = nullptr, *vout = nullptr, *vp = nullptr;
+    float *nin = nullptr, *nout = nullptr, *np = nullptr;
+    SolverState *st = nullptr;
+    double *part = nullptr;
+    cudaMallocAsync(&vin, 3 * cx * L.g->vh, L.stream);
+    cudaMallocAsync(&vout, 3 * cx * L.g->vh, L.stream);
+    cudaMallocAsync(&vp, 3 * cx * L.g->vh, L.stream);
+    cudaMemsetAsync(vin, 0, 3 * cx * L.g->vh, L.stream);
+    cudaMemsetAsync(vp, 0, 3 * cx * L.g->vh, L.stream);
+    if (pv == Prec::Half) {
+        cudaMallocAsync(&nin, sizeof(float) * L.g->vh, L.stream);
+        cudaMallocAsync(&nout, sizeof(float) * L.g->vh, L.stream);
+        cudaMallocAsync(&np, sizeof(float) * L.g->vh, L.stream);
+        cudaMemsetAsync(nin, 0, sizeof(float) * L.g->vh, L.stream);
+        cudaMemsetAsync(np, 0, sizeof(float) * L.g->vh, L.stream);
+    }
+    cudaMallocAsync(&st, sizeof(SolverState), L.stream);
+    cudaMemsetAsync(st, 0, sizeof(SolverState), L.stream);
+    cudaMallocAsync(&part, sizeof(double) * 4 * kMaxPartials, L.stream);
+    DslashArgs<SV, SL> s = a;
+    s.in = view<SV>(VecBlock{vin, nin}, L.g->vh);
+    s.out = view<SV>(VecBlock{vout, nout}, L.g->vh);
+    const VecView<SV> p = view<SV>(VecBlock{vp, np}, L.g->vh);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = 0;
+    for (int v = 0; v < kVariants; ++v) {
+        launch_mdagm_variant<SV, SL>(v, s, ls, p, 0.0, cb, st, part, -1, 0, L);  // warm
+        cudaEventRecord(e0, L.stream);
+        for (int r = 0; r < 3; ++r) launch_mdagm_variant<SV, SL>(v, s, ls, p, 0.0, cb, st, part, -1, 0, L);
+        cudaEventRecord(e1, L.stream);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        t.us[v] = ms * 1e3f / 3;
+        if (t.us[v] < t.us[best]) best = v;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (void *q : {vin, vout, vp, (void *)nin, (void *)nout, (void *)np, (void *)st, (void *)part})
+        if (q) cudaFreeAsync(q, L.stream);
+    t.vh = L.g->vh;
+    t.variant = best;
+    return best;
+}
+
+template <typename SV, typename SL>
+static void launch_mdagm(const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls,
+                         VecBlock pv, double m4, int cb, SolverState *st, double *partials,
+                         int gate, int mode, Prec p)
+{
+    auto a = make_args<SV, SL>(L, ttt, tmp, ls, cb);
+    const int variant = tuned_variant_mdagm<SV, SL>(p, ls.prec, L, a, ls, cb);
+    launch_mdagm_variant<SV, SL>(variant, a, ls, view<SV>(pv, L.g->vh), m4, cb, st, partials, gate, mode, L);
+}
+
 template <typename SV, typename SL>
 static void prepare_impl(Prec pv, const LinkSet &ls, const Launch &L)
 {
     VecBlock none{};
     auto a = make_args<SV, SL>(L, none, none, ls, 0);
     (void)tuned_variant<SV, SL>(pv, ls.prec, L, a, ls, 0);
+    (void)tuned_variant_mdagm<SV, SL>(pv, ls.prec, L, a, ls, 0);
     (void)resident_grid(k_dslash<SV, SL>, L.g->vh);
     (void)resident_grid(k_dslash_mdagm<SV, SL>, L.g->vh);
     (void)tma_grid<SV, SL, 0>(L.g->vh);
@@ -543,25 +632,6 @@ static void prepare_impl(Prec pv, const LinkSet &ls, const Launch &L)
 void dslash_prepare(Prec pv, const LinkSet &ls, const Launch &L)
 {
     QB_DISPATCH_VL(pv, ls.prec, prepare_impl, pv, ls, L);
-}
-
-template <typename SV, typename SL>
-static void launch_mdagm(const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls,
-                         VecBlock pv, double m4, int cb, SolverState *st, double *partials,
-                         int gate, int mode, Prec p)
-{
-    auto a = make_args<SV, SL>(L, ttt, tmp, ls, cb);
-    const int variant = tuned_variant<SV, SL>(p, ls.prec, L, a, ls, cb);
-    if (variant == 1) {
-        k_dslash_mdagm<SV, SL><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, view<SV>(pv, L.g->vh), m4, st,
-                                                                            partials, gate, mode);
-    } else if (variant == 2) {
-        k_dslash_tma<SV, SL, 1><<<tma_grid<SV, SL, 1>(L.g->vh), TmaCfg<SL>::T, tma_smem_bytes<SL>(), L.stream>>>(
-            a, static_cast<const char *>(ls.blk[cb]), view<SV>(pv, L.g->vh), m4, st, partials, gate, mode, L.err);
-    } else {
-        k_dslash_mdagm<SV, SL><<<resident_grid(k_dslash_mdagm<SV, SL>, L.g->vh), kBlock, 0, L.stream>>>(
-            a, view<SV>(pv, L.g->vh), m4, st, partials, gate, mode);
-    }
 }
 
 void dslash_mdagm_dot(Prec p, const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls,
