@@ -1,7 +1,8 @@
 """GPU: batched solves (QPHIX_B200_D3_batch_invert) through the C ABI.
 
 Several lattices of different sizes, several right-hand sides per lattice
-(segments of 4 + 2 + 1 systems), different masses, one device run.  Every
+(segments of 6 + 1, 2 and 1 systems: register groups of G = 3, 2 and 1),
+different masses, one device run.  Every
 system must reach its FP64 true-residual tolerance as measured by the oracle
 (the reference's own host code with the restated Dslash), agree with the
 oracle's FP64 CG solution, and be bit-reproducible run to run.
