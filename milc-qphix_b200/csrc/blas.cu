@@ -316,6 +316,12 @@ k_ms_residual(VecView<S> r, VecView<S> ttt, SolverState *st, double *partials, i
                 if (z * z * rsq <= st->shift_stop) st->shift_done_at[k] = st->iteration;
             }
         }
+        // the iteration completes (its vector updates are not gated off);
+        // the host then replaces r by the FP64 residual of the base shift
+        if (st->ms_delta2 > 0.0 && rsq < st->ms_delta2 * st->rsq_ru) {
+            st->ms_ru = 1;
+            stop_run(st, gate);
+        }
         if (st->iteration >= st->max_cg || run_guard(st)) stop_run(st, gate);
     });
 }

@@ -127,6 +127,11 @@ struct SolverState {
     // shift_stop (0: never; the reference recurrence updates every shift)
     double shift_stop;
     int shift_done_at[kMaxShifts];
+    // mixed multi-shift: the base shift's reliable update is due when its
+    // |r|^2 falls below ms_delta2 * rsq_ru (0: never); ms_ru records that
+    // the device loop stopped for it
+    double ms_delta2;
+    int ms_ru;
 };
 
 // ----------------------------------------------------------------------------

@@ -9,6 +9,7 @@
 // chunk that overshoots costs a few empty launches, never extra arithmetic,
 // and the sequence of arithmetic is exactly the reference's.
 #include <cmath>
+#include <functional>
 
 #include "context.h"
 #include "device_common.cuh"
@@ -577,6 +578,7 @@ namespace {
 
 struct MsPass {
     int iteration = 0;
+    int reliable_updates = 0;
     bool converged = false;
     double rsq = 0, source_norm = 0;
 };
@@ -587,7 +589,9 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
                std::vector<VecBlock> &pm, VecBlock ttt, VecBlock tmp, VecBlock resid, VecBlock *d_x,
                VecBlock *d_p, int parity, const std::vector<double> &shifts, int j_low,
                double offset_low, double rsqmin, int max_cg, bool single, TimedLaunches &tl,
-               double shift_rsqmin)
+               double shift_rsqmin, double ru_delta2 = 0.0,
+               const std::function<double()> &reliable_update = std::function<double()>(),
+               double ru_rsqmin = 0.0)
 {
     Context &c = ctx();
     const Launch L = c.launch();
@@ -622,25 +626,46 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
     S.prec_single = single;
     S.shift_stop = shift_rsqmin * out.source_norm;
     for (int j = 0; j < n; ++j) S.shift_done_at[j] = INT_MAX;
+    S.ms_delta2 = reliable_update ? ru_delta2 : 0.0;
+    S.rsq_ru = out.source_norm;
     const double m4 = round_prec(-1.0 * offset_low, single);
     double size_prev = out.rsq;
     dslash_prepare(p, ls, L);
     IterLoop loop;
-    loop.run(
-        [&](int k) {
-            tl.run(0, k, [&] { dslash_gated(p, L, tmp, pm[j_low], ls, other, c.d_state, k); });
-            tl.run(1, k, [&] {
-                dslash_mdagm_dot(p, L, ttt, tmp, ls, pm[j_low], m4, parity, c.d_state, c.d_partials, k, 1);
-            });
-            ms_residual(p, L, resid, ttt, c.d_state, c.d_partials, k);
-            ms_update(p, L, xp, d_x, d_p, resid, n, c.d_state, k);
-        },
-        [&](int chunk, int it0) {
-            const int m = next_chunk(chunk, size_prev, S.rsq, S.iteration - it0, S.rsqstop, max_cg - S.iteration);
-            size_prev = S.rsq;
-            return m;
-        },
-        tl, max_cg + 1);
+    int ru_stalls = 0;
+    for (;;) {
+        S.ms_ru = 0;
+        loop.run(
+            [&](int k) {
+                tl.run(0, k, [&] { dslash_gated(p, L, tmp, pm[j_low], ls, other, c.d_state, k); });
+                tl.run(1, k, [&] {
+                    dslash_mdagm_dot(p, L, ttt, tmp, ls, pm[j_low], m4, parity, c.d_state, c.d_partials, k, 1);
+                });
+                ms_residual(p, L, resid, ttt, c.d_state, c.d_partials, k);
+                ms_update(p, L, xp, d_x, d_p, resid, n, c.d_state, k);
+            },
+            [&](int chunk, int it0) {
+                const int m = next_chunk(chunk, size_prev, S.rsq, S.iteration - it0, S.rsqstop, max_cg - S.iteration);
+                size_prev = S.rsq;
+                return m;
+            },
+            tl, max_cg + 1);
+        if (S.converged || !S.ms_ru || S.iteration >= max_cg) break;
+        // reliable update of the base shift: r = b - (A + sigma_low) x_low in FP64
+        const double prev = S.rsq_ru;
+        const double rsq = reliable_update();
+        S.rsq = rsq;
+        S.rsq_ru = rsq;
+        ++out.reliable_updates;
+        if (rsq <= ru_rsqmin * out.source_norm) {
+            S.converged = 1;
+            break;
+        }
+        // two updates in a row that do not halve the true residual: the
+        // recurrence has lost the base shift; the refinement takes over
+        ru_stalls = (rsq > 0.5 * prev) ? ru_stalls + 1 : 0;
+        if (ru_stalls >= 2) break;
+    }
     out.iteration = S.iteration;
     out.converged = S.converged != 0;
     out.rsq = S.rsq;
@@ -769,11 +794,20 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
     std::vector<VecBlock> x = (parity0 != QPHIX_ODD) ? A.out[0] : A.out[1];
     const int max_cg = inv->max * inv->nrestart;
     int parity = parity0 & 1;
+    // The sloppy recurrence alone stalls near its residual gap (|r|^2/|b|^2 ~
+    // 1e-12 in FP32); reliable updates of the base shift (FP64 r = b - A x)
+    // carry the base, and with it the shifts nearest to it, to the target.
+    // Shifts far below the floor stop their vector updates (kShiftStopFactor).
     const double floor = (ps == Prec::Single) ? 1e-12 : 1e-6;
-    const double rsq_sloppy = std::max(A.res[0]->resid, floor);
+    const double target = A.res[0]->resid;
+    // (16-bit links perturb the operator too much for the base to reach the
+    // target; those modes stop at the floor and refine, as before)
+    const bool base_ru_on = ps == Prec::Single && lss.prec == Prec::Single;
+    const double rsq_sloppy = base_ru_on ? 1e-2 * target : std::max(target, floor);
 
     Ws ws;
     VecBlock ttt = ws.get(ps), tmp = ws.get(ps), resid = ws.get(ps), src_s = ws.get(ps);
+    VecBlock tmp64 = ws.get(Prec::Double), ttt64 = ws.get(Prec::Double), r64 = ws.get(Prec::Double);
     std::vector<VecBlock> pm(n);
     for (int j = 0; j < n; ++j) pm[j] = ws.get(ps);
     std::vector<double> shifts(n);
@@ -797,9 +831,24 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
         const Launch L = c.launch();
         vec_copy(ps, src_s, Prec::Double, src, L);
         upload_blocks(d_x, x);
+        auto base_ru = [&]() -> double {
+            const Launch Lr = c.launch();
+            c.h_state->msq_x4 = offset_low;
+            c.h_state->counter = c.h_state->counter2 = 0;
+            upload_state();
+            dslash(Prec::Double, Lr, tmp64, x[j_low], ls64, 1 - parity);
+            dslash(Prec::Double, Lr, ttt64, tmp64, ls64, parity);
+            cg_true_residual(Prec::Double, Lr, ttt64, x[j_low], src, r64, c.d_state, c.d_partials, c.d_scalars);
+            vec_copy(ps, resid, Prec::Double, r64, Lr);
+            QB_CUDA(cudaMemcpyAsync(c.h_scalars, c.d_scalars, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+            sync_check();
+            return c.h_scalars[0];
+        };
         MsPass r = ms_pass(ps, Prec::Double, lss, src_s, x, pm, ttt, tmp, resid, d_x, d_p,
                            parity, shifts, j_low, offset_low, rsq_sloppy, max_cg, false, tl,
-                           rsq_sloppy * kShiftStopFactor);
+                           floor * kShiftStopFactor, c.reliable_delta * c.reliable_delta,
+                           base_ru_on ? std::function<double()>(base_ru) : std::function<double()>(), target);
+        rus += r.reliable_updates;
         total += r.iteration;
         last = r.iteration;
         // refinement of every shift to its own tolerance from the sloppy solution
