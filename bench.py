@@ -111,7 +111,8 @@ def dist_setup():
         import torch.distributed as dist
         from datetime import timedelta
 
-        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+        if not dist.is_initialized():
+            dist.init_process_group("gloo", timeout=timedelta(seconds=600))
         pg = dist
     return world, rank, local, pg
 
