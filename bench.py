@@ -5,8 +5,9 @@ Workload (one "step" = one solve): even-odd asqtad CG for
 (4 m^2 - D_eo D_oe) x = b on a 24^3x48 lattice, mass 0.01, random SU(3)
 links exp(i 0.3 H) (fat x0.9, Naik x(-1/24), staggered phases, seeded),
 Gaussian source on the even sites, squared relative tolerance 1e-20, with the
-FP32 inner solve and FP64 reliable updates (every 0.1 residual drop).  The
-FP64 CG and the 16-bit inner variant are timed on the same input.
+FP32 inner solve (12-real Naik links, third rows rebuilt in the Dslash) and
+FP64 reliable updates (every 0.1 residual drop).  The FP64 CG, the FP32 inner
+solve with 18-real links and the 16-bit variants are timed on the same input.
 
 Arms:
   default           the product library through its C ABI (GPU)
@@ -46,9 +47,15 @@ LINK_SEED, SRC_SEED = 1001, 2002
 RU_DELTA = 0.1         # reliable update at every 0.1 drop of |r| (24^3x48 workload)
 DSLASH_BYTES_F32 = 1200  # algorithmic bytes per output site, FP32, 18-real links
 DSLASH_BYTES_F64 = 2400
+DSLASH_BYTES_R12 = 1012  # FP32 with 12-real Naik links: 8x72 + 8x48 + 4 (sign word) + 48
+# DRAM bytes per output site of one K1 launch measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum / Vh): 264.33 MB at 24^3x32
+K1_TRAFFIC_PER_SITE_F32 = 264.33e6 / 221184
+K1_TRAFFIC_PER_SITE_R12 = None  # filled in from the 12-real capture
 DSLASH_FLOPS = 1146
 METRIC = "time to |r|/|b|<1e-10, mixed vs FP64 CG on 1 B200; Dslash HBM GB/s"
-WORKLOAD = "asqtad mixed-precision CG 24^3x48 m=0.01 tol 1e-10 (FP32 inner, FP64 reliable updates)"
+WORKLOAD = ("asqtad mixed-precision CG 24^3x48 m=0.01 tol 1e-10 (FP32 inner with 12-real Naik links, "
+            "FP64 reliable updates)")
 
 
 def peaks():
@@ -175,6 +182,10 @@ def run_gpu(args):
     xsol64 = lib.extract_V("D", x64, "even")[: Vh * 6]
     lib.destroy_V("D", x64)
 
+    # the timed solves: FP32 inner solve with 12-real Naik links (the
+    # workload's long links are SU(3) times -1/24, so the third rows rebuild
+    # exactly; the library checks that and reports it in links_compressed)
+    lib.set_link_compression(True)
     for _ in range(args.warmup):
         x, _, _, _ = solve("single")
         lib.destroy_V("D", x)
@@ -204,6 +215,23 @@ def run_gpu(args):
     lib.destroy_V("D", x)
     lib.set_kernel_timing(False)
     dslash_ms, dslash_n, mdagm_ms, mdagm_n = st.dslash_ms, st.dslash_launches, st.mdagm_ms, st.mdagm_launches
+    compressed = bool(st.links_compressed)
+    k1_bytes = DSLASH_BYTES_R12 if compressed else DSLASH_BYTES_F32
+    lib.set_link_compression(False)
+
+    # the same FP32 inner solve with 18-real links (warm-up, measured, instrumented)
+    xr, _, _, _ = solve("single")
+    lib.destroy_V("D", xr)
+    ms18 = None
+    for _ in range(2):
+        xr, ms, res18, st18 = solve("single")
+        ms18 = ms if ms18 is None else min(ms18, ms)
+        xsol18 = lib.extract_V("D", xr, "even")[: Vh * 6]
+        lib.destroy_V("D", xr)
+    lib.set_kernel_timing(True)
+    xr, _, _, st18i = solve("single")
+    lib.destroy_V("D", xr)
+    lib.set_kernel_timing(False)
 
     # 16-bit links with FP32 vectors (one warm-up solve, then one measured)
     xl, _, _, _ = solve("half-links")
@@ -225,6 +253,7 @@ def run_gpu(args):
     pinned_zero = torch.zeros(src.shape, dtype=torch.float64).pin_memory().numpy()
     pinned_out = torch.zeros(src.shape, dtype=torch.float64).pin_memory().numpy()
     lib.set_inner_precision("single")
+    lib.set_link_compression(True)  # as in the timed solves
     e2e = []
     for _ in range(max(1, min(args.steps, 3))):
         barrier(pg)
@@ -241,6 +270,7 @@ def run_gpu(args):
         lib.destroy_V("D", xx)
         e2e.append(max(ms_dev, wall))
     e2e_ms = max_over_ranks(pg, float(np.mean(e2e)))
+    lib.set_link_compression(False)
 
     # isolated Dslash bandwidth (FP32 and FP64), timed with CUDA events
     vin = lib.create_V("F", np.random.default_rng(1).standard_normal(V * 6))
@@ -262,7 +292,7 @@ def run_gpu(args):
 
     peak, peak_kind = peaks()
     k1_ms = dslash_ms / max(dslash_n, 1)
-    achieved = DSLASH_BYTES_F32 * Vh / (k1_ms * 1e-3) / 1e9
+    achieved = k1_bytes * Vh / (k1_ms * 1e-3) / 1e9
     err_vs_fp64 = float(np.abs(xs_last - xsol64).max() / np.abs(xsol64).max())
     err_half = float(np.abs(xsolh - xsol64).max() / np.abs(xsol64).max())
     err_hl = float(np.abs(xsoll - xsol64).max() / np.abs(xsol64).max())
@@ -300,19 +330,28 @@ def run_gpu(args):
         "half_links_cg": {"s": msl / 1e3, "iterations": stl.iterations, "reliable_updates": stl.reliable_updates,
                           "true_rsq_rel": resl.final_rsq, "err_vs_fp64_solution": err_hl,
                           "escalated_to_fp32": stl.escalated, "storage": "FP32 vectors, 16-bit fixed-point links"},
+        "mixed_cg_18real_links": {
+            "s": ms18 / 1e3, "iterations": st18.iterations, "reliable_updates": st18.reliable_updates,
+            "true_rsq_rel": res18.final_rsq,
+            "err_vs_fp64_solution": float(np.abs(xsol18 - xsol64).max() / np.abs(xsol64).max()),
+            "k1_us": st18i.dslash_ms / max(st18i.dslash_launches, 1) * 1e3,
+            "k1_gbs": DSLASH_BYTES_F32 * Vh / (st18i.dslash_ms / max(st18i.dslash_launches, 1) * 1e-3) / 1e9,
+            "speedup_vs_fp64": ms64 / ms18, "storage": "FP32 vectors and 18-real FP32 links"},
         "dslash": {"f32_us": ms_f32 * 1e3, "f32_gbs": DSLASH_BYTES_F32 * Vh / (ms_f32 * 1e-3) / 1e9,
                    "f64_us": ms_f64 * 1e3, "f64_gbs": DSLASH_BYTES_F64 * Vh / (ms_f64 * 1e-3) / 1e9,
                    "f32_gflops": DSLASH_FLOPS * Vh / (ms_f32 * 1e-3) / 1e9,
                    "bytes_per_site": {"f32": DSLASH_BYTES_F32, "f64": DSLASH_BYTES_F64},
                    "autotuner": {k: {"variant": ["resident-grid", "full-grid", "tma-pipeline"][v] if v >= 0 else None,
                                      "us": [round(x, 2) for x in us]} for k, (v, us) in tuning.items()}},
-        "roofline": {"kernel": "k_dslash<float> (K1) in a solve of the timed workload (CUDA events per launch)",
+        "roofline": {"kernel": ("k_dslash<float, Recon12>" if compressed else "k_dslash<float, float>")
+                               + " (K1) in a solve of the timed workload (CUDA events per launch)",
                      "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind,
-                     # ncu dram__bytes_read+write of k_dslash<float> at 24^3x32 (264.3 MB,
-                     # profiles/k_dslash_f32_24x24x24x32.md) scaled by sites to 24^3x48
-                     "traffic": 264.33e6 * Vh / 221184,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_site": k1_bytes,
+                     # ncu dram__bytes_read+write per output site of one K1 launch
+                     # (profiles/), times the sites of this lattice
+                     "traffic": (None if (compressed and K1_TRAFFIC_PER_SITE_R12 is None) else
+                                 (K1_TRAFFIC_PER_SITE_R12 if compressed else K1_TRAFFIC_PER_SITE_F32) * Vh),
                      "launches": int(dslash_n), "avg_launch_us": k1_ms * 1e3},
         "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": 2 * Vh * 6 * 8,
                 "d2h_bytes_per_step": Vh * 6 * 8},
@@ -348,7 +387,29 @@ def ref_iteration_sample(links, src, n_iter):
     return dt, res.final_iter
 
 
+class _StdoutToStderr:
+    """The reference host code prints progress lines to stdout; while it runs
+    inside the GPU arm they go to stderr, so stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
 def cpu_baseline_sample(full_iters, links=None, src=None, n_iter=12):
+    with _StdoutToStderr():
+        return _cpu_baseline_sample(full_iters, links, src, n_iter)
+
+
+def _cpu_baseline_sample(full_iters, links=None, src=None, n_iter=12):
     import orc
 
     if not os.path.exists(orc.REF_LIB):
@@ -375,7 +436,8 @@ def run_reference(args):
     full_iters = FP64_ITERATIONS
     samples = []
     for k in range(args.warmup + args.steps):
-        dt, done = ref_iteration_sample(links, src, args.ref_iters)
+        with _StdoutToStderr():
+            dt, done = ref_iteration_sample(links, src, args.ref_iters)
         if k >= args.warmup:
             samples.append(dt / max(done, 1) * full_iters)
     v = float(np.mean(samples))
@@ -428,6 +490,7 @@ def run_profile_mixed(args):
     lib = capi.QphixLib(LIB_PATH)
     assert lib.init(DIMS) == 0, lib.last_error()
     lib.set_reliable_delta(RU_DELTA)
+    lib.set_link_compression(args.compress)
     L = lib.create_L("D", links)
     b = lib.create_V("D", src, "even")
     lib.set_inner_precision(args.inner)
@@ -816,6 +879,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--compress", action="store_true",
+                    help="mixed mode: FP32 inner solve with 12-real Naik links")
     ap.add_argument("--fd-dirs", type=int, default=32,
                     help="force mode: finite-difference directions (0: force only)")
     ap.add_argument("--no-sequential", action="store_true",

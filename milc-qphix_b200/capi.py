@@ -80,7 +80,8 @@ class Stats(C.Structure):
     _fields_ = [("solve_ms", C.c_double), ("iterations", C.c_int),
                 ("reliable_updates", C.c_int), ("dslash_launches", C.c_int),
                 ("dslash_ms", C.c_double), ("mdagm_launches", C.c_int),
-                ("mdagm_ms", C.c_double), ("true_rsq", C.c_double), ("escalated", C.c_int)]
+                ("mdagm_ms", C.c_double), ("true_rsq", C.c_double), ("escalated", C.c_int),
+                ("links_compressed", C.c_int)]
 
 
 PRECISION = {"half": 0, "single": 1, "double": 2, "half-links": 3}
@@ -224,6 +225,9 @@ class QphixLib:
 
     def set_inner_precision(self, name):
         return self.lib.QPHIX_B200_set_inner_precision(PRECISION[name])
+
+    def set_link_compression(self, on):
+        return self.lib.QPHIX_B200_set_link_compression(1 if on else 0)
 
     def set_reliable_delta(self, delta):
         return self.lib.QPHIX_B200_set_reliable_delta(delta)

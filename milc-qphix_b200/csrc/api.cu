@@ -210,7 +210,10 @@ void free_link_handle(FL *L)
 {
     free_links(L->links);
     free_links(L->sloppy_half);
-    if constexpr (std::is_same<FL, QPHIX_D3_FermionLinksAsqtad>::value) free_links(L->sloppy_single);
+    if constexpr (std::is_same<FL, QPHIX_D3_FermionLinksAsqtad>::value) {
+        free_links(L->sloppy_single);
+        free_links(L->sloppy_recon);
+    }
 }
 
 template <typename Real>
@@ -338,10 +341,27 @@ struct SloppyCfg {
     const LinkSet *up;
 };
 
+// FP32 links with 12-real Naik links when compression is on and the field
+// has the form it needs; otherwise the 18-real FP32 copy
+const LinkSet &single_inner_links(QPHIX_D3_FermionLinksAsqtad *H)
+{
+    Context &c = ctx();
+    if (!c.link_compression) return single_links(H);
+    if (!H->recon_checked) {
+        double dev[4];
+        H->recon_checked = 1;
+        if (!links_compress12(H->sloppy_recon, H->links, c.launch(), dev) && c.verbose)
+            std::fprintf(stderr,
+                         "qphix_b200: Naik links keep 18 reals (|ratio| %.6e spread %.2e imag %.2e residual %.2e)\n",
+                         dev[0], dev[1], dev[2], dev[3]);
+    }
+    return H->sloppy_recon.valid ? H->sloppy_recon : single_links(H);
+}
+
 SloppyCfg sloppy_cfg(QPHIX_D3_FermionLinksAsqtad *H, int mode)
 {
     switch (mode) {
-    case QPHIX_B200_PREC_SINGLE: return {Prec::Single, &single_links(H), nullptr};
+    case QPHIX_B200_PREC_SINGLE: return {Prec::Single, &single_inner_links(H), nullptr};
     case QPHIX_B200_PREC_HALF: return {Prec::Half, &half_links(H), &single_links(H)};
     case QPHIX_B200_PREC_HALF_LINKS: return {Prec::Single, &half_links(H), &single_links(H)};
     default: throw Error("unknown inner precision");
@@ -370,6 +390,7 @@ int asqtad_invert(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_invert_ar
             } else {
                 const SloppyCfg s = sloppy_cfg(H, c.inner_mode);
                 iters = cg_mixed(s.vec, H->links, *s.links, s.up, a);
+                c.stats.links_compressed = s.links->recon ? 1 : 0;
             }
         } else {
             iters = cg_reference(Prec::Single, H->links, a);
@@ -422,6 +443,7 @@ int asqtad_invert_multi(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_inv
             } else {
                 const SloppyCfg s = sloppy_cfg(H, c.inner_mode);
                 iters = multishift_mixed(s.vec, H->links, *s.links, s.up, a);
+                c.stats.links_compressed = s.links->recon ? 1 : 0;
             }
         } else {
             iters = multishift_reference(Prec::Single, H->links, a);
@@ -585,6 +607,10 @@ QPHIX_status_t QPHIX_B200_set_inner_precision(QPHIX_B200_precision_t p)
     });
 }
 QPHIX_B200_precision_t QPHIX_B200_get_inner_precision(void) { return static_cast<QPHIX_B200_precision_t>(ctx().inner_mode); }
+QPHIX_status_t QPHIX_B200_set_link_compression(int on)
+{
+    return guarded([&] { ctx().link_compression = on ? 1 : 0; });
+}
 QPHIX_status_t QPHIX_B200_set_reliable_delta(double delta)
 {
     return guarded([&] {
@@ -605,6 +631,7 @@ QPHIX_status_t QPHIX_B200_get_last_stats(QPHIX_B200_stats_t *s)
         s->mdagm_launches = t.mdagm_launches;
         s->mdagm_ms = t.mdagm_ms;
         s->true_rsq = t.true_rsq;
+        s->links_compressed = t.links_compressed;
         s->escalated = t.escalated;
     });
 }

@@ -87,9 +87,12 @@ void free_links(LinkSet &ls)
 {
     for (int cb = 0; cb < 2; ++cb) {
         dev_free(ls.blk[cb]);
+        dev_free(ls.sign[cb]);
         ls.blk[cb] = nullptr;
+        ls.sign[cb] = nullptr;
     }
     ls.valid = false;
+    ls.recon = false;
 }
 
 void upload_state()

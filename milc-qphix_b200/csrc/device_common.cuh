@@ -163,6 +163,54 @@ template <> struct LinkView<__half> {
     }
 };
 
+// FP32 fat links and 12-real Naik links (layout: internal.h, LinkSet::recon)
+template <> struct LinkView<Recon12> {
+    const float4 *p;
+    const unsigned *sign;
+    int vh;
+    float scale;
+    // the fat forward/backward pair of direction d (18 complex)
+    __device__ __forceinline__ void load_fat(int d, int j, float u[36]) const {
+        const float4 *q = p + (size_t)d * kReconChunks * vh + j;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const float4 z = __ldcs(q + (size_t)c * vh);
+            u[4 * c] = z.x; u[4 * c + 1] = z.y; u[4 * c + 2] = z.z; u[4 * c + 3] = z.w;
+        }
+    }
+    // the Naik forward (uf) and backward (ub) links of direction d, third
+    // rows rebuilt: row2 = sign * scale * conj(row0 x row1)
+    __device__ __forceinline__ void load_naik(int d, int j, unsigned bits, float uf[18], float ub[18]) const {
+        const float4 *q = p + ((size_t)d * kReconChunks + 9) * vh + j;
+        float w[24];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const float4 z = __ldcs(q + (size_t)c * vh);
+            w[4 * c] = z.x; w[4 * c + 1] = z.y; w[4 * c + 2] = z.z; w[4 * c + 3] = z.w;
+        }
+#pragma unroll
+        for (int e = 0; e < 12; ++e) {
+            uf[e] = w[e];
+            ub[e] = w[12 + e];
+        }
+        rebuild(uf, (bits >> (2 * d)) & 1u ? -scale : scale);
+        rebuild(ub, (bits >> (2 * d + 1)) & 1u ? -scale : scale);
+    }
+    __device__ __forceinline__ static void rebuild(float u[18], float f) {
+        // a = row 0, b = row 1: (a x b)_k = a_{k+1} b_{k+2} - a_{k+2} b_{k+1}
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+            const float ar1 = u[2 * k1], ai1 = u[2 * k1 + 1], ar2 = u[2 * k2], ai2 = u[2 * k2 + 1];
+            const float br1 = u[6 + 2 * k1], bi1 = u[6 + 2 * k1 + 1], br2 = u[6 + 2 * k2], bi2 = u[6 + 2 * k2 + 1];
+            const float cr = (ar1 * br2 - ai1 * bi2) - (ar2 * br1 - ai2 * bi1);
+            const float ci = (ar1 * bi2 + ai1 * br2) - (ar2 * bi1 + ai2 * br1);
+            u[12 + 2 * k] = f * cr;
+            u[12 + 2 * k + 1] = -f * ci;  // conjugate
+        }
+    }
+};
+
 // ------------------------------------------------------------------ SU(3) --
 // acc += U v
 template <typename A>

@@ -70,6 +70,24 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
                 mv_adj_sub(acc, u + 18, vb);
             }
         }
+    } else if constexpr (std::is_same<SL, Recon12>::value) {
+        // FP32 fat pair (9 x 16 bytes) + 12-real Naik pair (6 x 16 bytes) with
+        // their third rows rebuilt from the site's sign bits
+        const unsigned bits = __ldg(a.links.sign + j);
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            A u[36], vf[6], vb[6];
+            a.in.load(neighbor(a.g, s, 2 * d + 1), vf);
+            a.in.load(neighbor(a.g, s, 2 * d), vb);
+            a.links.load_fat(d, j, u);
+            mv_add(acc, u, vf);
+            mv_adj_sub(acc, u + 18, vb);
+            a.in.load(neighbor(a.g, s, 8 + 2 * d + 1), vf);
+            a.in.load(neighbor(a.g, s, 8 + 2 * d), vb);
+            a.links.load_naik(d, j, bits, u, u + 18);
+            mv_add(acc, u, vf);
+            mv_adj_sub(acc, u + 18, vb);
+        }
     } else {
         // 16-bit: the four matrices of a direction, 9 x 16 bytes + 4 neighbours
 #pragma unroll
@@ -351,6 +369,9 @@ static DslashArgs<SV, SL> make_args(const Launch &L, VecBlock out, VecBlock in, 
                                    ls.link_max[0] / 32767.0f, ls.link_max[1] / 32767.0f};
     } else if constexpr (std::is_same<SL, float>::value) {
         a.links = LinkView<float>{static_cast<const float4 *>(ls.blk[cb]), L.g->vh};
+    } else if constexpr (std::is_same<SL, Recon12>::value) {
+        a.links = LinkView<Recon12>{static_cast<const float4 *>(ls.blk[cb]), static_cast<const unsigned *>(ls.sign[cb]),
+                                    L.g->vh, ls.recon_scale};
     } else {
         a.links = LinkView<double>{static_cast<const double2 *>(ls.blk[cb]), L.g->vh};
     }
@@ -425,17 +446,32 @@ struct TuneEntry {
     int variant = 0;
     float us[kVariants] = {0, 0, 0};
 };
-static TuneEntry g_tune[3][3];  // per (vector precision, link precision)
+static TuneEntry g_tune[3][4];  // per (vector precision, link storage: Prec or 3 = 12-real Naik)
+
+template <typename SL>
+static int link_slot(Prec pl)
+{
+    return std::is_same<SL, Recon12>::value ? 3 : (int)pl;
+}
+
+// the TMA pipeline stages 18-real FP32 pairs; 12-real Naik links run the
+// register variants only
+template <typename SL>
+constexpr bool has_tma() { return !std::is_same<SL, Recon12>::value; }
 
 template <typename SV, typename SL>
 static void launch_variant(int variant, const DslashArgs<SV, SL> &a, const LinkSet &ls, int cb, const Launch &L,
                            const SolverState *st, int gate)
 {
-    if (variant == 2) {
+    if constexpr (!has_tma<SL>()) {
+        if (variant == 2) variant = 1;
+    } else if (variant == 2) {
         k_dslash_tma<SV, SL, 0><<<tma_grid<SV, SL, 0>(L.g->vh), TmaCfg<SL>::T, tma_smem_bytes<SL>(), L.stream>>>(
             a, static_cast<const char *>(ls.blk[cb]), a.out, 0.0, const_cast<SolverState *>(st), nullptr, gate, 0,
             L.err);
-    } else if (variant == 1) {
+        return;
+    }
+    if (variant == 1) {
         k_dslash<SV, SL><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, st, gate);
     } else {
         k_dslash<SV, SL><<<resident_grid(k_dslash<SV, SL>, L.g->vh), kBlock, 0, L.stream>>>(a, st, gate);
@@ -447,7 +483,7 @@ static int tuned_variant(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV,
 {
     const int f = forced_variant();
     if (f >= 0) return f;
-    TuneEntry &t = g_tune[(int)pv][(int)pl];
+    TuneEntry &t = g_tune[(int)pv][link_slot<SL>(pl)];
     if (t.vh == L.g->vh) return t.variant;
     // time the variants on scratch vectors so no caller data is touched twice
     const size_t cx = pv == Prec::Double ? 16 : (pv == Prec::Single ? 8 : 4);
@@ -468,7 +504,7 @@ static int tuned_variant(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV,
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int best = 0;
-    for (int v = 0; v < kVariants; ++v) {
+    for (int v = 0; v < (has_tma<SL>() ? kVariants : 2); ++v) {
         launch_variant<SV, SL>(v, s, ls, cb, L, nullptr, -1);  // warm
         cudaEventRecord(e0, L.stream);
         for (int r = 0; r < 3; ++r) launch_variant<SV, SL>(v, s, ls, cb, L, nullptr, -1);
@@ -500,24 +536,28 @@ static void launch_dslash(const Launch &L, VecBlock out, VecBlock in, const Link
 
 // storage combinations served: vectors and links in the same precision, and
 // FP32 vectors with 16-bit links
-#define QB_DISPATCH_VL(pv, pl, F, ...)                                                           \
+#define QB_DISPATCH_VL(pv, ls_, F, ...)                                                          \
     do {                                                                                        \
-        if ((pv) == Prec::Double && (pl) == Prec::Double) F<double, double>(__VA_ARGS__);       \
-        else if ((pv) == Prec::Single && (pl) == Prec::Single) F<float, float>(__VA_ARGS__);    \
-        else if ((pv) == Prec::Half && (pl) == Prec::Half) F<__half, __half>(__VA_ARGS__);     \
-        else if ((pv) == Prec::Single && (pl) == Prec::Half) F<float, __half>(__VA_ARGS__);     \
+        const Prec pl_ = (ls_).prec;                                                            \
+        if ((ls_).recon) {                                                                      \
+            if ((pv) != Prec::Single) throw std::runtime_error("Dslash: 12-real links need FP32 vectors"); \
+            F<float, Recon12>(__VA_ARGS__);                                                     \
+        } else if ((pv) == Prec::Double && pl_ == Prec::Double) F<double, double>(__VA_ARGS__); \
+        else if ((pv) == Prec::Single && pl_ == Prec::Single) F<float, float>(__VA_ARGS__);     \
+        else if ((pv) == Prec::Half && pl_ == Prec::Half) F<__half, __half>(__VA_ARGS__);      \
+        else if ((pv) == Prec::Single && pl_ == Prec::Half) F<float, __half>(__VA_ARGS__);      \
         else throw std::runtime_error("Dslash: unsupported vector/link precision pair");       \
     } while (0)
 
 void dslash(Prec p, const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb)
 {
-    QB_DISPATCH_VL(p, ls.prec, launch_dslash, L, out, in, ls, cb, nullptr, -1, p);
+    QB_DISPATCH_VL(p, ls, launch_dslash, L, out, in, ls, cb, nullptr, -1, p);
 }
 
 void dslash_gated(Prec p, const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb,
                   SolverState *st, int gate)
 {
-    QB_DISPATCH_VL(p, ls.prec, launch_dslash, L, out, in, ls, cb, st, gate, p);
+    QB_DISPATCH_VL(p, ls, launch_dslash, L, out, in, ls, cb, st, gate, p);
 }
 
 int dslash_variant(Prec pv, Prec pl, float us[3])
@@ -534,11 +574,15 @@ static void launch_mdagm_variant(int variant, const DslashArgs<SV, SL> &a, const
                                  double m4, int cb, SolverState *st, double *partials, int gate, int mode,
                                  const Launch &L)
 {
-    if (variant == 1) {
-        k_dslash_mdagm<SV, SL><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, pv, m4, st, partials, gate, mode);
+    if constexpr (!has_tma<SL>()) {
+        if (variant == 2) variant = 1;
     } else if (variant == 2) {
         k_dslash_tma<SV, SL, 1><<<tma_grid<SV, SL, 1>(L.g->vh), TmaCfg<SL>::T, tma_smem_bytes<SL>(), L.stream>>>(
             a, static_cast<const char *>(ls.blk[cb]), pv, m4, st, partials, gate, mode, L.err);
+        return;
+    }
+    if (variant == 1) {
+        k_dslash_mdagm<SV, SL><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(a, pv, m4, st, partials, gate, mode);
     } else {
         k_dslash_mdagm<SV, SL><<<resident_grid(k_dslash_mdagm<SV, SL>, L.g->vh), kBlock, 0, L.stream>>>(
             a, pv, m4, st, partials, gate, mode);
@@ -547,7 +591,7 @@ static void launch_mdagm_variant(int variant, const DslashArgs<SV, SL> &a, const
 
 // The fused M^dag M kernel (K2) is tuned on its own: its grid-wide reduction
 // favours fewer, longer-lived blocks more than the plain Dslash does.
-static TuneEntry g_tune_mdagm[3][3];
+static TuneEntry g_tune_mdagm[3][4];
 
 template <typename SV, typename SL>
 static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV, SL> &a, const LinkSet &ls,
@@ -555,7 +599,7 @@ static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashAr
 {
     const int f = forced_variant();
     if (f >= 0) return f;
-    TuneEntry &t = g_tune_mdagm[(int)pv][(int)pl];
+    TuneEntry &t = g_tune_mdagm[(int)pv][link_slot<SL>(pl)];
     if (t.vh == L.g->vh) return t.variant;
     // scratch vectors, solver state and partials: no caller data is touched
     const size_t cx = pv == Prec::Double ? 16 : (pv == Prec::Single ? 8 : 4);
@@ -586,7 +630,7 @@ static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashAr
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int best = 0;
-    for (int v = 0; v < kVariants; ++v) {
+    for (int v = 0; v < (has_tma<SL>() ? kVariants : 2); ++v) {
         launch_mdagm_variant<SV, SL>(v, s, ls, p, 0.0, cb, st, part, -1, 0, L);  // warm
         cudaEventRecord(e0, L.stream);
         for (int r = 0; r < 3; ++r) launch_mdagm_variant<SV, SL>(v, s, ls, p, 0.0, cb, st, part, -1, 0, L);
@@ -625,20 +669,22 @@ static void prepare_impl(Prec pv, const LinkSet &ls, const Launch &L)
     (void)tuned_variant_mdagm<SV, SL>(pv, ls.prec, L, a, ls, 0);
     (void)resident_grid(k_dslash<SV, SL>, L.g->vh);
     (void)resident_grid(k_dslash_mdagm<SV, SL>, L.g->vh);
-    (void)tma_grid<SV, SL, 0>(L.g->vh);
-    (void)tma_grid<SV, SL, 1>(L.g->vh);
+    if constexpr (has_tma<SL>()) {
+        (void)tma_grid<SV, SL, 0>(L.g->vh);
+        (void)tma_grid<SV, SL, 1>(L.g->vh);
+    }
 }
 
 void dslash_prepare(Prec pv, const LinkSet &ls, const Launch &L)
 {
-    QB_DISPATCH_VL(pv, ls.prec, prepare_impl, pv, ls, L);
+    QB_DISPATCH_VL(pv, ls, prepare_impl, pv, ls, L);
 }
 
 void dslash_mdagm_dot(Prec p, const Launch &L, VecBlock ttt, VecBlock tmp, const LinkSet &ls,
                       VecBlock pv, double m4, int cb, SolverState *st, double *partials, int gate,
                       int mode)
 {
-    QB_DISPATCH_VL(p, ls.prec, launch_mdagm, L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode, p);
+    QB_DISPATCH_VL(p, ls, launch_mdagm, L, ttt, tmp, ls, pv, m4, cb, st, partials, gate, mode, p);
 }
 
 // FP64 Dslash and fused M^dag M launches with a fixed kernel variant (one

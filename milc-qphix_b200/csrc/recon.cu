@@ -1,0 +1,201 @@
+// FP32 link sets with 12-real Naik links.
+//
+// The reference can store the long (Naik) links without their third row
+// (COMPRESSED_12 in asqtad_create_L_from_raw, qphix_f3.cpp:1008-1016) and
+// rebuild it as conj(row0 x row1) with the staggered-phase sign
+// (reconstruct_gauge_third_row, qphix_f3.cpp:1072-1084).  MILC's Naik links
+// carry the Naik coefficient and the phases, so here the rebuilt row is
+// sign * s * conj(row0 x row1) with one magnitude s for the whole field and a
+// sign bit per link, both measured from the FP64 links: an SU(3) matrix times
+// a real factor c satisfies row2 = conj(row0 x row1) / c.  A field that does
+// not have that form (U(3) links with arbitrary phases, a varying factor) is
+// detected and keeps its 18-real links.  Only the FP32 copy used by the
+// mixed-precision inner solve is compressed; FP64 links stay complete.
+//
+// Bytes per output site of the FP32 Dslash: 8 fat x 72 + 8 Naik x 48 + 4
+// (sign word) + 48 (vectors) = 1012 instead of 1200.
+#include "context.h"
+#include "device_common.cuh"
+
+namespace qb {
+
+namespace {
+
+constexpr int kProbeNV = 4;
+
+__device__ __forceinline__ void load_link64(const double2 *blk, int d, int slot, int j, int vh, double2 u[9])
+{
+#pragma unroll
+    for (int e = 0; e < 9; ++e) u[e] = blk[link_cx_index(1, d, 9 * slot + e, j, vh)];
+}
+
+// c = conj(row0 x row1) of u
+__device__ __forceinline__ void conj_cross(const double2 u[9], double2 c[3])
+{
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+        const double2 a1 = u[k1], a2 = u[k2], b1 = u[3 + k1], b2 = u[3 + k2];
+        const double re = (a1.x * b2.x - a1.y * b2.y) - (a2.x * b1.x - a2.y * b1.y);
+        const double im = (a1.x * b2.y + a1.y * b2.x) - (a2.x * b1.y + a2.y * b1.x);
+        c[k] = make_double2(re, -im);
+    }
+}
+
+// ratio rho = <c, row2> / |c|^2 of one Naik link (complex)
+__device__ __forceinline__ double2 ratio(const double2 u[9], const double2 c[3], double *c2)
+{
+    double nr = 0, ni = 0, n2 = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double2 r = u[6 + k];
+        nr += c[k].x * r.x + c[k].y * r.y;
+        ni += c[k].x * r.y - c[k].y * r.x;
+        n2 += c[k].x * c[k].x + c[k].y * c[k].y;
+    }
+    *c2 = n2;
+    return n2 > 0 ? make_double2(nr / n2, ni / n2) : make_double2(0.0, 0.0);
+}
+
+// pass 0: sums of |rho|, (Im rho)^2, |row2 - Re(rho) c|^2, |row2|^2
+// pass 1: sum of (|rho| - mean)^2
+__global__ void __launch_bounds__(kBlock) k_recon_probe(const double2 *blk, int vh, int pass, double mean,
+                                                        double *partials)
+{
+    double s[kProbeNV] = {0, 0, 0, 0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < vh * 8; t += gridDim.x * blockDim.x) {
+        const int j = t >> 3, d = (t >> 1) & 3, slot = 2 + (t & 1);
+        double2 u[9], c[3];
+        load_link64(blk, d, slot, j, vh, u);
+        conj_cross(u, c);
+        double c2;
+        const double2 rho = ratio(u, c, &c2);
+        const double mag = fabs(rho.x);
+        if (pass == 0) {
+            s[0] += mag;
+            s[1] += rho.y * rho.y;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double dr = u[6 + k].x - rho.x * c[k].x, di = u[6 + k].y - rho.x * c[k].y;
+                s[2] += dr * dr + di * di;
+                s[3] += u[6 + k].x * u[6 + k].x + u[6 + k].y * u[6 + k].y;
+            }
+        } else {
+            s[0] += (mag - mean) * (mag - mean);
+        }
+    }
+    __shared__ double sm[kProbeNV][kBlock / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < kProbeNV; ++i) {
+        const double v = warp_sum(s[i]);
+        if (lane == 0) sm[i][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kProbeNV) {
+        double v = 0;
+        for (int k = 0; k < kBlock / 32; ++k) v += sm[threadIdx.x][k];
+        partials[threadIdx.x * gridDim.x + blockIdx.x] = v;
+    }
+}
+
+__global__ void k_sum_partials(const double *partials, int nb, double *out)
+{
+    const int i = threadIdx.x;
+    if (i >= kProbeNV) return;
+    double v = 0;
+    for (int b = 0; b < nb; ++b) v += partials[i * nb + b];
+    out[i] = v;
+}
+
+// FP32 blocks: per direction the fat pair (complex 0..17 -> 9 float4) and
+// rows 0-1 of the Naik forward and backward links (12 complex -> 6 float4);
+// sign bit 2d (forward) / 2d+1 (backward) when Re(rho) < 0
+__global__ void __launch_bounds__(kBlock) k_recon_pack(float4 *dst, unsigned *sign, const double2 *blk, int vh)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= vh) return;
+    unsigned bits = 0;
+#pragma unroll 1
+    for (int d = 0; d < 4; ++d) {
+        float4 *q = dst + (size_t)d * kReconChunks * vh + j;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const double2 a = blk[link_cx_index(1, d, 2 * c, j, vh)];
+            const double2 b = blk[link_cx_index(1, d, 2 * c + 1, j, vh)];
+            q[(size_t)c * vh] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+        }
+#pragma unroll
+        for (int slot = 2; slot < 4; ++slot) {
+            double2 u[9], c3[3];
+            load_link64(blk, d, slot, j, vh, u);
+            conj_cross(u, c3);
+            double c2;
+            if (ratio(u, c3, &c2).x < 0) bits |= 1u << (2 * d + (slot - 2));
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                // rows 0-1 (6 complex) of this link: chunks 9 + 3*(slot-2) + c
+                q[(size_t)(9 + 3 * (slot - 2) + c) * vh] =
+                    make_float4((float)u[2 * c].x, (float)u[2 * c].y, (float)u[2 * c + 1].x, (float)u[2 * c + 1].y);
+            }
+        }
+    }
+    sign[j] = bits;
+}
+
+}  // namespace
+
+bool links_compress12(LinkSet &dst, const LinkSet &src64, const Launch &L, double dev[4])
+{
+    Context &c = ctx();
+    const int vh = L.g->vh;
+    if (src64.prec != Prec::Double || !src64.valid) throw Error("links_compress12: needs FP64 links");
+    const int nb = 296;
+    double *part = static_cast<double *>(dev_alloc(sizeof(double) * (kProbeNV * nb + kProbeNV)));
+    double *sums = part + kProbeNV * nb;
+    double h[kProbeNV], tot[kProbeNV] = {0, 0, 0, 0};
+    double mean = 0, spread = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        double acc[kProbeNV] = {0, 0, 0, 0};
+        for (int cb = 0; cb < 2; ++cb) {
+            k_recon_probe<<<nb, kBlock, 0, L.stream>>>(static_cast<const double2 *>(src64.blk[cb]), vh, pass, mean,
+                                                      part);
+            k_sum_partials<<<1, 32, 0, L.stream>>>(part, nb, sums);
+            QB_CUDA(cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, L.stream));
+            sync_check();
+            for (int i = 0; i < kProbeNV; ++i) acc[i] += h[i];
+        }
+        const double n = 2.0 * vh * 8;
+        if (pass == 0) {
+            for (int i = 0; i < kProbeNV; ++i) tot[i] = acc[i];
+            mean = tot[0] / n;
+        } else {
+            spread = std::sqrt(acc[0] / n) / (mean > 0 ? mean : 1.0);
+        }
+    }
+    dev_free(part);
+    const double n = 2.0 * vh * 8;
+    dev[0] = mean;
+    dev[1] = spread;
+    dev[2] = mean > 0 ? std::sqrt(tot[1] / n) / mean : 1.0;
+    dev[3] = tot[3] > 0 ? std::sqrt(tot[2] / tot[3]) : 1.0;
+    // the rebuilt rows must be exact far below FP32 rounding
+    if (!(mean > 0) || !(spread < 1e-9) || !(dev[2] < 1e-9) || !(dev[3] < 1e-9)) return false;
+    dst = LinkSet{};
+    for (int cb = 0; cb < 2; ++cb) {
+        dst.blk[cb] = dev_alloc(sizeof(float4) * kReconChunks * 4 * (size_t)vh);
+        dst.sign[cb] = dev_alloc(sizeof(unsigned) * (size_t)vh);
+        k_recon_pack<<<grid_for(vh), kBlock, 0, L.stream>>>(static_cast<float4 *>(dst.blk[cb]),
+                                                            static_cast<unsigned *>(dst.sign[cb]),
+                                                            static_cast<const double2 *>(src64.blk[cb]), vh);
+    }
+    QB_CUDA(cudaGetLastError());
+    sync_check();
+    dst.prec = Prec::Single;
+    dst.recon = true;
+    dst.recon_scale = (float)mean;
+    dst.valid = true;
+    return true;
+}
+
+}  // namespace qb

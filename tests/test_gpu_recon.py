@@ -1,0 +1,87 @@
+"""GPU: FP32 inner solves with 12-real Naik links (QPHIX_B200_set_link_compression).
+
+The rebuilt third rows make the FP32 operator equal to the 18-real one up to
+FP32 rounding, so a mixed-precision solve with compression must take the same
+number of inner iterations to within a few and reach the same FP64 true
+residual (checked by the oracle).  A Naik field that is not SU(3) times one
+real factor must be detected and solved with 18-real links.
+"""
+import numpy as np
+import pytest
+
+from conftest import fields, orc, synthetic
+
+pytestmark = pytest.mark.gpu
+
+DIMS = (8, 8, 8, 8)
+RESID = 1e-20
+
+
+def _solve(lib, links, src, mass, compress, multi=None):
+    lib.set_link_compression(compress)
+    lib.set_inner_precision("single")
+    try:
+        L = lib.create_L("D", links)
+        b = lib.create_V("D", src, "even")
+        if multi is None:
+            x = lib.create_V("D", np.zeros_like(src), "even")
+            it, info, res = lib.invert("D", L, x, b, mass, parity="even", max_iter=4000, nrestart=5, resid=RESID)
+            st = lib.last_stats()
+            sols = [lib.extract_V("D", x, "even")]
+            lib.destroy_V("D", x)
+        else:
+            xs = [lib.create_V("D", np.zeros_like(src), "even") for _ in multi]
+            it, info, res = lib.invert_multi("D", L, xs, b, multi, parity="even", max_iter=4000, nrestart=5,
+                                             resid=RESID)
+            st = lib.last_stats()
+            sols = [lib.extract_V("D", x, "even") for x in xs]
+            for x in xs:
+                lib.destroy_V("D", x)
+        assert info.status == 0, lib.last_error()
+        lib.destroy_V("D", b)
+        lib.destroy_L("D", L)
+    finally:
+        lib.set_link_compression(False)
+        lib.set_inner_precision("double")
+    return st, sols
+
+
+@pytest.mark.parametrize("smear", [False, True])
+def test_compressed_naik_links_solve(gpu, smear):
+    lib = gpu.use(DIMS)
+    links = fields(DIMS, seed=21, smear=smear, eps_fat=0.2 if smear else 0.3)
+    src = synthetic.gaussian_source(DIMS, seed=2002, parity="even")
+    st0, (x0,) = _solve(lib, links, src, 0.03, False)
+    st1, (x1,) = _solve(lib, links, src, 0.03, True)
+    assert st0.links_compressed == 0 and st1.links_compressed == 1
+    # the two FP32 operators differ by rounding: the reliable-update schedule,
+    # and with it the inner iteration count, can move by a few per cent
+    assert abs(st1.iterations - st0.iterations) <= max(20, st0.iterations // 20)
+    assert orc.true_residual(DIMS, links, x1, src, 0.03, "even") < 1.5 * RESID
+
+
+def test_compressed_multishift(gpu):
+    lib = gpu.use(DIMS)
+    links = fields(DIMS, seed=21)
+    src = synthetic.gaussian_source(DIMS, seed=2002, parity="even")
+    masses = np.sqrt(0.02 ** 2 + np.logspace(-3, 0, 4) / 4)
+    st, xs = _solve(lib, links, src, None, True, multi=masses)
+    assert st.links_compressed == 1
+    for m, x in zip(masses, xs):
+        assert orc.true_residual(DIMS, links, x, src, m, "even") < 1.5 * RESID
+
+
+def test_non_su3_naik_links_keep_18_reals(gpu):
+    """Naik links scaled by a site-dependent factor have no single magnitude:
+    the check refuses them and the solve runs with 18-real links."""
+    lib = gpu.use(DIMS)
+    links = dict(fields(DIMS, seed=21))
+    V = int(np.prod(DIMS))
+    scale = 1.0 + 0.1 * np.random.default_rng(5).random(V)
+    lng = (links["lng"].reshape(V, 72) * scale[:, None]).reshape(-1)
+    links["lng"] = lng
+    links["lngback"] = synthetic.backlinks_raw(DIMS, lng, 3)
+    src = synthetic.gaussian_source(DIMS, seed=2002, parity="even")
+    st, (x,) = _solve(lib, links, src, 0.03, True)
+    assert st.links_compressed == 0
+    assert orc.true_residual(DIMS, links, x, src, 0.03, "even") < 1.5 * RESID
