@@ -51,7 +51,8 @@ DSLASH_BYTES_R12 = 1012  # FP32 with 12-real Naik links: 8x72 + 8x48 + 4 (sign w
 # DRAM bytes per output site of one K1 launch measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum / Vh): 264.33 MB at 24^3x32
 K1_TRAFFIC_PER_SITE_F32 = 264.33e6 / 221184
-K1_TRAFFIC_PER_SITE_R12 = None  # filled in from the 12-real capture
+# 332.48 MB (327.83 read + 4.65 write) at 24^3x48 for k_dslash<float, Recon12>
+K1_TRAFFIC_PER_SITE_R12 = 332.477696e6 / 331776
 DSLASH_FLOPS = 1146
 METRIC = "time to |r|/|b|<1e-10, mixed vs FP64 CG on 1 B200; Dslash HBM GB/s"
 WORKLOAD = ("asqtad mixed-precision CG 24^3x48 m=0.01 tol 1e-10 (FP32 inner with 12-real Naik links, "
@@ -319,7 +320,8 @@ def run_gpu(args):
                    "reliable_delta": RU_DELTA,
                    "seeds": {"links": LINK_SEED, "source": SRC_SEED}, "parallelism": f"replicas{world}",
                    "l2": "working set (links 0.76 GB FP32, 1.5 GB FP64) exceeds the 126 MB L2"},
-        "solve": {"iterations": int(np.median(iters)), "reliable_updates": int(np.median(rus)),
+        "solve": {"ms_each": [round(t, 3) for t in times], "links_compressed": compressed,
+                  "iterations": int(np.median(iters)), "reliable_updates": int(np.median(rus)),
                   "true_rsq_rel": float(max(trues)), "err_vs_fp64_solution": err_vs_fp64},
         "fp64_cg": {"s": ms64 / 1e3, "iterations": res64.final_iter, "true_rsq_rel": res64.final_rsq,
                     "speedup_mixed_vs_fp64": ms64 / ms_step},

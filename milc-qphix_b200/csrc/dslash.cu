@@ -109,6 +109,11 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
     }
 }
 
+// blocks of 256 per SM the register allocation must allow: the 12-real
+// kernel is latency-bound at 4 (56 registers), so it is held to 5
+template <typename SL> struct MinBlocks { static constexpr int value = 1; };
+template <> struct MinBlocks<Recon12> { static constexpr int value = 5; };
+
 // Scalar step after p.(M^dag M p) is known: CG (mode 0) a = -rsq/pkp;
 // multi-shift (mode 1) the shift recurrences.  Runs in one thread.
 __device__ __forceinline__ void mdagm_finalize(SolverState *st, double pkp, int mode)
@@ -155,7 +160,7 @@ __device__ __forceinline__ void mdagm_finalize(SolverState *st, double pkp, int 
 }
 
 template <typename SV, typename SL>
-__global__ void __launch_bounds__(kBlock) k_dslash(DslashArgs<SV, SL> a, const SolverState *st, int gate)
+__global__ void __launch_bounds__(kBlock, MinBlocks<SL>::value) k_dslash(DslashArgs<SV, SL> a, const SolverState *st, int gate)
 {
     using A = typename Acc<SV>::type;
     if (st && gated_off(st, gate)) return;
@@ -169,7 +174,7 @@ __global__ void __launch_bounds__(kBlock) k_dslash(DslashArgs<SV, SL> a, const S
 // ttt = D tmp + m4 * p ;  pkp = sum p . ttt  (calc_pkp, ks_d_congrad_fn.cpp:159-171;
 // ks_multicg_offset.cpp:107-122), then the scalar step of the solver.
 template <typename SV, typename SL>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, MinBlocks<SL>::value)
 k_dslash_mdagm(DslashArgs<SV, SL> a, VecView<SV> pv, double m4, SolverState *st, double *partials,
                int gate, int mode)
 {
