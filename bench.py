@@ -561,6 +561,7 @@ def run_multishift(args):
     lib = capi.QphixLib(LIB_PATH)
     assert lib.init(dims) == 0, lib.last_error()
     lib.set_reliable_delta(0.2)
+    lib.set_link_compression(not args.no_compress)  # FP32 inner solves with 12-real Naik links
     L = lib.create_L("D", links)
     b = lib.create_V("D", src, "even")
     assert L and b, lib.last_error()
@@ -624,7 +625,8 @@ def run_multishift(args):
             continue
         ms, st, res, x = cg(inner, reps)
         d = {"s": ms / 1e3, "iterations": st.iterations, "reliable_updates": st.reliable_updates,
-             "escalated": st.escalated, "true_rsq_rel": _true_rel_rsq(lib, L, x, src, MS_MASS, V)}
+             "escalated": st.escalated, "links_compressed": st.links_compressed,
+             "true_rsq_rel": _true_rel_rsq(lib, L, x, src, MS_MASS, V)}
         if x64 is not None:
             d["err_vs_fp64"] = rel(x, x64)
             d["speedup_vs_fp64_cg"] = ms64 / ms
@@ -649,7 +651,7 @@ def run_multishift(args):
             continue
         ms, st, res, xs = multi(inner, reps)
         d = {"s": ms / 1e3, "iterations": st.iterations, "reliable_updates": st.reliable_updates,
-             "final_iter_per_shift": [r.final_iter for r in res],
+             "links_compressed": st.links_compressed, "final_iter_per_shift": [r.final_iter for r in res],
              "true_rsq_rel": [_true_rel_rsq(lib, L, x, src, m, V) for x, m in zip(xs, masses)]}
         if xs64 is not None:
             d["err_vs_fp64"] = [rel(x, y) for x, y in zip(xs, xs64)]
@@ -881,6 +883,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compress", action="store_true",
+                    help="multishift mode: 18-real links in the FP32 inner solves")
     ap.add_argument("--compress", action="store_true",
                     help="mixed mode: FP32 inner solve with 12-real Naik links")
     ap.add_argument("--fd-dirs", type=int, default=32,
