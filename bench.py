@@ -369,18 +369,18 @@ def run_gpu(args):
 
 
 # ------------------------------------------------------- reference (CPU) --
-def ref_iteration_sample(links, src, n_iter):
+def ref_iteration_sample(links, src, n_iter, dims=DIMS, mass=MASS):
     """Time n_iter FP64 CG iterations of the reference's own solver
     (ks_d_congrad_fn.cpp, OpenMP on all host cores) on the full lattice."""
     import orc
 
     ref = capi.QphixLib(orc.REF_LIB)
-    ref.init(DIMS)
+    ref.init(dims)
     L = ref.create_L("D", links)
     b = ref.create_V("D", src, "even")
     x = ref.create_V("D", np.zeros_like(src), "even")
     t0 = time.perf_counter()
-    it, info, res = ref.invert("D", L, x, b, MASS, parity="even", max_iter=n_iter, nrestart=1, resid=RESID)
+    it, info, res = ref.invert("D", L, x, b, mass, parity="even", max_iter=n_iter, nrestart=1, resid=RESID)
     dt = time.perf_counter() - t0
     ref.destroy_V("D", b)
     ref.destroy_V("D", x)
@@ -664,6 +664,16 @@ def run_multishift(args):
     lib.destroy_L("D", L)
     out["autotuner"] = {k: lib.dslash_variant(k) for k in ("single", "double", "half-links")}
     lib.finalize()
+    if not args.no_cpu_baseline and "fp64_cg" in out:
+        import orc
+
+        if os.path.exists(orc.REF_LIB):
+            with _StdoutToStderr():
+                dt, done = ref_iteration_sample(links, src, 8, dims, MS_MASS)
+            out["cpu_baseline_fp64_cg"] = {
+                "s": dt / max(done, 1) * out["fp64_cg"]["iterations"], "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"{done} FP64 CG iterations of the reference solver on the full lattice ({dt:.1f} s), "
+                          f"scaled to the {out['fp64_cg']['iterations']} iterations of the FP64 solve"}
     print(json.dumps(out))
 
 
