@@ -319,7 +319,7 @@ def run_gpu(args):
         "config": {"workload": WORKLOAD, "lattice": "24x24x24x48", "mass": MASS, "resid_sq": RESID,
                    "reliable_delta": RU_DELTA,
                    "seeds": {"links": LINK_SEED, "source": SRC_SEED}, "parallelism": f"replicas{world}",
-                   "l2": "working set (links 0.76 GB FP32, 1.5 GB FP64) exceeds the 126 MB L2"},
+                   "l2": "working set (FP32 links 0.64 GB with 12-real Naik links, 0.76 GB with 18; FP64 1.5 GB) exceeds the 126 MB L2"},
         "solve": {"ms_each": [round(t, 3) for t in times], "links_compressed": compressed,
                   "iterations": int(np.median(iters)), "reliable_updates": int(np.median(rus)),
                   "true_rsq_rel": float(max(trues)), "err_vs_fp64_solution": err_vs_fp64},
@@ -714,6 +714,8 @@ def run_batch(args):
     pinned_src = [torch.from_numpy(s[2]).pin_memory().numpy() for s in systems]
     psys = [(l, m, p) for (l, m, _), p in zip(systems, pinned_src)]
 
+    batch_g = [0]
+
     def batch_solve():
         for o in outs:
             o[:] = 0.0
@@ -723,6 +725,7 @@ def run_batch(args):
                                              outs=outs)
         wall = time.perf_counter() - w0
         ms = lib.timer_stop()
+        batch_g[0] = lib.last_stats().batch_rhs_per_thread
         assert info.status == 0, lib.last_error()
         return max(ms / 1e3, wall), res, [x.copy() for x in xs]
 
@@ -738,7 +741,7 @@ def run_batch(args):
     if args.no_sequential:
         lib.finalize()
         print(json.dumps({"mode": "batch", "workload": BATCH_WORKLOAD, "batch_s": s_batch,
-                          "batch_iterations": [r.final_iter for r in res]}))
+                          "rhs_per_thread": batch_g[0], "batch_iterations": [r.final_iter for r in res]}))
         return
 
     # the same systems one at a time (FP32 inner, FP64 reliable updates)
@@ -772,6 +775,7 @@ def run_batch(args):
     print(json.dumps({
         "mode": "batch", "workload": BATCH_WORKLOAD, "systems": len(systems), "lattices": len(lats),
         "field_generation_s": gen_s, "batch_s": s_batch, "batch_all_s": times,
+        "rhs_per_thread": batch_g[0],
         "sequential_s": seq, "speedup_vs_sequential": seq / s_batch,
         "batch_iterations": [r.final_iter for r in res], "batch_reliable_updates": [r.final_restart for r in res],
         "sequential_iterations": seq_iters,

@@ -55,7 +55,7 @@ QPHIX_status_t QPHIX_B200_set_reliable_delta(double delta);
  * of the FP32 Dslash's bytes. */
 QPHIX_status_t QPHIX_B200_set_link_compression(int on);
 
-/* Diagnostics of the most recent invert / invert_multi call. */
+/* Diagnostics of the most recent invert / invert_multi / batch_invert call. */
 typedef struct {
   double solve_ms;        /* device time of the call (CUDA events) */
   int iterations;         /* Krylov iterations (all precisions) */
@@ -67,6 +67,7 @@ typedef struct {
   double true_rsq;        /* final |b - M x|^2 / |b|^2 (largest over masses) */
   int escalated;          /* 1 if a 16-bit inner solve stalled and continued in FP32 */
   int links_compressed;   /* 1 if the FP32 inner solve used 12-real Naik links */
+  int batch_rhs_per_thread; /* batched solves: systems per thread the FP32 Dslash tuner chose */
 } QPHIX_B200_stats_t;
 
 QPHIX_status_t QPHIX_B200_get_last_stats(QPHIX_B200_stats_t *stats);

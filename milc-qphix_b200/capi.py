@@ -81,7 +81,7 @@ class Stats(C.Structure):
                 ("reliable_updates", C.c_int), ("dslash_launches", C.c_int),
                 ("dslash_ms", C.c_double), ("mdagm_launches", C.c_int),
                 ("mdagm_ms", C.c_double), ("true_rsq", C.c_double), ("escalated", C.c_int),
-                ("links_compressed", C.c_int)]
+                ("links_compressed", C.c_int), ("batch_rhs_per_thread", C.c_int)]
 
 
 PRECISION = {"half": 0, "single": 1, "double": 2, "half-links": 3}

@@ -362,8 +362,8 @@ SloppyCfg sloppy_cfg(QPHIX_D3_FermionLinksAsqtad *H, int mode)
 {
     switch (mode) {
     case QPHIX_B200_PREC_SINGLE: return {Prec::Single, &single_inner_links(H), nullptr};
-    case QPHIX_B200_PREC_HALF: return {Prec::Half, &half_links(H), &single_links(H)};
-    case QPHIX_B200_PREC_HALF_LINKS: return {Prec::Single, &half_links(H), &single_links(H)};
+    case QPHIX_B200_PREC_HALF: return {Prec::Half, &half_links(H), &single_inner_links(H)};
+    case QPHIX_B200_PREC_HALF_LINKS: return {Prec::Single, &half_links(H), &single_inner_links(H)};
     default: throw Error("unknown inner precision");
     }
 }
@@ -632,6 +632,7 @@ QPHIX_status_t QPHIX_B200_get_last_stats(QPHIX_B200_stats_t *s)
         s->mdagm_ms = t.mdagm_ms;
         s->true_rsq = t.true_rsq;
         s->links_compressed = t.links_compressed;
+        s->batch_rhs_per_thread = t.batch_rhs_per_thread;
         s->escalated = t.escalated;
     });
 }

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -780,7 +781,7 @@ std::vector<SegPlan> plan_segments(int nlat, int nsys, const int *lat, std::vect
 // kind 0: FP32 Dslash (G = 3 for multiples of 3, else <= 4; measured: G = 4
 // at 2 blocks/SM beats G = 2 at 3 blocks/SM by 4-5 %), 1: FP64 Dslash (G = 3
 // for multiples of 3, else <= 2), 2: vector kernels
-BTable make_table(const std::vector<SegPlan> &plan, const std::vector<LatRef> &lats, int kind)
+BTable make_table(const std::vector<SegPlan> &plan, const std::vector<LatRef> &lats, int kind, int gpref = 4)
 {
     BTable t{};
     t.nseg = (int)plan.size();
@@ -803,7 +804,7 @@ BTable make_table(const std::vector<SegPlan> &plan, const std::vector<LatRef> &l
             g.lg_ngrp = log2i(ngrp);
             g.items = 3 * L.g->vh * ngrp;
         } else {
-            g.G = (n % 3 == 0) ? 3 : std::min(n, kind == 0 ? 4 : 2);
+            g.G = (n % 3 == 0) ? 3 : std::min(n, kind == 0 ? gpref : 2);
             g.lg_ngrp = log2i(n / g.G);
             g.items = L.g->vh * (n / g.G);
             const LinkSet &ls = kind == 0 ? *L.l32 : *L.l64;
@@ -823,6 +824,16 @@ BState *pinned_state()
     if (!h) QB_CUDA(cudaMallocHost(&h, sizeof(BState)));
     return h;
 }
+
+// QPHIX_B200_BATCH_G=4|2 skips the batched-Dslash tuning and uses that many
+// systems per thread where the segment size allows it
+int batch_tuning_forced()
+{
+    const char *e = std::getenv("QPHIX_B200_BATCH_G");
+    return (e && (e[0] == '4' || e[0] == '2')) ? e[0] - '0' : 0;
+}
+
+int last_batch_g = 0;  // systems per thread of the last batched solve's FP32 Dslash
 
 bool batch_graphs_enabled()
 {
@@ -950,7 +961,7 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
                const double *resid, int cb, int iter_cap, Load load, Store store)
 {
     Context &c = ctx();
-    const BTable tabs[3] = {make_table(plan, lats, 0), make_table(plan, lats, 1), make_table(plan, lats, 2)};
+    BTable tabs[3] = {make_table(plan, lats, 0), make_table(plan, lats, 1), make_table(plan, lats, 2)};
     long long ncx = 0;
     for (const auto &p : plan) ncx += 3LL * lats[p.lat].g->vh * p.nrhs;
 
@@ -1012,6 +1023,67 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
     BState *h = pinned_state();
     std::memset(h, 0, sizeof(BState));
     h->nsys = nsys;
+    // Autotuning of the FP32 batched Dslash: for segments whose size allows
+    // both, G = 4 or G = 2 systems per thread (registers against occupancy).
+    // Timed once per set of (lattice, segment size) on the solve's own
+    // fields, all systems active; the choice is kept for later solves.
+    {
+        static std::map<std::string, int> chosen;
+        std::string key;
+        bool choice = false;
+        for (const auto &p : plan) {
+            key += std::to_string(lats[p.lat].g->vh) + ":" + std::to_string(p.nrhs) + ",";
+            choice |= p.nrhs >= 4 && p.nrhs % 3 != 0;
+        }
+        auto it = chosen.find(key);
+        int gpref = 4;
+        if (batch_tuning_forced()) {
+            gpref = batch_tuning_forced();
+        } else if (it != chosen.end()) {
+            gpref = it->second;
+        } else if (choice) {
+            h->active_mask = nsys >= 64 ? ~0ull : ((1ull << nsys) - 1ull);
+            upload(d_st, h, c.stream);
+            float best = 0;
+            for (int g : {4, 2}) {
+                const BTable t = make_table(plan, lats, 0, g);
+                QB_CUDA(cudaMemcpyAsync(d_tabs, &t, sizeof(BTable), cudaMemcpyHostToDevice, c.stream));
+                int gm = 1;
+                for (int k = 0; k < t.nseg; ++k) gm = std::max(gm, t.seg[k].G);
+                const int gr = grid(gm > 2 ? rb_s0w : rb_s0, t.ntiles);
+                cudaEvent_t e0, e1;
+                QB_CUDA(cudaEventCreate(&e0));
+                QB_CUDA(cudaEventCreate(&e1));
+                for (int r = 0; r < 4; ++r) {
+                    if (r == 1) QB_CUDA(cudaEventRecord(e0, c.stream));
+                    if (gm > 2) k_bdslash_s<false, 4><<<gr, kBlock, 0, c.stream>>>(d_tabs, d_st, f.t32, f.p, f.p, 1 - cb, R.partials);
+                    else k_bdslash_s<false, 2><<<gr, kBlock, 0, c.stream>>>(d_tabs, d_st, f.t32, f.p, f.p, 1 - cb, R.partials);
+                }
+                QB_CUDA(cudaEventRecord(e1, c.stream));
+                QB_CUDA(cudaEventSynchronize(e1));
+                float ms = 0;
+                QB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                if (g == 4 || ms < best) {
+                    best = ms;
+                    gpref = g;
+                }
+            }
+            chosen[key] = gpref;
+            h->active_mask = 0;
+        }
+        last_batch_g = gpref;
+        if (gpref != 4) {
+            tabs[0] = make_table(plan, lats, 0, gpref);
+            gmax_s = 1;
+            for (int k = 0; k < tabs[0].nseg; ++k) gmax_s = std::max(gmax_s, tabs[0].seg[k].G);
+            R.gmax_s = gmax_s;
+            R.grid_s0 = grid(gmax_s > 2 ? rb_s0w : rb_s0, tabs[0].ntiles);
+            R.grid_s1 = grid(gmax_s > 2 ? rb_s1w : rb_s1, tabs[0].ntiles);
+        }
+        QB_CUDA(cudaMemcpyAsync(d_tabs, &tabs[0], sizeof(BTable), cudaMemcpyHostToDevice, c.stream));
+    }
     h->delta2 = c.reliable_delta * c.reliable_delta;
     h->iter_cap = std::max(1, iter_cap);
     for (int s = 0; s < nsys; ++s) {
@@ -1065,6 +1137,7 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
     sync_check();
     c.stats = Stats{};
     c.stats.iterations = h->iteration;
+    c.stats.batch_rhs_per_thread = last_batch_g;
     for (int k = 0; k < h->nsys; ++k) c.stats.reliable_updates += h->sys[k].reliable_updates;
 }
 

@@ -47,6 +47,7 @@ struct Stats {
     double true_rsq = 0;
     int escalated = 0;
     int links_compressed = 0;
+    int batch_rhs_per_thread = 0;
 };
 
 // CUDA-event timing of individual kernel launches inside a solve

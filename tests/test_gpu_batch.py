@@ -128,3 +128,32 @@ def test_batch_rejects_bad_arguments(batch):
     assert info.status != 0 and "nsys" in lib.last_error()
     bad = lib.batch_create_L([((6, 4, 4, 4), _links(1))])
     assert not bad and "Nx/2 must be even" in lib.last_error()
+
+
+def test_batch_dslash_tuner(batch):
+    """16 systems on one lattice: the tuner picks 4 or 2 systems per thread
+    for the FP32 batched Dslash; forcing the other choice gives the same
+    solutions to the solve tolerance."""
+    lib, B = batch
+    systems = [(0, 0.04 + 0.01 * (k % 5), synthetic.gaussian_source(LATS[0], seed=900 + k, parity="even"))
+               for k in range(16)]
+    _, info, res, xs = lib.batch_invert(B, systems, max_iter=4000, resid=RESID)
+    assert info.status == 0, lib.last_error()
+    g = lib.last_stats().batch_rhs_per_thread
+    assert g in (2, 4)
+    _check_solutions(systems, res, xs)
+    other = 2 if g == 4 else 4
+    old = os.environ.get("QPHIX_B200_BATCH_G")
+    os.environ["QPHIX_B200_BATCH_G"] = str(other)
+    try:
+        _, info2, _, xs2 = lib.batch_invert(B, systems, max_iter=4000, resid=RESID)
+        assert lib.last_stats().batch_rhs_per_thread == other
+    finally:
+        if old is None:
+            del os.environ["QPHIX_B200_BATCH_G"]
+        else:
+            os.environ["QPHIX_B200_BATCH_G"] = old
+    assert info2.status == 0
+    V = int(np.prod(LATS[0]))
+    for a, b in zip(xs, xs2):
+        assert rel_err(a[: V * 3], b[: V * 3]) < 1e-8
