@@ -140,6 +140,12 @@ template <> struct LinkView<float> {
             u[4 * c] = z.x; u[4 * c + 1] = z.y; u[4 * c + 2] = z.z; u[4 * c + 3] = z.w;
         }
     }
+    // the same 9 chunks, left packed (the pipelined Dslash unpacks them later)
+    __device__ __forceinline__ void fetch_pair(int d, int h, int j, float4 c[9]) const {
+        const float4 *q = p + ((size_t)d * 18 + 9 * h) * vh + j;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) c[k] = __ldcs(q + (size_t)k * vh);
+    }
 };
 
 // 16-bit fixed point: value = q * link_max / 32767 with one range for the fat
@@ -192,6 +198,28 @@ template <> struct LinkView<Recon12> {
         for (int e = 0; e < 12; ++e) {
             uf[e] = w[e];
             ub[e] = w[12 + e];
+        }
+        rebuild(uf, (bits >> (2 * d)) & 1u ? -scale : scale);
+        rebuild(ub, (bits >> (2 * d + 1)) & 1u ? -scale : scale);
+    }
+    // split forms of the two loads above, so a caller can issue the loads of
+    // one stage before the arithmetic of the previous one
+    __device__ __forceinline__ void fetch_fat(int d, int j, float4 c[9]) const {
+        const float4 *q = p + (size_t)d * kReconChunks * vh + j;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) c[k] = __ldcs(q + (size_t)k * vh);
+    }
+    __device__ __forceinline__ void fetch_naik(int d, int j, float4 c[6]) const {
+        const float4 *q = p + ((size_t)d * kReconChunks + 9) * vh + j;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) c[k] = __ldcs(q + (size_t)k * vh);
+    }
+    __device__ __forceinline__ void naik_from(const float4 c[6], int d, unsigned bits, float uf[18],
+                                              float ub[18]) const {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            uf[4 * k] = c[k].x; uf[4 * k + 1] = c[k].y; uf[4 * k + 2] = c[k].z; uf[4 * k + 3] = c[k].w;
+            ub[4 * k] = c[3 + k].x; ub[4 * k + 1] = c[3 + k].y; ub[4 * k + 2] = c[3 + k].z; ub[4 * k + 3] = c[3 + k].w;
         }
         rebuild(uf, (bits >> (2 * d)) & 1u ? -scale : scale);
         rebuild(ub, (bits >> (2 * d + 1)) & 1u ? -scale : scale);

@@ -55,38 +55,46 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
                 else mv_add(acc, u, v);
             }
         }
-    } else if constexpr (std::is_same<SL, float>::value) {
-        // FP32: forward/backward pair, 9 float4 + 2 neighbours per batch
-#pragma unroll
-        for (int d = 0; d < 4; ++d) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int kf = 8 * h + 2 * d + 1, kb = 8 * h + 2 * d;
-                A u[36], vf[6], vb[6];
-                a.in.load(neighbor(a.g, s, kf), vf);
-                a.in.load(neighbor(a.g, s, kb), vb);
-                a.links.load_pair(d, h, j, u);
-                mv_add(acc, u, vf);
-                mv_adj_sub(acc, u + 18, vb);
+    } else if constexpr (std::is_same<SL, float>::value || std::is_same<SL, Recon12>::value) {
+        // FP32: eight stages, the forward/backward pair of fat (h = 0) and of
+        // Naik (h = 1) links of each direction: 9 x 16 bytes, or 6 x 16 bytes
+        // for 12-real Naik links whose third rows are rebuilt from the site's
+        // sign bits.  Software-pipelined: the loads of stage i + 1 are issued
+        // before the arithmetic of stage i, so every thread keeps one stage of
+        // links and neighbours in flight.
+        constexpr bool R12 = std::is_same<SL, Recon12>::value;
+        unsigned bits = 0;
+        if constexpr (R12) bits = __ldg(a.links.sign + j);
+        float4 c[2][9];
+        A v[2][2][6];
+        auto issue = [&](int st, int b) {
+            const int d = st >> 1, h = st & 1;
+            a.in.load(neighbor(a.g, s, 8 * h + 2 * d + 1), v[b][0]);
+            a.in.load(neighbor(a.g, s, 8 * h + 2 * d), v[b][1]);
+            if constexpr (R12) {
+                if (h) a.links.fetch_naik(d, j, c[b]);
+                else a.links.fetch_fat(d, j, c[b]);
+            } else {
+                a.links.fetch_pair(d, h, j, c[b]);
             }
-        }
-    } else if constexpr (std::is_same<SL, Recon12>::value) {
-        // FP32 fat pair (9 x 16 bytes) + 12-real Naik pair (6 x 16 bytes) with
-        // their third rows rebuilt from the site's sign bits
-        const unsigned bits = __ldg(a.links.sign + j);
+        };
+        issue(0, 0);
 #pragma unroll
-        for (int d = 0; d < 4; ++d) {
-            A u[36], vf[6], vb[6];
-            a.in.load(neighbor(a.g, s, 2 * d + 1), vf);
-            a.in.load(neighbor(a.g, s, 2 * d), vb);
-            a.links.load_fat(d, j, u);
-            mv_add(acc, u, vf);
-            mv_adj_sub(acc, u + 18, vb);
-            a.in.load(neighbor(a.g, s, 8 + 2 * d + 1), vf);
-            a.in.load(neighbor(a.g, s, 8 + 2 * d), vb);
-            a.links.load_naik(d, j, bits, u, u + 18);
-            mv_add(acc, u, vf);
-            mv_adj_sub(acc, u + 18, vb);
+        for (int st = 0; st < 8; ++st) {
+            const int b = st & 1;
+            if (st + 1 < 8) issue(st + 1, b ^ 1);
+            A u[36];
+            if (R12 && (st & 1)) {
+                if constexpr (R12) a.links.naik_from(c[b], st >> 1, bits, u, u + 18);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) {
+                    u[4 * k] = c[b][k].x; u[4 * k + 1] = c[b][k].y;
+                    u[4 * k + 2] = c[b][k].z; u[4 * k + 3] = c[b][k].w;
+                }
+            }
+            mv_add(acc, u, v[b][0]);
+            mv_adj_sub(acc, u + 18, v[b][1]);
         }
     } else {
         // 16-bit: the four matrices of a direction, 9 x 16 bytes + 4 neighbours
@@ -109,10 +117,13 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
     }
 }
 
-// blocks of 256 per SM the register allocation must allow: the 12-real
-// kernel is latency-bound at 4 (56 registers), so it is held to 5
+// blocks of 256 per SM the register allocation must allow.  The pipelined
+// FP32 kernels keep one stage in flight in 80 registers at 3 blocks/SM.  In
+// the 24^3x48 mixed solve: 12-real 100.7 ms (4 blocks, 64 registers: 107.8
+// ms); 18-real 113.9 ms (1 block at 241 registers: 116.7 ms)
 template <typename SL> struct MinBlocks { static constexpr int value = 1; };
-template <> struct MinBlocks<Recon12> { static constexpr int value = 5; };
+template <> struct MinBlocks<float> { static constexpr int value = 3; };
+template <> struct MinBlocks<Recon12> { static constexpr int value = 3; };
 
 // Scalar step after p.(M^dag M p) is known: CG (mode 0) a = -rsq/pkp;
 // multi-shift (mode 1) the shift recurrences.  Runs in one thread.
