@@ -305,27 +305,32 @@ __device__ __forceinline__ void bsite(const BSeg &sg, int cb, int j, int q, cons
     // matrix is in chunks 0-4 and the backward one in chunks 4-8 (chunk 4
     // holds the last forward and the first backward complex).  Loading five
     // chunks per matrix keeps 20 link floats live instead of 36, which leaves
-    // registers for the G right-hand sides.
+    // registers for the G right-hand sides.  Sixteen stages (one matrix and
+    // its neighbour each), software-pipelined: the loads of stage i + 1 are
+    // issued before the arithmetic of stage i.
+    float4 wc[2][5];
+    float v[2][G][6];
+    auto issue = [&](int st, int b) {
+        const int d = st >> 2, h = (st >> 1) & 1, half = st & 1;
+        const float4 *pair = lv.p + ((size_t)d * 18 + 9 * h) * lv.vh + j;
 #pragma unroll
-    for (int d = 0; d < 4; ++d) {
+        for (int c = 0; c < 5; ++c) wc[b][c] = __ldcs(pair + (size_t)(4 * half + c) * lv.vh);
+        bload<G>(in, sg.g.vh, sg.nrhs, neighbor(sg.g, s, 8 * h + 2 * d + (half ? 0 : 1)), q, v[b]);
+    };
+    issue(0, 0);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const float4 *pair = lv.p + ((size_t)d * 18 + 9 * h) * lv.vh + j;
+    for (int st = 0; st < 16; ++st) {
+        const int b = st & 1;
+        if (st + 1 < 16) issue(st + 1, b ^ 1);
+        float w[20];
 #pragma unroll
-            for (int half = 0; half < 2; ++half) {
-                float w[20], v[G][6];
+        for (int c = 0; c < 5; ++c) {
+            w[4 * c] = wc[b][c].x; w[4 * c + 1] = wc[b][c].y; w[4 * c + 2] = wc[b][c].z; w[4 * c + 3] = wc[b][c].w;
+        }
 #pragma unroll
-                for (int c = 0; c < 5; ++c) {
-                    const float4 z = __ldcs(pair + (size_t)(4 * half + c) * lv.vh);
-                    w[4 * c] = z.x; w[4 * c + 1] = z.y; w[4 * c + 2] = z.z; w[4 * c + 3] = z.w;
-                }
-                bload<G>(in, sg.g.vh, sg.nrhs, neighbor(sg.g, s, 8 * h + 2 * d + (half ? 0 : 1)), q, v);
-#pragma unroll
-                for (int e = 0; e < G; ++e) {
-                    if (half) mv_adj_sub(acc[e], w + 2, v[e]);
-                    else mv_add(acc[e], w, v[e]);
-                }
-            }
+        for (int e = 0; e < G; ++e) {
+            if (st & 1) mv_adj_sub(acc[e], w + 2, v[b][e]);
+            else mv_add(acc[e], w, v[b][e]);
         }
     }
 }

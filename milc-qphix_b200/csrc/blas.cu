@@ -384,9 +384,11 @@ k_ms_update(VecBlock *xs, VecBlock *ps, VecView<S> r, int n, SolverState *st, in
 // passes the target.  The request cancels this iteration's p update, which the
 // host redoes with the true residual.
 
-template <typename S>
+// SX: storage of x_s (FP32 when the other vectors are 16-bit: a 16-bit
+// partial solution would round every update to the site's 15-bit range)
+template <typename SX, typename S>
 __global__ void __launch_bounds__(kBlock)
-k_mx_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverState *st,
+k_mx_update(VecView<SX> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverState *st,
             double *partials, int gate, double delta2)
 {
     using A = typename Acc<S>::type;
@@ -552,8 +554,9 @@ static void mx_impl(const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlo
 {
     const int vh = L.g->vh;
     if constexpr (std::is_same<S, __half>::value) {
-        k_mx_update<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(x, vh), view<S>(pv, vh), view<S>(r, vh),
-                                                              view<S>(ttt, vh), st, partials, gate, delta2);
+        k_mx_update<float, S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<float>(x, vh), view<S>(pv, vh),
+                                                                     view<S>(r, vh), view<S>(ttt, vh), st,
+                                                                     partials, gate, delta2);
     } else {
         using V = typename Wide<S>::type;
         const long long n = 6LL * vh / Wide<S>::n;
@@ -594,9 +597,7 @@ void vec_copy(Prec dst_p, VecBlock dst, Prec src_p, VecBlock src, const Launch &
 
 void vec_zero(Prec p, VecBlock v, const Launch &L)
 {
-    const size_t n = (size_t)3 * L.g->vh * (p == Prec::Double ? 16 : (p == Prec::Single ? 8 : 4));
-    cudaMemsetAsync(v.data, 0, n, L.stream);
-    if (p == Prec::Half) cudaMemsetAsync(v.norm, 0, sizeof(float) * L.g->vh, L.stream);
+    cudaMemsetAsync(v.data, 0, vec_bytes(p, L.g->vh), L.stream);
 }
 
 template <typename Y, typename X>

@@ -49,22 +49,15 @@ VecBlock alloc_vec(Prec p)
 {
     Context &c = ctx();
     VecBlock b;
-    const size_t n = (size_t)3 * c.g.vh;
-    b.data = dev_alloc(n * cx_bytes(p));
-    QB_CUDA(cudaMemsetAsync(b.data, 0, n * cx_bytes(p), c.stream));
-    if (p == Prec::Half) {
-        b.norm = static_cast<float *>(dev_alloc(sizeof(float) * c.g.vh));
-        QB_CUDA(cudaMemsetAsync(b.norm, 0, sizeof(float) * c.g.vh, c.stream));
-    }
+    b.data = dev_alloc(vec_bytes(p, c.g.vh));
+    QB_CUDA(cudaMemsetAsync(b.data, 0, vec_bytes(p, c.g.vh), c.stream));
     return b;
 }
 
 void free_vec(VecBlock &b)
 {
     dev_free(b.data);
-    dev_free(b.norm);
     b.data = nullptr;
-    b.norm = nullptr;
 }
 
 LinkSet alloc_links(Prec p) { return alloc_links(p, ctx().g.vh); }

@@ -58,21 +58,22 @@ template <> struct VecView<float> {
 
 // 16-bit storage: per-site norm = max |component| of the site (float), each
 // component stored as 16-bit fixed point q = round(32767 v / norm).  Inside a
-// normalised site fixed point keeps 15 bits where FP16 keeps 11.
+// normalised site fixed point keeps 15 bits where FP16 keeps 11.  A site is
+// one 16-byte record {q0|q1, q2|q3, q4|q5, norm}.
 template <> struct VecView<__half> {
-    short2 *p;
-    float *norm;
+    int4 *p;
     int vh;
-    __device__ __forceinline__ void load(int j, float v[6]) const {
-        const float n = __ldg(norm + j) * (1.0f / 32767.0f);
-        const short2 a = __ldg(p + j), b = __ldg(p + vh + j), c = __ldg(p + 2 * vh + j);
-        v[0] = a.x * n; v[1] = a.y * n; v[2] = b.x * n; v[3] = b.y * n; v[4] = c.x * n; v[5] = c.y * n;
+    static __device__ __forceinline__ void unpack(const int4 w, float v[6]) {
+        const float n = __int_as_float(w.w) * (1.0f / 32767.0f);
+        const int q[3] = {w.x, w.y, w.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            v[2 * k] = (float)(short)(q[k] & 0xffff) * n;
+            v[2 * k + 1] = (float)(short)((unsigned)q[k] >> 16) * n;
+        }
     }
-    __device__ __forceinline__ void load_cg(int j, float v[6]) const {
-        const float n = __ldcg(norm + j) * (1.0f / 32767.0f);
-        const short2 a = __ldcg(p + j), b = __ldcg(p + vh + j), c = __ldcg(p + 2 * vh + j);
-        v[0] = a.x * n; v[1] = a.y * n; v[2] = b.x * n; v[3] = b.y * n; v[4] = c.x * n; v[5] = c.y * n;
-    }
+    __device__ __forceinline__ void load(int j, float v[6]) const { unpack(__ldg(p + j), v); }
+    __device__ __forceinline__ void load_cg(int j, float v[6]) const { unpack(__ldcg(p + j), v); }
     // Stores v and replaces it by the value a later load returns, so callers
     // never read back what they just wrote (a read-only-path load of data
     // written by the same kernel is not coherent).
@@ -82,16 +83,15 @@ template <> struct VecView<__half> {
         for (int k = 0; k < 6; ++k) m = fmaxf(m, fabsf(v[k]));
         const float inv = m > 0.f ? 32767.0f / m : 0.f;
         const float n = m * (1.0f / 32767.0f);
-        short q[6];
+        int q[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            q[k] = (short)__float2int_rn(v[k] * inv);
-            v[k] = q[k] * n;
+            q[k] = __float2int_rn(v[k] * inv);
+            v[k] = (float)q[k] * n;
         }
-        norm[j] = m;
-        p[j] = make_short2(q[0], q[1]);
-        p[vh + j] = make_short2(q[2], q[3]);
-        p[2 * vh + j] = make_short2(q[4], q[5]);
+        p[j] = make_int4((int)(((unsigned)q[0] & 0xffffu) | ((unsigned)q[1] << 16)),
+                         (int)(((unsigned)q[2] & 0xffffu) | ((unsigned)q[3] << 16)),
+                         (int)(((unsigned)q[4] & 0xffffu) | ((unsigned)q[5] << 16)), __float_as_int(m));
     }
 };
 
@@ -103,7 +103,7 @@ template <> __host__ __device__ inline VecView<float> view<float>(VecBlock b, in
     return VecView<float>{static_cast<float2 *>(b.data), vh};
 }
 template <> __host__ __device__ inline VecView<__half> view<__half>(VecBlock b, int vh) {
-    return VecView<__half>{static_cast<short2 *>(b.data), b.norm, vh};
+    return VecView<__half>{static_cast<int4 *>(b.data), vh};
 }
 
 // ------------------------------------------------------------------ links --

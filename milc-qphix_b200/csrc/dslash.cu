@@ -97,33 +97,43 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
             mv_adj_sub(acc, u + 18, v[b][1]);
         }
     } else {
-        // 16-bit: the four matrices of a direction, 9 x 16 bytes + 4 neighbours
-#pragma unroll
-        for (int d = 0; d < 4; ++d) {
-            int4 raw[9];
-            A v[4][6];
+        // 16-bit links: the four matrices of a direction, 9 x 16 bytes + 4
+        // neighbours per stage, pipelined over the directions like FP32
+        int4 raw[2][9];
+        A v[2][4][6];
+        auto issue = [&](int d, int b) {
 #pragma unroll
             for (int sl = 0; sl < 4; ++sl)
-                a.in.load(neighbor(a.g, s, (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1)), v[sl]);
-            a.links.load_quad(d, j, raw);
+                a.in.load(neighbor(a.g, s, (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1)), v[b][sl]);
+            a.links.load_quad(d, j, raw[b]);
+        };
+        issue(0, 0);
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const int b = d & 1;
+            if (d + 1 < 4) issue(d + 1, b ^ 1);
 #pragma unroll
             for (int sl = 0; sl < 4; ++sl) {
                 A u[18];
-                a.links.unpack(raw, sl, u);
-                if (sl & 1) mv_adj_sub(acc, u, v[sl]);
-                else mv_add(acc, u, v[sl]);
+                a.links.unpack(raw[b], sl, u);
+                if (sl & 1) mv_adj_sub(acc, u, v[b][sl]);
+                else mv_add(acc, u, v[b][sl]);
             }
         }
     }
 }
 
 // blocks of 256 per SM the register allocation must allow.  The pipelined
-// FP32 kernels keep one stage in flight in 80 registers at 3 blocks/SM.  In
-// the 24^3x48 mixed solve: 12-real 100.7 ms (4 blocks, 64 registers: 107.8
-// ms); 18-real 113.9 ms (1 block at 241 registers: 116.7 ms)
-template <typename SL> struct MinBlocks { static constexpr int value = 1; };
-template <> struct MinBlocks<float> { static constexpr int value = 3; };
-template <> struct MinBlocks<Recon12> { static constexpr int value = 3; };
+// kernels keep one stage in flight in 80 registers at 3 blocks/SM (2 with
+// 16-bit vectors, whose per-neighbour loads are smaller and more numerous).
+// 24^3x48 mixed solves: 12-real 100.7 ms (4 blocks: 107.8 ms); 18-real
+// 113.9 ms (1 block at 241 registers: 116.7 ms); 16-bit links 93.6 ms (1
+// block: 118.1 ms); 16-bit vectors and links 216.5 ms (3 blocks: 224.5 ms)
+template <typename SV, typename SL> struct MinBlocks { static constexpr int value = 1; };
+template <> struct MinBlocks<float, float> { static constexpr int value = 3; };
+template <> struct MinBlocks<float, Recon12> { static constexpr int value = 3; };
+template <> struct MinBlocks<float, __half> { static constexpr int value = 3; };
+template <> struct MinBlocks<__half, __half> { static constexpr int value = 2; };
 
 // Scalar step after p.(M^dag M p) is known: CG (mode 0) a = -rsq/pkp;
 // multi-shift (mode 1) the shift recurrences.  Runs in one thread.
@@ -171,7 +181,7 @@ __device__ __forceinline__ void mdagm_finalize(SolverState *st, double pkp, int 
 }
 
 template <typename SV, typename SL>
-__global__ void __launch_bounds__(kBlock, MinBlocks<SL>::value) k_dslash(DslashArgs<SV, SL> a, const SolverState *st, int gate)
+__global__ void __launch_bounds__(kBlock, MinBlocks<SV, SL>::value) k_dslash(DslashArgs<SV, SL> a, const SolverState *st, int gate)
 {
     using A = typename Acc<SV>::type;
     if (st && gated_off(st, gate)) return;
@@ -185,7 +195,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<SL>::value) k_dslash(DslashA
 // ttt = D tmp + m4 * p ;  pkp = sum p . ttt  (calc_pkp, ks_d_congrad_fn.cpp:159-171;
 // ks_multicg_offset.cpp:107-122), then the scalar step of the solver.
 template <typename SV, typename SL>
-__global__ void __launch_bounds__(kBlock, MinBlocks<SL>::value)
+__global__ void __launch_bounds__(kBlock, MinBlocks<SV, SL>::value)
 k_dslash_mdagm(DslashArgs<SV, SL> a, VecView<SV> pv, double m4, SolverState *st, double *partials,
                int gate, int mode)
 {
@@ -502,20 +512,14 @@ static int tuned_variant(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV,
     TuneEntry &t = g_tune[(int)pv][link_slot<SL>(pl)];
     if (t.vh == L.g->vh) return t.variant;
     // time the variants on scratch vectors so no caller data is touched twice
-    const size_t cx = pv == Prec::Double ? 16 : (pv == Prec::Single ? 8 : 4);
+    const size_t vb = vec_bytes(pv, L.g->vh);
     void *vin = nullptr, *vout = nullptr;
-    float *nin = nullptr, *nout = nullptr;
-    cudaMallocAsync(&vin, 3 * cx * L.g->vh, L.stream);
-    cudaMallocAsync(&vout, 3 * cx * L.g->vh, L.stream);
-    cudaMemsetAsync(vin, 0, 3 * cx * L.g->vh, L.stream);
-    if (pv == Prec::Half) {
-        cudaMallocAsync(&nin, sizeof(float) * L.g->vh, L.stream);
-        cudaMallocAsync(&nout, sizeof(float) * L.g->vh, L.stream);
-        cudaMemsetAsync(nin, 0, sizeof(float) * L.g->vh, L.stream);
-    }
+    cudaMallocAsync(&vin, vb, L.stream);
+    cudaMallocAsync(&vout, vb, L.stream);
+    cudaMemsetAsync(vin, 0, vb, L.stream);
     DslashArgs<SV, SL> s = a;
-    s.in = view<SV>(VecBlock{vin, nin}, L.g->vh);
-    s.out = view<SV>(VecBlock{vout, nout}, L.g->vh);
+    s.in = view<SV>(VecBlock{vin}, L.g->vh);
+    s.out = view<SV>(VecBlock{vout}, L.g->vh);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -535,8 +539,6 @@ static int tuned_variant(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV,
     cudaEventDestroy(e1);
     cudaFreeAsync(vin, L.stream);
     cudaFreeAsync(vout, L.stream);
-    if (nin) cudaFreeAsync(nin, L.stream);
-    if (nout) cudaFreeAsync(nout, L.stream);
     t.vh = L.g->vh;
     t.variant = best;
     return best;
@@ -618,30 +620,22 @@ static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashAr
     TuneEntry &t = g_tune_mdagm[(int)pv][link_slot<SL>(pl)];
     if (t.vh == L.g->vh) return t.variant;
     // scratch vectors, solver state and partials: no caller data is touched
-    const size_t cx = pv == Prec::Double ? 16 : (pv == Prec::Single ? 8 : 4);
+    const size_t vb = vec_bytes(pv, L.g->vh);
     void *vin = nullptr, *vout = nullptr, *vp = nullptr;
-    float *nin = nullptr, *nout = nullptr, *np = nullptr;
     SolverState *st = nullptr;
     double *part = nullptr;
-    cudaMallocAsync(&vin, 3 * cx * L.g->vh, L.stream);
-    cudaMallocAsync(&vout, 3 * cx * L.g->vh, L.stream);
-    cudaMallocAsync(&vp, 3 * cx * L.g->vh, L.stream);
-    cudaMemsetAsync(vin, 0, 3 * cx * L.g->vh, L.stream);
-    cudaMemsetAsync(vp, 0, 3 * cx * L.g->vh, L.stream);
-    if (pv == Prec::Half) {
-        cudaMallocAsync(&nin, sizeof(float) * L.g->vh, L.stream);
-        cudaMallocAsync(&nout, sizeof(float) * L.g->vh, L.stream);
-        cudaMallocAsync(&np, sizeof(float) * L.g->vh, L.stream);
-        cudaMemsetAsync(nin, 0, sizeof(float) * L.g->vh, L.stream);
-        cudaMemsetAsync(np, 0, sizeof(float) * L.g->vh, L.stream);
-    }
+    cudaMallocAsync(&vin, vb, L.stream);
+    cudaMallocAsync(&vout, vb, L.stream);
+    cudaMallocAsync(&vp, vb, L.stream);
+    cudaMemsetAsync(vin, 0, vb, L.stream);
+    cudaMemsetAsync(vp, 0, vb, L.stream);
     cudaMallocAsync(&st, sizeof(SolverState), L.stream);
     cudaMemsetAsync(st, 0, sizeof(SolverState), L.stream);
     cudaMallocAsync(&part, sizeof(double) * 4 * kMaxPartials, L.stream);
     DslashArgs<SV, SL> s = a;
-    s.in = view<SV>(VecBlock{vin, nin}, L.g->vh);
-    s.out = view<SV>(VecBlock{vout, nout}, L.g->vh);
-    const VecView<SV> p = view<SV>(VecBlock{vp, np}, L.g->vh);
+    s.in = view<SV>(VecBlock{vin}, L.g->vh);
+    s.out = view<SV>(VecBlock{vout}, L.g->vh);
+    const VecView<SV> p = view<SV>(VecBlock{vp}, L.g->vh);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -659,7 +653,7 @@ static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashAr
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    for (void *q : {vin, vout, vp, (void *)nin, (void *)nout, (void *)np, (void *)st, (void *)part})
+    for (void *q : {vin, vout, vp, (void *)st, (void *)part})
         if (q) cudaFreeAsync(q, L.stream);
     t.vh = L.g->vh;
     t.variant = best;

@@ -21,9 +21,10 @@ namespace qb {
 //                  c2[c*Vh + j]  (double2 / float2).  A warp reading 32
 //                  consecutive sites issues one fully used 512 B / 256 B
 //                  transaction per component.
-// 16-bit vector  : short2 q[c*Vh + j], 16-bit fixed point of v/norm[j],
-//                  float norm[j] = max |component| of the site (per-site
-//                  scaling).
+// 16-bit vector  : one 16-byte record per site, int4 rec[j] = {q0|q1,
+//                  q2|q3, q4|q5, norm}: the 6 reals as 16-bit fixed point of
+//                  v/norm and the float norm = max |component| of the site
+//                  (per-site scaling), so a neighbour gather is one load.
 // Link block     : the 16 matrices an output site needs, grouped by
 //                  direction d: slot s = 0 fat forward F_d(x), 1 fat backward
 //                  B_d(x), 2 Naik forward L_d(x), 3 Naik backward LB_d(x);
@@ -61,9 +62,11 @@ inline size_t prec_real_bytes(Prec p) { return p == Prec::Double ? 8 : (p == Pre
 
 // One parity block of a colour vector in device memory.
 struct VecBlock {
-    void *data = nullptr;   // cx_t<R>[3*Vh]   (16-bit: short2[3*Vh])
-    float *norm = nullptr;  // half only: float[Vh]
+    void *data = nullptr;   // cx_t<R>[3*Vh]   (16-bit: int4[Vh])
 };
+
+// bytes of one parity block of a colour vector
+inline size_t vec_bytes(Prec p, size_t vh) { return vh * (p == Prec::Double ? 48 : (p == Prec::Single ? 24 : 16)); }
 
 // Link blocks of both output parities.
 struct LinkSet {
@@ -211,9 +214,11 @@ void cg_true_residual(Prec p, const Launch &L, VecBlock ttt, VecBlock x, VecBloc
 void norm2_dev(Prec p, const Launch &L, VecBlock v, SolverState *st, double *partials, double *out);
 
 // Mixed-precision CG inner-loop kernels (sloppy precision p, FP64 reductions)
-// state: rsq (sloppy), pkp, a, b as for CG; reliable-update trigger in host
+// state: rsq (sloppy), pkp, a, b as for CG; reliable-update trigger in host.
+// x is FP32 when p is Half (see inner_x_prec)
 void mx_update(Prec p, const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlock ttt,
                SolverState *st, double *partials, int gate, double delta2);
+inline Prec inner_x_prec(Prec p) { return p == Prec::Half ? Prec::Single : p; }
 
 // layout remap (remap.cu) -------------------------------------------------------
 // raw MILC block (6 reals/site, AoS) <-> device block

@@ -86,7 +86,7 @@ extern "C" QPHIX_status_t QPHIX_B200_D3_asqtad_mdagm_noalloc(QPHIX_D3_FermionLin
         unsigned char *base = scratch_for_current_device();
         SolverState *st = reinterpret_cast<SolverState *>(base);
         double *partials = reinterpret_cast<double *>(base + kStateBytes);
-        VecBlock tmp{base + kStateBytes + kPartialBytes, nullptr};
+        VecBlock tmp{base + kStateBytes + kPartialBytes};
         const Launch Lh = c.launch();
         // the grid reduction needs its arrival counter at zero; clear the whole
         // scalar block so nothing of an earlier call is read

@@ -414,7 +414,8 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
     }
     Ws ws;
     VecBlock tmp64 = ws.get(Prec::Double), ttt64 = ws.get(Prec::Double), r64 = ws.get(Prec::Double);
-    VecBlock xs = ws.get(ps), rs = ws.get(ps), pv = ws.get(ps), tmps = ws.get(ps), ttts = ws.get(ps);
+    // the partial solution x_s is FP32 under a 16-bit inner solve
+    VecBlock xs = ws.get(inner_x_prec(ps)), rs = ws.get(ps), pv = ws.get(ps), tmps = ws.get(ps), ttts = ws.get(ps);
 
     auto true_residual = [&]() {
         S.msq_x4 = m4;
@@ -434,7 +435,7 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
 
     vec_copy(ps, rs, Prec::Double, r64, L);
     vec_copy(ps, pv, ps, rs, L);
-    vec_zero(ps, xs, L);
+    vec_zero(inner_x_prec(ps), xs, L);
     S.rsq = rsq;
     S.rsq_ru = rsq;
     S.rsqstop = tol * bnorm;
@@ -471,8 +472,8 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
         const double oldrsq = S.oldrsq;
         const double sloppy_rsq = S.rsq;
         // reliable update: x += x_s, r = b - M x in FP64
-        vec_add(Prec::Double, x, ps, xs, L);
-        vec_zero(ps, xs, L);
+        vec_add(Prec::Double, x, inner_x_prec(ps), xs, L);
+        vec_zero(inner_x_prec(ps), xs, L);
         const double prev_true = rsq;
         rsq = true_residual();
         out.reliable_updates++;
