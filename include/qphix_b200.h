@@ -21,8 +21,8 @@ extern "C" {
  * SINGLE:     FP32 inner CG with FP64 reliable updates; FP64 solution, FP64
  *             reductions; converges on the FP64 true residual.
  * HALF:       16-bit inner CG: vectors as 16-bit fixed point with a per-site
- *             norm, 16-bit fixed-point links, FP32 arithmetic; FP64
- *             reliable updates.
+ *             norm, 16-bit fixed-point links, FP32 arithmetic and an FP32
+ *             partial solution; FP64 reliable updates.
  * HALF_LINKS: FP32 vectors with 16-bit fixed-point links (half the link
  *             bytes of SINGLE); FP64 reliable updates.
  * A 16-bit inner solve that stops reducing the true residual continues
