@@ -51,8 +51,8 @@ DSLASH_BYTES_R12 = 1012  # FP32 with 12-real Naik links: 8x72 + 8x48 + 4 (sign w
 # DRAM bytes per output site of one K1 launch measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum / Vh): 264.33 MB at 24^3x32
 K1_TRAFFIC_PER_SITE_F32 = 264.33e6 / 221184
-# 332.48 MB (327.83 read + 4.65 write) at 24^3x48 for k_dslash<float, Recon12>
-K1_TRAFFIC_PER_SITE_R12 = 332.477696e6 / 331776
+# 332.36 MB (327.83 read + 4.53 write) at 24^3x48 for the pipelined k_dslash<float, Recon12>
+K1_TRAFFIC_PER_SITE_R12 = 332.361728e6 / 331776
 DSLASH_FLOPS = 1146
 METRIC = "time to |r|/|b|<1e-10, mixed vs FP64 CG on 1 B200; Dslash HBM GB/s"
 WORKLOAD = ("asqtad mixed-precision CG 24^3x48 m=0.01 tol 1e-10 (FP32 inner with 12-real Naik links, "

@@ -397,7 +397,7 @@ __device__ __forceinline__ void bdslash_s_item(int item, int cb, float2 *out, co
 // GMAX: largest G of the table's segments.  With G <= 2 the kernel fits in
 // 80 registers (3 blocks of 256 per SM); G = 3, 4 need 128 (2 blocks).
 template <bool MDAGM, int GMAX>
-__global__ void __launch_bounds__(kBlock, GMAX <= 2 ? 3 : 2) k_bdslash_s(const BTable *tab, BState *st, float2 *out,
+__global__ void __launch_bounds__(kBlock, GMAX == 1 ? 4 : (GMAX == 2 ? 3 : 2)) k_bdslash_s(const BTable *tab, BState *st, float2 *out,
                                                          const float2 *in, const float2 *pv, int cb,
                                                          double *partials)
 {
@@ -426,8 +426,10 @@ __global__ void __launch_bounds__(kBlock, GMAX <= 2 ? 3 : 2) k_bdslash_s(const B
                 if (sh.seg.G == 4) bdslash_s_item<4, MDAGM>(item, cb, out, in, pv, sh, acc);
                 else if (sh.seg.G == 3) bdslash_s_item<3, MDAGM>(item, cb, out, in, pv, sh, acc);
             }
-            if (sh.seg.G == 2) bdslash_s_item<2, MDAGM>(item, cb, out, in, pv, sh, acc);
-            else if (sh.seg.G == 1) bdslash_s_item<1, MDAGM>(item, cb, out, in, pv, sh, acc);
+            if constexpr (GMAX > 1) {
+                if (sh.seg.G == 2) bdslash_s_item<2, MDAGM>(item, cb, out, in, pv, sh, acc);
+            }
+            if (sh.seg.G == 1) bdslash_s_item<1, MDAGM>(item, cb, out, in, pv, sh, acc);
         }
     }
     if constexpr (MDAGM) {
@@ -830,12 +832,12 @@ BState *pinned_state()
     return h;
 }
 
-// QPHIX_B200_BATCH_G=4|2 skips the batched-Dslash tuning and uses that many
-// systems per thread where the segment size allows it
+// QPHIX_B200_BATCH_G=4|2|1 skips the batched-Dslash tuning and uses that
+// many systems per thread where the segment size allows it
 int batch_tuning_forced()
 {
     const char *e = std::getenv("QPHIX_B200_BATCH_G");
-    return (e && (e[0] == '4' || e[0] == '2')) ? e[0] - '0' : 0;
+    return (e && (e[0] == '4' || e[0] == '2' || e[0] == '1')) ? e[0] - '0' : 0;
 }
 
 int last_batch_g = 0;  // systems per thread of the last batched solve's FP32 Dslash
@@ -870,9 +872,12 @@ struct BatchRun {
         if (gmax_s > 2) {
             k_bdslash_s<false, 4><<<grid_s0, kBlock, 0, stream>>>(tab_s, st, f.t32, f.p, f.p, other, partials);
             k_bdslash_s<true, 4><<<grid_s1, kBlock, 0, stream>>>(tab_s, st, f.ap, f.t32, f.p, cb, partials);
-        } else {
+        } else if (gmax_s == 2) {
             k_bdslash_s<false, 2><<<grid_s0, kBlock, 0, stream>>>(tab_s, st, f.t32, f.p, f.p, other, partials);
             k_bdslash_s<true, 2><<<grid_s1, kBlock, 0, stream>>>(tab_s, st, f.ap, f.t32, f.p, cb, partials);
+        } else {
+            k_bdslash_s<false, 1><<<grid_s0, kBlock, 0, stream>>>(tab_s, st, f.t32, f.p, f.p, other, partials);
+            k_bdslash_s<true, 1><<<grid_s1, kBlock, 0, stream>>>(tab_s, st, f.ap, f.t32, f.p, cb, partials);
         }
         k_bvec<kBUpdate><<<grid_v[kBUpdate], kBlock, 0, stream>>>(tab_v, st, f, partials);
         k_bvec<kBAxpy><<<grid_v[kBAxpy], kBlock, 0, stream>>>(tab_v, st, f, partials);
@@ -990,11 +995,13 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
 
     int gmax_s = 1;
     for (int s = 0; s < tabs[0].nseg; ++s) gmax_s = std::max(gmax_s, tabs[0].seg[s].G);
-    static int rb_s0 = 0, rb_s1, rb_s0w, rb_s1w, rb_d0, rb_d1, rb_v[5];
+    static int rb_s0 = 0, rb_s1, rb_s0w, rb_s1w, rb_s0n, rb_s1n, rb_d0, rb_d1, rb_v[5];
     if (!rb_s0) {
         rb_s1 = resident_blocks(k_bdslash_s<true, 2>);
         rb_s0w = resident_blocks(k_bdslash_s<false, 4>);
         rb_s1w = resident_blocks(k_bdslash_s<true, 4>);
+        rb_s0n = resident_blocks(k_bdslash_s<false, 1>);
+        rb_s1n = resident_blocks(k_bdslash_s<true, 1>);
         rb_d0 = resident_blocks(k_bdslash_d<false>);
         rb_d1 = resident_blocks(k_bdslash_d<true>);
         rb_v[0] = resident_blocks(k_bvec<0>);
@@ -1005,13 +1012,17 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
         rb_s0 = resident_blocks(k_bdslash_s<false, 2>);
     }
     auto grid = [](int res_blocks, int ntiles) { return std::max(1, std::min(res_blocks, ntiles)); };
+    // resident blocks of the FP32 Dslash kernel for the table's largest G
+    auto rb_s = [&](int gm, bool mdagm) {
+        return gm > 2 ? (mdagm ? rb_s1w : rb_s0w) : gm == 2 ? (mdagm ? rb_s1 : rb_s0) : (mdagm ? rb_s1n : rb_s0n);
+    };
     BatchRun R{};
     R.tab_s = d_tabs;
     R.tab_d = d_tabs + 1;
     R.tab_v = d_tabs + 2;
     R.gmax_s = gmax_s;
-    R.grid_s0 = grid(gmax_s > 2 ? rb_s0w : rb_s0, tabs[0].ntiles);
-    R.grid_s1 = grid(gmax_s > 2 ? rb_s1w : rb_s1, tabs[0].ntiles);
+    R.grid_s0 = grid(rb_s(gmax_s, false), tabs[0].ntiles);
+    R.grid_s1 = grid(rb_s(gmax_s, true), tabs[0].ntiles);
     R.grid_d0 = grid(rb_d0, tabs[1].ntiles);
     R.grid_d1 = grid(rb_d1, tabs[1].ntiles);
     for (int i = 0; i < 5; ++i) R.grid_v[i] = grid(rb_v[i], tabs[2].ntiles);
@@ -1029,7 +1040,10 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
     std::memset(h, 0, sizeof(BState));
     h->nsys = nsys;
     // Autotuning of the FP32 batched Dslash: for segments whose size allows
-    // both, G = 4 or G = 2 systems per thread (registers against occupancy).
+    // it, G = 4, 2 or 1 systems per thread (registers against occupancy).
+    // With G = 1 the 16 lanes of a 16-system segment share one site: every
+    // colour component is one 128-byte run per site and the kernel fits in
+    // 64 registers (4 blocks/SM).
     // Timed once per set of (lattice, segment size) on the solve's own
     // fields, all systems active; the choice is kept for later solves.
     {
@@ -1038,7 +1052,7 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
         bool choice = false;
         for (const auto &p : plan) {
             key += std::to_string(lats[p.lat].g->vh) + ":" + std::to_string(p.nrhs) + ",";
-            choice |= p.nrhs >= 4 && p.nrhs % 3 != 0;
+            choice |= p.nrhs >= 2 && p.nrhs % 3 != 0;
         }
         auto it = chosen.find(key);
         int gpref = 4;
@@ -1050,19 +1064,20 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
             h->active_mask = nsys >= 64 ? ~0ull : ((1ull << nsys) - 1ull);
             upload(d_st, h, c.stream);
             float best = 0;
-            for (int g : {4, 2}) {
+            for (int g : {4, 2, 1}) {
                 const BTable t = make_table(plan, lats, 0, g);
                 QB_CUDA(cudaMemcpyAsync(d_tabs, &t, sizeof(BTable), cudaMemcpyHostToDevice, c.stream));
                 int gm = 1;
                 for (int k = 0; k < t.nseg; ++k) gm = std::max(gm, t.seg[k].G);
-                const int gr = grid(gm > 2 ? rb_s0w : rb_s0, t.ntiles);
+                const int gr = grid(rb_s(gm, false), t.ntiles);
                 cudaEvent_t e0, e1;
                 QB_CUDA(cudaEventCreate(&e0));
                 QB_CUDA(cudaEventCreate(&e1));
                 for (int r = 0; r < 4; ++r) {
                     if (r == 1) QB_CUDA(cudaEventRecord(e0, c.stream));
                     if (gm > 2) k_bdslash_s<false, 4><<<gr, kBlock, 0, c.stream>>>(d_tabs, d_st, f.t32, f.p, f.p, 1 - cb, R.partials);
-                    else k_bdslash_s<false, 2><<<gr, kBlock, 0, c.stream>>>(d_tabs, d_st, f.t32, f.p, f.p, 1 - cb, R.partials);
+                    else if (gm == 2) k_bdslash_s<false, 2><<<gr, kBlock, 0, c.stream>>>(d_tabs, d_st, f.t32, f.p, f.p, 1 - cb, R.partials);
+                    else k_bdslash_s<false, 1><<<gr, kBlock, 0, c.stream>>>(d_tabs, d_st, f.t32, f.p, f.p, 1 - cb, R.partials);
                 }
                 QB_CUDA(cudaEventRecord(e1, c.stream));
                 QB_CUDA(cudaEventSynchronize(e1));
@@ -1084,8 +1099,8 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
             gmax_s = 1;
             for (int k = 0; k < tabs[0].nseg; ++k) gmax_s = std::max(gmax_s, tabs[0].seg[k].G);
             R.gmax_s = gmax_s;
-            R.grid_s0 = grid(gmax_s > 2 ? rb_s0w : rb_s0, tabs[0].ntiles);
-            R.grid_s1 = grid(gmax_s > 2 ? rb_s1w : rb_s1, tabs[0].ntiles);
+            R.grid_s0 = grid(rb_s(gmax_s, false), tabs[0].ntiles);
+            R.grid_s1 = grid(rb_s(gmax_s, true), tabs[0].ntiles);
         }
         QB_CUDA(cudaMemcpyAsync(d_tabs, &tabs[0], sizeof(BTable), cudaMemcpyHostToDevice, c.stream));
     }

@@ -131,8 +131,8 @@ def test_batch_rejects_bad_arguments(batch):
 
 
 def test_batch_dslash_tuner(batch):
-    """16 systems on one lattice: the tuner picks 4 or 2 systems per thread
-    for the FP32 batched Dslash; forcing the other choice gives the same
+    """16 systems on one lattice: the tuner picks 4, 2 or 1 systems per
+    thread for the FP32 batched Dslash; forcing another choice gives the same
     solutions to the solve tolerance."""
     lib, B = batch
     systems = [(0, 0.04 + 0.01 * (k % 5), synthetic.gaussian_source(LATS[0], seed=900 + k, parity="even"))
@@ -140,9 +140,9 @@ def test_batch_dslash_tuner(batch):
     _, info, res, xs = lib.batch_invert(B, systems, max_iter=4000, resid=RESID)
     assert info.status == 0, lib.last_error()
     g = lib.last_stats().batch_rhs_per_thread
-    assert g in (2, 4)
+    assert g in (1, 2, 4)
     _check_solutions(systems, res, xs)
-    other = 2 if g == 4 else 4
+    other = 2 if g != 2 else 1
     old = os.environ.get("QPHIX_B200_BATCH_G")
     os.environ["QPHIX_B200_BATCH_G"] = str(other)
     try:
