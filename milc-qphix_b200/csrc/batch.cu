@@ -291,6 +291,41 @@ __device__ __forceinline__ void bstore(double2 *f, int vh, int nrhs, int j, int 
 }
 
 // -------------------------------------------------- multi-RHS Dslash site --
+// The FP32 multi-RHS site is bound by the FP32 pipe rather than by HBM, so
+// its complex multiply-adds are written as explicit FMA chains: two FFMAs
+// per real product pair, where acc += a*b - c*d compiles to FMUL, FFMA and
+// FADD.  (The rounding order differs from mv_add by one FP32 ulp per term.)
+__device__ __forceinline__ void fmv_add(float acc[6], const float u[18], const float v[6])
+{
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float ur = u[6 * r + 2 * c], ui = u[6 * r + 2 * c + 1];
+            acc[2 * r] = __fmaf_rn(ur, v[2 * c], acc[2 * r]);
+            acc[2 * r] = __fmaf_rn(-ui, v[2 * c + 1], acc[2 * r]);
+            acc[2 * r + 1] = __fmaf_rn(ur, v[2 * c + 1], acc[2 * r + 1]);
+            acc[2 * r + 1] = __fmaf_rn(ui, v[2 * c], acc[2 * r + 1]);
+        }
+    }
+}
+
+// acc -= U^dag v
+__device__ __forceinline__ void fmv_adj_sub(float acc[6], const float u[18], const float v[6])
+{
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float ur = u[6 * c + 2 * r], ui = u[6 * c + 2 * r + 1];
+            acc[2 * r] = __fmaf_rn(-ur, v[2 * c], acc[2 * r]);
+            acc[2 * r] = __fmaf_rn(-ui, v[2 * c + 1], acc[2 * r]);
+            acc[2 * r + 1] = __fmaf_rn(-ur, v[2 * c + 1], acc[2 * r + 1]);
+            acc[2 * r + 1] = __fmaf_rn(ui, v[2 * c], acc[2 * r + 1]);
+        }
+    }
+}
+
 // acc[e] = (D in)(site j) for the G right-hand sides of group q
 template <int G>
 __device__ __forceinline__ void bsite(const BSeg &sg, int cb, int j, int q, const float2 *in, float acc[G][6])
@@ -329,8 +364,8 @@ __device__ __forceinline__ void bsite(const BSeg &sg, int cb, int j, int q, cons
         }
 #pragma unroll
         for (int e = 0; e < G; ++e) {
-            if (st & 1) mv_adj_sub(acc[e], w + 2, v[b][e]);
-            else mv_add(acc[e], w, v[b][e]);
+            if (st & 1) fmv_adj_sub(acc[e], w + 2, v[b][e]);
+            else fmv_add(acc[e], w, v[b][e]);
         }
     }
 }
