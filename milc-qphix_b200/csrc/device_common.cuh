@@ -132,15 +132,8 @@ template <> struct LinkView<double> {
 template <> struct LinkView<float> {
     const float4 *p;
     int vh;
-    __device__ __forceinline__ void load_pair(int d, int h, int j, float u[36]) const {
-        const float4 *q = p + ((size_t)d * 18 + 9 * h) * vh + j;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-            const float4 z = __ldcs(q + (size_t)c * vh);
-            u[4 * c] = z.x; u[4 * c + 1] = z.y; u[4 * c + 2] = z.z; u[4 * c + 3] = z.w;
-        }
-    }
-    // the same 9 chunks, left packed (the pipelined Dslash unpacks them later)
+    // the 9 chunks of pair h of direction d, left packed: the pipelined
+    // Dslash issues them one stage ahead and unpacks them when it uses them
     __device__ __forceinline__ void fetch_pair(int d, int h, int j, float4 c[9]) const {
         const float4 *q = p + ((size_t)d * 18 + 9 * h) * vh + j;
 #pragma unroll
@@ -175,35 +168,9 @@ template <> struct LinkView<Recon12> {
     const unsigned *sign;
     int vh;
     float scale;
-    // the fat forward/backward pair of direction d (18 complex)
-    __device__ __forceinline__ void load_fat(int d, int j, float u[36]) const {
-        const float4 *q = p + (size_t)d * kReconChunks * vh + j;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-            const float4 z = __ldcs(q + (size_t)c * vh);
-            u[4 * c] = z.x; u[4 * c + 1] = z.y; u[4 * c + 2] = z.z; u[4 * c + 3] = z.w;
-        }
-    }
-    // the Naik forward (uf) and backward (ub) links of direction d, third
-    // rows rebuilt: row2 = sign * scale * conj(row0 x row1)
-    __device__ __forceinline__ void load_naik(int d, int j, unsigned bits, float uf[18], float ub[18]) const {
-        const float4 *q = p + ((size_t)d * kReconChunks + 9) * vh + j;
-        float w[24];
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-            const float4 z = __ldcs(q + (size_t)c * vh);
-            w[4 * c] = z.x; w[4 * c + 1] = z.y; w[4 * c + 2] = z.z; w[4 * c + 3] = z.w;
-        }
-#pragma unroll
-        for (int e = 0; e < 12; ++e) {
-            uf[e] = w[e];
-            ub[e] = w[12 + e];
-        }
-        rebuild(uf, (bits >> (2 * d)) & 1u ? -scale : scale);
-        rebuild(ub, (bits >> (2 * d + 1)) & 1u ? -scale : scale);
-    }
-    // split forms of the two loads above, so a caller can issue the loads of
-    // one stage before the arithmetic of the previous one
+    // raw chunks of the fat forward/backward pair (9) and of rows 0-1 of the
+    // Naik forward and backward links (6) of direction d, left packed so the
+    // pipelined Dslash can issue them one stage ahead
     __device__ __forceinline__ void fetch_fat(int d, int j, float4 c[9]) const {
         const float4 *q = p + (size_t)d * kReconChunks * vh + j;
 #pragma unroll
@@ -214,6 +181,8 @@ template <> struct LinkView<Recon12> {
 #pragma unroll
         for (int k = 0; k < 6; ++k) c[k] = __ldcs(q + (size_t)k * vh);
     }
+    // the Naik forward (uf) and backward (ub) links of direction d from their
+    // chunks, third rows rebuilt: row2 = sign * scale * conj(row0 x row1)
     __device__ __forceinline__ void naik_from(const float4 c[6], int d, unsigned bits, float uf[18],
                                               float ub[18]) const {
 #pragma unroll

@@ -5,7 +5,8 @@ mixed-precision workload) and 32^3x64 (the multi-shift workload) the tests
 check properties that hold at any size, with the FP64 operator applied
 through QPHIX_D3_asqtad_dslash as the independent check:
   * every inner precision reaches |b - M x|^2 / |b|^2 < 1e-20, the FP64 true
-    residual recomputed here, and the solutions agree with the FP64 CG's;
+    residual recomputed here, the solutions agree with the FP64 CG's, and the
+    16-bit inner solves take at most 30% more iterations than the FP32 one;
   * D is anti-Hermitian (<y, D_eo x> = -<D_oe y, x>) and M = 4m^2 - D D is
     Hermitian and positive, in FP64, on the full 32^3x64 lattice.
 """
@@ -57,13 +58,14 @@ def test_mixed_cg_24x24x24x48_every_inner_precision(gpu):
     src = synthetic.gaussian_source(dims, seed=2002, parity="even")
     L = lib.create_L("D", links)
     b = lib.create_V("D", src, "even")
-    sols = {}
+    sols, iters = {}, {}
     try:
         for inner in ("double", "single", "half-links", "half"):
             lib.set_inner_precision(inner)
             x = lib.create_V("D", np.zeros_like(src), "even")
             it, info, res = lib.invert("D", L, x, b, mass, parity="even", max_iter=20000, nrestart=5, resid=RESID)
             assert info.status == 0, lib.last_error()
+            iters[inner] = lib.last_stats().iterations
             sols[inner] = lib.extract_V("D", x, "even")
             lib.destroy_V("D", x)
             assert _true_rsq(lib, L, sols[inner], src, mass, V) < 1.5 * RESID, inner
@@ -73,6 +75,10 @@ def test_mixed_cg_24x24x24x48_every_inner_precision(gpu):
         lib.destroy_L("D", L)
     for inner in ("single", "half-links", "half"):
         assert rel_err(sols[inner][: 3 * V], sols["double"][: 3 * V]) < 1e-7, inner
+    # 16-bit storage perturbs the operator by ~3e-5: a few more iterations
+    # than FP32 (927 against 806 here), not twice as many
+    for inner in ("half-links", "half"):
+        assert iters[inner] <= 1.3 * iters["single"], (inner, iters)
 
 
 def test_operator_identities_32x32x32x64(gpu):
