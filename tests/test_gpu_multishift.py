@@ -93,3 +93,24 @@ def test_multishift_mixed_every_shift_converges(gpu, inner):
     for m, x, r in zip(masses, xs, res):
         assert r.final_rsq < 1e-20
         assert orc.true_residual(dims, links, x, src, m, "even") < 1e-20
+
+
+@pytest.mark.parametrize("parity", ["odd", "evenodd"])
+def test_multishift_mixed_both_parities(gpu, parity):
+    """The mixed multi-shift on the odd and on both parities: each parity's
+    shifted solutions (accumulated in FP32 partial sums between reliable
+    updates and added into FP64) reach the tolerance on the FP64 residual."""
+    dims = (8, 8, 8, 8)
+    lib = gpu.use(dims)
+    links = fields(dims)
+    src = synthetic.gaussian_source(dims, seed=2002, parity="evenodd")
+    masses = _masses(0.02, 6)
+    lib.set_inner_precision("single")
+    try:
+        it, xs, res, info = _multi(lib, "D", links, src, masses, parity, max_iter=4000, nrestart=5, resid=1e-20)
+    finally:
+        lib.set_inner_precision("double")
+    parities = ["even", "odd"] if parity == "evenodd" else [parity]
+    for m, x in zip(masses, xs):
+        for p in parities:
+            assert orc.true_residual(dims, links, x, src, m, p) < 1e-20, (m, p)
