@@ -67,7 +67,8 @@ typedef struct {
   double true_rsq;        /* final |b - M x|^2 / |b|^2 (largest over masses) */
   int escalated;          /* 1 if a 16-bit inner solve stalled and continued in FP32 */
   int links_compressed;   /* 1 if the FP32 inner solve used 12-real Naik links */
-  int batch_rhs_per_thread; /* batched solves: systems per thread the FP32 Dslash tuner chose */
+  int batch_rhs_per_thread; /* batched solves: systems per thread (4, 2 or 1) the FP32 Dslash tuner chose;
+                              QPHIX_B200_BATCH_G=4|2|1 in the environment forces it */
 } QPHIX_B200_stats_t;
 
 QPHIX_status_t QPHIX_B200_get_last_stats(QPHIX_B200_stats_t *stats);
