@@ -43,16 +43,20 @@ QPHIX_B200_precision_t QPHIX_B200_get_inner_precision(void);
  * factor since the last update (default 0.2). */
 QPHIX_status_t QPHIX_B200_set_reliable_delta(double delta);
 
-/* 12-real Naik links for the FP32 inner solves of QPHIX_D3_asqtad_invert /
- * _invert_multi (0 = off, the default).  Like the reference's
- * COMPRESSED_12 storage of the long links (qphix_f3.cpp:1008-1016), the
- * third row of every Naik link is dropped and rebuilt in the Dslash, here as
- * sign * s * conj(row0 x row1) with one magnitude s for the field and a sign
- * per link, both measured from the FP64 links when the FP32 copy is made.
- * A field without that form (the Naik links are not SU(3) times one real
- * factor) keeps its 18-real links; QPHIX_B200_get_last_stats reports which
- * was used.  FP64 links and all FP64 arithmetic are unaffected.  Saves 16 %
- * of the FP32 Dslash's bytes. */
+/* Compressed Naik links for the FP32 inner solves of QPHIX_D3_asqtad_invert /
+ * _invert_multi (0 = off, the default).  Like the reference's COMPRESSED_12
+ * storage of the long links (qphix_f3.cpp:1008-1016), the third row of every
+ * Naik link is dropped and rebuilt in the Dslash, here as
+ * lambda * conj(row0 x row1), with lambda measured from the FP64 links when
+ * the FP32 copy is made:
+ *   12-real: lambda = sign * s, one magnitude s for the field and a sign per
+ *            link (Naik links SU(3) times one real factor: asqtad);
+ *   13-real: one complex lambda per link (U(3) times a real factor per link:
+ *            HISQ Naik links built from unitarised links).
+ * A field of neither form keeps its 18-real links; QPHIX_B200_get_last_stats
+ * reports which was used.  FP64 links and all FP64 arithmetic are
+ * unaffected.  Saves 16 % (12-real) or 11 % (13-real) of the FP32 Dslash's
+ * bytes. */
 QPHIX_status_t QPHIX_B200_set_link_compression(int on);
 
 /* Diagnostics of the most recent invert / invert_multi / batch_invert call. */
@@ -66,7 +70,7 @@ typedef struct {
   double mdagm_ms;        /* their summed device time */
   double true_rsq;        /* final |b - M x|^2 / |b|^2 (largest over masses) */
   int escalated;          /* 1 if a 16-bit inner solve stalled and continued in FP32 */
-  int links_compressed;   /* 1 if the FP32 inner solve used 12-real Naik links */
+  int links_compressed;   /* Naik links of the FP32 inner solve: 0 18-real, 1 12-real, 2 13-real */
   int batch_rhs_per_thread; /* batched solves: systems per thread (4, 2 or 1) the FP32 Dslash tuner chose;
                               QPHIX_B200_BATCH_G=4|2|1 in the environment forces it */
 } QPHIX_B200_stats_t;

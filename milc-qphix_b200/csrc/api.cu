@@ -341,19 +341,21 @@ struct SloppyCfg {
     const LinkSet *up;
 };
 
-// FP32 links with 12-real Naik links when compression is on and the field
-// has the form it needs; otherwise the 18-real FP32 copy
+// FP32 links with 12-real or 13-real Naik links when compression is on and
+// the field has a form they need; otherwise the 18-real FP32 copy
 const LinkSet &single_inner_links(QPHIX_D3_FermionLinksAsqtad *H)
 {
     Context &c = ctx();
     if (!c.link_compression) return single_links(H);
     if (!H->recon_checked) {
-        double dev[4];
+        double dev[5];
         H->recon_checked = 1;
-        if (!links_compress12(H->sloppy_recon, H->links, c.launch(), dev) && c.verbose)
+        const int mode = links_compress(H->sloppy_recon, H->links, c.launch(), dev);
+        if (c.verbose)
             std::fprintf(stderr,
-                         "qphix_b200: Naik links keep 18 reals (|ratio| %.6e spread %.2e imag %.2e residual %.2e)\n",
-                         dev[0], dev[1], dev[2], dev[3]);
+                         "qphix_b200: Naik links %s (|ratio| %.6e spread %.2e imag %.2e residual %.2e / %.2e)\n",
+                         mode == 1 ? "12-real" : mode == 2 ? "13-real" : "keep 18 reals", dev[0], dev[1], dev[2],
+                         dev[3], dev[4]);
     }
     return H->sloppy_recon.valid ? H->sloppy_recon : single_links(H);
 }
@@ -390,7 +392,7 @@ int asqtad_invert(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_invert_ar
             } else {
                 const SloppyCfg s = sloppy_cfg(H, c.inner_mode);
                 iters = cg_mixed(s.vec, H->links, *s.links, s.up, a);
-                c.stats.links_compressed = s.links->recon ? 1 : 0;
+                c.stats.links_compressed = s.links->recon;
             }
         } else {
             iters = cg_reference(Prec::Single, H->links, a);
@@ -443,7 +445,7 @@ int asqtad_invert_multi(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_inv
             } else {
                 const SloppyCfg s = sloppy_cfg(H, c.inner_mode);
                 iters = multishift_mixed(s.vec, H->links, *s.links, s.up, a);
-                c.stats.links_compressed = s.links->recon ? 1 : 0;
+                c.stats.links_compressed = s.links->recon;
             }
         } else {
             iters = multishift_reference(Prec::Single, H->links, a);

@@ -81,11 +81,13 @@ void free_links(LinkSet &ls)
     for (int cb = 0; cb < 2; ++cb) {
         dev_free(ls.blk[cb]);
         dev_free(ls.sign[cb]);
+        dev_free(ls.lam[cb]);
         ls.blk[cb] = nullptr;
         ls.sign[cb] = nullptr;
+        ls.lam[cb] = nullptr;
     }
     ls.valid = false;
-    ls.recon = false;
+    ls.recon = 0;
 }
 
 void upload_state()

@@ -162,12 +162,11 @@ template <> struct LinkView<__half> {
     }
 };
 
-// FP32 fat links and 12-real Naik links (layout: internal.h, LinkSet::recon)
-template <> struct LinkView<Recon12> {
+// FP32 fat links and Naik links without their third rows (layout: internal.h,
+// LinkSet::recon): the loads shared by the 12-real and 13-real forms
+struct ReconLinks {
     const float4 *p;
-    const unsigned *sign;
     int vh;
-    float scale;
     // raw chunks of the fat forward/backward pair (9) and of rows 0-1 of the
     // Naik forward and backward links (6) of direction d, left packed so the
     // pipelined Dslash can issue them one stage ahead
@@ -181,30 +180,73 @@ template <> struct LinkView<Recon12> {
 #pragma unroll
         for (int k = 0; k < 6; ++k) c[k] = __ldcs(q + (size_t)k * vh);
     }
-    // the Naik forward (uf) and backward (ub) links of direction d from their
-    // chunks, third rows rebuilt: row2 = sign * scale * conj(row0 x row1)
-    __device__ __forceinline__ void naik_from(const float4 c[6], int d, unsigned bits, float uf[18],
-                                              float ub[18]) const {
+    // rows 0-1 of the forward (uf) and backward (ub) Naik links
+    __device__ __forceinline__ static void unpack_naik(const float4 c[6], float uf[18], float ub[18]) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             uf[4 * k] = c[k].x; uf[4 * k + 1] = c[k].y; uf[4 * k + 2] = c[k].z; uf[4 * k + 3] = c[k].w;
             ub[4 * k] = c[3 + k].x; ub[4 * k + 1] = c[3 + k].y; ub[4 * k + 2] = c[3 + k].z; ub[4 * k + 3] = c[3 + k].w;
         }
-        rebuild(uf, (bits >> (2 * d)) & 1u ? -scale : scale);
-        rebuild(ub, (bits >> (2 * d + 1)) & 1u ? -scale : scale);
     }
+    // (cr, ci)_k = (row0 x row1)_k: (a x b)_k = a_{k+1} b_{k+2} - a_{k+2} b_{k+1}
+    __device__ __forceinline__ static void cross01(const float u[18], int k, float &cr, float &ci) {
+        const int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+        const float ar1 = u[2 * k1], ai1 = u[2 * k1 + 1], ar2 = u[2 * k2], ai2 = u[2 * k2 + 1];
+        const float br1 = u[6 + 2 * k1], bi1 = u[6 + 2 * k1 + 1], br2 = u[6 + 2 * k2], bi2 = u[6 + 2 * k2 + 1];
+        cr = (ar1 * br2 - ai1 * bi2) - (ar2 * br1 - ai2 * bi1);
+        ci = (ar1 * bi2 + ai1 * br2) - (ar2 * bi1 + ai2 * br1);
+    }
+    // row 2 = f * conj(row0 x row1), f real
     __device__ __forceinline__ static void rebuild(float u[18], float f) {
-        // a = row 0, b = row 1: (a x b)_k = a_{k+1} b_{k+2} - a_{k+2} b_{k+1}
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
-            const float ar1 = u[2 * k1], ai1 = u[2 * k1 + 1], ar2 = u[2 * k2], ai2 = u[2 * k2 + 1];
-            const float br1 = u[6 + 2 * k1], bi1 = u[6 + 2 * k1 + 1], br2 = u[6 + 2 * k2], bi2 = u[6 + 2 * k2 + 1];
-            const float cr = (ar1 * br2 - ai1 * bi2) - (ar2 * br1 - ai2 * bi1);
-            const float ci = (ar1 * bi2 + ai1 * br2) - (ar2 * bi1 + ai2 * br1);
+            float cr, ci;
+            cross01(u, k, cr, ci);
             u[12 + 2 * k] = f * cr;
             u[12 + 2 * k + 1] = -f * ci;  // conjugate
         }
+    }
+    // row 2 = (lr + i li) * conj(row0 x row1)
+    __device__ __forceinline__ static void rebuild(float u[18], float lr, float li) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float cr, ci;
+            cross01(u, k, cr, ci);
+            u[12 + 2 * k] = lr * cr + li * ci;
+            u[12 + 2 * k + 1] = li * cr - lr * ci;
+        }
+    }
+};
+
+// 12-real: lambda = sign * scale, one magnitude for the field
+template <> struct LinkView<Recon12> : ReconLinks {
+    const unsigned *sign;
+    float scale;
+    static constexpr bool has_lam = false;
+    __device__ __forceinline__ unsigned fetch_aux(int j) const { return __ldg(sign + j); }
+    __device__ __forceinline__ float4 fetch_lam(int, int) const { return make_float4(0.f, 0.f, 0.f, 0.f); }
+    // the Naik forward (uf) and backward (ub) links of direction d from their
+    // chunks, third rows rebuilt
+    __device__ __forceinline__ void naik_from(const float4 c[6], int d, unsigned bits, float4, float uf[18],
+                                              float ub[18]) const {
+        unpack_naik(c, uf, ub);
+        rebuild(uf, (bits >> (2 * d)) & 1u ? -scale : scale);
+        rebuild(ub, (bits >> (2 * d + 1)) & 1u ? -scale : scale);
+    }
+};
+
+// 13-real: a complex lambda per link, (forward, backward) of direction d in
+// one float4
+template <> struct LinkView<Recon13> : ReconLinks {
+    const float4 *lam;
+    static constexpr bool has_lam = true;
+    __device__ __forceinline__ unsigned fetch_aux(int) const { return 0u; }
+    __device__ __forceinline__ float4 fetch_lam(int d, int j) const { return __ldcs(lam + (size_t)d * vh + j); }
+    __device__ __forceinline__ void naik_from(const float4 c[6], int, unsigned, float4 l, float uf[18],
+                                              float ub[18]) const {
+        unpack_naik(c, uf, ub);
+        rebuild(uf, l.x, l.y);
+        rebuild(ub, l.z, l.w);
     }
 };
 

@@ -55,25 +55,32 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
                 else mv_add(acc, u, v);
             }
         }
-    } else if constexpr (std::is_same<SL, float>::value || std::is_same<SL, Recon12>::value) {
+    } else if constexpr (std::is_same<SL, float>::value || std::is_same<SL, Recon12>::value ||
+                         std::is_same<SL, Recon13>::value) {
         // FP32: eight stages, the forward/backward pair of fat (h = 0) and of
         // Naik (h = 1) links of each direction: 9 x 16 bytes, or 6 x 16 bytes
-        // for 12-real Naik links whose third rows are rebuilt from the site's
-        // sign bits.  Software-pipelined: the loads of stage i + 1 are issued
-        // before the arithmetic of stage i, so every thread keeps one stage of
-        // links and neighbours in flight.
-        constexpr bool R12 = std::is_same<SL, Recon12>::value;
+        // for compressed Naik links whose third rows are rebuilt from the
+        // site's sign bits (12-real) or the links' complex ratios (13-real,
+        // one more 16-byte load per direction).  Software-pipelined: the loads
+        // of stage i + 1 are issued before the arithmetic of stage i, so every
+        // thread keeps one stage of links and neighbours in flight.
+        constexpr bool RN = !std::is_same<SL, float>::value;
         unsigned bits = 0;
-        if constexpr (R12) bits = __ldg(a.links.sign + j);
+        if constexpr (RN) bits = a.links.fetch_aux(j);
         float4 c[2][9];
+        float4 lam[2];
         A v[2][2][6];
         auto issue = [&](int st, int b) {
             const int d = st >> 1, h = st & 1;
             a.in.load(neighbor(a.g, s, 8 * h + 2 * d + 1), v[b][0]);
             a.in.load(neighbor(a.g, s, 8 * h + 2 * d), v[b][1]);
-            if constexpr (R12) {
-                if (h) a.links.fetch_naik(d, j, c[b]);
-                else a.links.fetch_fat(d, j, c[b]);
+            if constexpr (RN) {
+                if (h) {
+                    a.links.fetch_naik(d, j, c[b]);
+                    if constexpr (LinkView<SL>::has_lam) lam[b] = a.links.fetch_lam(d, j);
+                } else {
+                    a.links.fetch_fat(d, j, c[b]);
+                }
             } else {
                 a.links.fetch_pair(d, h, j, c[b]);
             }
@@ -84,8 +91,8 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
             const int b = st & 1;
             if (st + 1 < 8) issue(st + 1, b ^ 1);
             A u[36];
-            if (R12 && (st & 1)) {
-                if constexpr (R12) a.links.naik_from(c[b], st >> 1, bits, u, u + 18);
+            if (RN && (st & 1)) {
+                if constexpr (RN) a.links.naik_from(c[b], st >> 1, bits, lam[b], u, u + 18);
             } else {
 #pragma unroll
                 for (int k = 0; k < 9; ++k) {
@@ -132,6 +139,7 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
 template <typename SV, typename SL> struct MinBlocks { static constexpr int value = 1; };
 template <> struct MinBlocks<float, float> { static constexpr int value = 3; };
 template <> struct MinBlocks<float, Recon12> { static constexpr int value = 3; };
+template <> struct MinBlocks<float, Recon13> { static constexpr int value = 3; };
 template <> struct MinBlocks<float, __half> { static constexpr int value = 3; };
 template <> struct MinBlocks<__half, __half> { static constexpr int value = 4; };
 
@@ -396,8 +404,11 @@ static DslashArgs<SV, SL> make_args(const Launch &L, VecBlock out, VecBlock in, 
     } else if constexpr (std::is_same<SL, float>::value) {
         a.links = LinkView<float>{static_cast<const float4 *>(ls.blk[cb]), L.g->vh};
     } else if constexpr (std::is_same<SL, Recon12>::value) {
-        a.links = LinkView<Recon12>{static_cast<const float4 *>(ls.blk[cb]), static_cast<const unsigned *>(ls.sign[cb]),
-                                    L.g->vh, ls.recon_scale};
+        a.links = LinkView<Recon12>{{static_cast<const float4 *>(ls.blk[cb]), L.g->vh},
+                                    static_cast<const unsigned *>(ls.sign[cb]), ls.recon_scale};
+    } else if constexpr (std::is_same<SL, Recon13>::value) {
+        a.links = LinkView<Recon13>{{static_cast<const float4 *>(ls.blk[cb]), L.g->vh},
+                                    static_cast<const float4 *>(ls.lam[cb])};
     } else {
         a.links = LinkView<double>{static_cast<const double2 *>(ls.blk[cb]), L.g->vh};
     }
@@ -472,18 +483,19 @@ struct TuneEntry {
     int variant = 0;
     float us[kVariants] = {0, 0, 0};
 };
-static TuneEntry g_tune[3][4];  // per (vector precision, link storage: Prec or 3 = 12-real Naik)
+// per (vector precision, link storage: Prec, or 3 / 4 = 12-real / 13-real Naik)
+static TuneEntry g_tune[3][5];
 
 template <typename SL>
 static int link_slot(Prec pl)
 {
-    return std::is_same<SL, Recon12>::value ? 3 : (int)pl;
+    return std::is_same<SL, Recon12>::value ? 3 : std::is_same<SL, Recon13>::value ? 4 : (int)pl;
 }
 
-// the TMA pipeline stages 18-real FP32 pairs; 12-real Naik links run the
+// the TMA pipeline stages 18-real FP32 pairs; compressed Naik links run the
 // register variants only
 template <typename SL>
-constexpr bool has_tma() { return !std::is_same<SL, Recon12>::value; }
+constexpr bool has_tma() { return !std::is_same<SL, Recon12>::value && !std::is_same<SL, Recon13>::value; }
 
 template <typename SV, typename SL>
 static void launch_variant(int variant, const DslashArgs<SV, SL> &a, const LinkSet &ls, int cb, const Launch &L,
@@ -558,8 +570,9 @@ static void launch_dslash(const Launch &L, VecBlock out, VecBlock in, const Link
     do {                                                                                        \
         const Prec pl_ = (ls_).prec;                                                            \
         if ((ls_).recon) {                                                                      \
-            if ((pv) != Prec::Single) throw std::runtime_error("Dslash: 12-real links need FP32 vectors"); \
-            F<float, Recon12>(__VA_ARGS__);                                                     \
+            if ((pv) != Prec::Single) throw std::runtime_error("Dslash: compressed links need FP32 vectors"); \
+            if ((ls_).recon == 2) F<float, Recon13>(__VA_ARGS__);                               \
+            else F<float, Recon12>(__VA_ARGS__);                                                \
         } else if ((pv) == Prec::Double && pl_ == Prec::Double) F<double, double>(__VA_ARGS__); \
         else if ((pv) == Prec::Single && pl_ == Prec::Single) F<float, float>(__VA_ARGS__);     \
         else if ((pv) == Prec::Half && pl_ == Prec::Half) F<__half, __half>(__VA_ARGS__);      \
@@ -609,7 +622,7 @@ static void launch_mdagm_variant(int variant, const DslashArgs<SV, SL> &a, const
 
 // The fused M^dag M kernel (K2) is tuned on its own: its grid-wide reduction
 // favours fewer, longer-lived blocks more than the plain Dslash does.
-static TuneEntry g_tune_mdagm[3][4];
+static TuneEntry g_tune_mdagm[3][5];
 
 template <typename SV, typename SL>
 static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV, SL> &a, const LinkSet &ls,

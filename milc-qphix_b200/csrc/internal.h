@@ -74,17 +74,24 @@ struct LinkSet {
     float link_max[2] = {0.f, 0.f};     // half only: fixed-point range of fat / Naik links
     Prec prec = Prec::Double;           // storage precision of the blocks
     bool valid = false;
-    // FP32 with 12-real Naik links (recon = true): per direction the fat
-    // pair (9 float4) and rows 0-1 of the Naik pair (6 float4); row 2 is
-    // rebuilt as sign * recon_scale * conj(row0 x row1), the sign bits per
-    // site in sign[cb] (bit 2d: forward, 2d+1: backward Naik link of d)
-    bool recon = false;
+    // FP32 with compressed Naik links (recon 1: 12-real, 2: 13-real): per
+    // direction the fat pair (9 float4) and rows 0-1 of the Naik pair (6
+    // float4); row 2 is rebuilt as lambda * conj(row0 x row1) with
+    //   recon 1: lambda = sign * recon_scale, one real magnitude for the
+    //            field, the sign bits per site in sign[cb] (bit 2d: forward,
+    //            2d+1: backward Naik link of d) -- SU(3) times a real factor;
+    //   recon 2: lambda complex per link, lam[cb][d*Vh + j] = float4(lambda
+    //            forward, lambda backward) -- U(3) times a real factor, the
+    //            form of HISQ Naik links built from unitarised links.
+    int recon = 0;
     float recon_scale = 0.f;
-    void *sign[2] = {nullptr, nullptr};  // unsigned[Vh] per parity
+    void *sign[2] = {nullptr, nullptr};  // unsigned[Vh] per parity (recon 1)
+    void *lam[2] = {nullptr, nullptr};   // float4[4*Vh] per parity (recon 2)
 };
 
-// storage tag of FP32 links with 12-real Naik links (LinkSet::recon)
+// storage tags of FP32 links with 12-real / 13-real Naik links (LinkSet::recon)
 struct Recon12 {};
+struct Recon13 {};
 constexpr int kReconChunks = 15;  // float4 chunks per direction and site
 
 // ----------------------------------------------------------------------------
@@ -232,13 +239,15 @@ void links_to_raw(Prec p, void *raw_dev, bool raw_double, const LinkSet &ls, int
                   const Launch &L);
 // convert a link set between precisions (FP64 -> FP32 / half)
 void links_convert(Prec dst_p, LinkSet &dst, Prec src_p, const LinkSet &src, const Launch &L);
-// FP32 copy of an FP64 link set with 12-real Naik links (recon.cu).  Checks
-// that every Naik link's third row is sign * s * conj(row0 x row1) with one
-// magnitude s for all links; if so fills dst (allocated here) and returns
-// true, else leaves dst empty and returns false.  dev[0..3] receive the
-// check's statistics (mean |ratio|, relative spread of |ratio|, relative
-// imaginary part, relative residual of the rebuilt rows).
-bool links_compress12(LinkSet &dst, const LinkSet &src64, const Launch &L, double dev[4]);
+// FP32 copy of an FP64 link set with compressed Naik links (recon.cu).
+// Checks every Naik link's third row against lambda * conj(row0 x row1):
+// 12-real when lambda = sign * s with one magnitude s for all links, else
+// 13-real when each link has its own complex lambda; fills dst (allocated
+// here) and returns its recon mode (1 or 2), or leaves dst empty and returns
+// 0 when neither holds.  dev[0..4] receive the check's statistics (mean
+// |ratio|, relative spread of |ratio|, relative imaginary part, relative
+// residual of the rows rebuilt with a real ratio, and with a complex one).
+int links_compress(LinkSet &dst, const LinkSet &src64, const Launch &L, double dev[5]);
 // fills ls_half.link_max[] from the ranges of `src` (fat and Naik slots)
 void links_absmax(Prec p, const LinkSet &src, LinkSet &ls_half, const Launch &L, double *scratch);
 

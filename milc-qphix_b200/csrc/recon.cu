@@ -1,19 +1,23 @@
-// FP32 link sets with 12-real Naik links.
+// FP32 link sets with 12-real and 13-real Naik links.
 //
 // The reference can store the long (Naik) links without their third row
 // (COMPRESSED_12 in asqtad_create_L_from_raw, qphix_f3.cpp:1008-1016) and
 // rebuild it as conj(row0 x row1) with the staggered-phase sign
 // (reconstruct_gauge_third_row, qphix_f3.cpp:1072-1084).  MILC's Naik links
-// carry the Naik coefficient and the phases, so here the rebuilt row is
-// sign * s * conj(row0 x row1) with one magnitude s for the whole field and a
-// sign bit per link, both measured from the FP64 links: an SU(3) matrix times
-// a real factor c satisfies row2 = conj(row0 x row1) / c.  A field that does
-// not have that form (U(3) links with arbitrary phases, a varying factor) is
+// carry the Naik coefficient and the phases: a link c * U with U in U(3) and
+// c real satisfies row2 = lambda * conj(row0 x row1) with lambda = det(U)/c.
+// Two forms are kept here, both measured from the FP64 links:
+//   12-real: U in SU(3) up to a sign (asqtad Naik links): lambda = sign * s
+//            with one magnitude s for the field and a sign bit per link;
+//   13-real: any U in U(3) (HISQ Naik links built from unitarised links):
+//            lambda complex per link, stored as FP32.
+// A field of neither form (a varying real factor, non-unitary links) is
 // detected and keeps its 18-real links.  Only the FP32 copy used by the
 // mixed-precision inner solve is compressed; FP64 links stay complete.
 //
-// Bytes per output site of the FP32 Dslash: 8 fat x 72 + 8 Naik x 48 + 4
-// (sign word) + 48 (vectors) = 1012 instead of 1200.
+// Bytes per output site of the FP32 Dslash: 8 fat x 72 + 8 Naik x 48 + 48
+// (vectors) + 4 (12-real sign word) = 1012 or + 64 (13-real ratios) = 1072,
+// instead of 1200.
 #include "context.h"
 #include "device_common.cuh"
 
@@ -21,7 +25,7 @@ namespace qb {
 
 namespace {
 
-constexpr int kProbeNV = 4;
+constexpr int kProbeNV = 5;
 
 __device__ __forceinline__ void load_link64(const double2 *blk, int d, int slot, int j, int vh, double2 u[9])
 {
@@ -57,12 +61,13 @@ __device__ __forceinline__ double2 ratio(const double2 u[9], const double2 c[3],
     return n2 > 0 ? make_double2(nr / n2, ni / n2) : make_double2(0.0, 0.0);
 }
 
-// pass 0: sums of |rho|, (Im rho)^2, |row2 - Re(rho) c|^2, |row2|^2
+// pass 0: sums of |rho|, (Im rho)^2, |row2 - Re(rho) c|^2, |row2|^2,
+//         |row2 - rho c|^2
 // pass 1: sum of (|rho| - mean)^2
 __global__ void __launch_bounds__(kBlock) k_recon_probe(const double2 *blk, int vh, int pass, double mean,
                                                         double *partials)
 {
-    double s[kProbeNV] = {0, 0, 0, 0};
+    double s[kProbeNV] = {0, 0, 0, 0, 0};
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < vh * 8; t += gridDim.x * blockDim.x) {
         const int j = t >> 3, d = (t >> 1) & 3, slot = 2 + (t & 1);
         double2 u[9], c[3];
@@ -79,6 +84,9 @@ __global__ void __launch_bounds__(kBlock) k_recon_probe(const double2 *blk, int 
                 const double dr = u[6 + k].x - rho.x * c[k].x, di = u[6 + k].y - rho.x * c[k].y;
                 s[2] += dr * dr + di * di;
                 s[3] += u[6 + k].x * u[6 + k].x + u[6 + k].y * u[6 + k].y;
+                const double er = u[6 + k].x - (rho.x * c[k].x - rho.y * c[k].y);
+                const double ei = u[6 + k].y - (rho.x * c[k].y + rho.y * c[k].x);
+                s[4] += er * er + ei * ei;
             }
         } else {
             s[0] += (mag - mean) * (mag - mean);
@@ -109,9 +117,13 @@ __global__ void k_sum_partials(const double *partials, int nb, double *out)
 }
 
 // FP32 blocks: per direction the fat pair (complex 0..17 -> 9 float4) and
-// rows 0-1 of the Naik forward and backward links (12 complex -> 6 float4);
-// sign bit 2d (forward) / 2d+1 (backward) when Re(rho) < 0
-__global__ void __launch_bounds__(kBlock) k_recon_pack(float4 *dst, unsigned *sign, const double2 *blk, int vh)
+// rows 0-1 of the Naik forward and backward links (12 complex -> 6 float4).
+// MODE 1: sign bit 2d (forward) / 2d+1 (backward) when Re(rho) < 0;
+// MODE 2: rho of the forward and backward Naik links of direction d as one
+// float4 in lam[d*vh + j]
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_recon_pack(float4 *dst, unsigned *sign, float4 *lam, const double2 *blk,
+                                                       int vh)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= vh) return;
@@ -125,13 +137,15 @@ __global__ void __launch_bounds__(kBlock) k_recon_pack(float4 *dst, unsigned *si
             const double2 b = blk[link_cx_index(1, d, 2 * c + 1, j, vh)];
             q[(size_t)c * vh] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
         }
+        double2 rh[2];
 #pragma unroll
         for (int slot = 2; slot < 4; ++slot) {
             double2 u[9], c3[3];
             load_link64(blk, d, slot, j, vh, u);
             conj_cross(u, c3);
             double c2;
-            if (ratio(u, c3, &c2).x < 0) bits |= 1u << (2 * d + (slot - 2));
+            rh[slot - 2] = ratio(u, c3, &c2);
+            if (MODE == 1 && rh[slot - 2].x < 0) bits |= 1u << (2 * d + (slot - 2));
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 // rows 0-1 (6 complex) of this link: chunks 9 + 3*(slot-2) + c
@@ -139,24 +153,25 @@ __global__ void __launch_bounds__(kBlock) k_recon_pack(float4 *dst, unsigned *si
                     make_float4((float)u[2 * c].x, (float)u[2 * c].y, (float)u[2 * c + 1].x, (float)u[2 * c + 1].y);
             }
         }
+        if (MODE == 2)
+            lam[(size_t)d * vh + j] = make_float4((float)rh[0].x, (float)rh[0].y, (float)rh[1].x, (float)rh[1].y);
     }
-    sign[j] = bits;
+    if (MODE == 1) sign[j] = bits;
 }
 
 }  // namespace
 
-bool links_compress12(LinkSet &dst, const LinkSet &src64, const Launch &L, double dev[4])
+int links_compress(LinkSet &dst, const LinkSet &src64, const Launch &L, double dev[5])
 {
-    Context &c = ctx();
     const int vh = L.g->vh;
-    if (src64.prec != Prec::Double || !src64.valid) throw Error("links_compress12: needs FP64 links");
+    if (src64.prec != Prec::Double || !src64.valid) throw Error("links_compress: needs FP64 links");
     const int nb = 296;
     double *part = static_cast<double *>(dev_alloc(sizeof(double) * (kProbeNV * nb + kProbeNV)));
     double *sums = part + kProbeNV * nb;
-    double h[kProbeNV], tot[kProbeNV] = {0, 0, 0, 0};
+    double h[kProbeNV], tot[kProbeNV] = {0, 0, 0, 0, 0};
     double mean = 0, spread = 0;
     for (int pass = 0; pass < 2; ++pass) {
-        double acc[kProbeNV] = {0, 0, 0, 0};
+        double acc[kProbeNV] = {0, 0, 0, 0, 0};
         for (int cb = 0; cb < 2; ++cb) {
             k_recon_probe<<<nb, kBlock, 0, L.stream>>>(static_cast<const double2 *>(src64.blk[cb]), vh, pass, mean,
                                                       part);
@@ -179,23 +194,33 @@ bool links_compress12(LinkSet &dst, const LinkSet &src64, const Launch &L, doubl
     dev[1] = spread;
     dev[2] = mean > 0 ? std::sqrt(tot[1] / n) / mean : 1.0;
     dev[3] = tot[3] > 0 ? std::sqrt(tot[2] / tot[3]) : 1.0;
+    dev[4] = tot[3] > 0 ? std::sqrt(tot[4] / tot[3]) : 1.0;
     // the rebuilt rows must be exact far below FP32 rounding
-    if (!(mean > 0) || !(spread < 1e-9) || !(dev[2] < 1e-9) || !(dev[3] < 1e-9)) return false;
+    int mode = 0;
+    if (mean > 0 && spread < 1e-9 && dev[2] < 1e-9 && dev[3] < 1e-9) mode = 1;
+    else if (mean > 0 && dev[4] < 1e-9) mode = 2;
+    if (!mode) return 0;
     dst = LinkSet{};
     for (int cb = 0; cb < 2; ++cb) {
         dst.blk[cb] = dev_alloc(sizeof(float4) * kReconChunks * 4 * (size_t)vh);
-        dst.sign[cb] = dev_alloc(sizeof(unsigned) * (size_t)vh);
-        k_recon_pack<<<grid_for(vh), kBlock, 0, L.stream>>>(static_cast<float4 *>(dst.blk[cb]),
-                                                            static_cast<unsigned *>(dst.sign[cb]),
-                                                            static_cast<const double2 *>(src64.blk[cb]), vh);
+        const double2 *src = static_cast<const double2 *>(src64.blk[cb]);
+        if (mode == 1) {
+            dst.sign[cb] = dev_alloc(sizeof(unsigned) * (size_t)vh);
+            k_recon_pack<1><<<grid_for(vh), kBlock, 0, L.stream>>>(
+                static_cast<float4 *>(dst.blk[cb]), static_cast<unsigned *>(dst.sign[cb]), nullptr, src, vh);
+        } else {
+            dst.lam[cb] = dev_alloc(sizeof(float4) * 4 * (size_t)vh);
+            k_recon_pack<2><<<grid_for(vh), kBlock, 0, L.stream>>>(static_cast<float4 *>(dst.blk[cb]), nullptr,
+                                                                   static_cast<float4 *>(dst.lam[cb]), src, vh);
+        }
     }
     QB_CUDA(cudaGetLastError());
     sync_check();
     dst.prec = Prec::Single;
-    dst.recon = true;
+    dst.recon = mode;
     dst.recon_scale = (float)mean;
     dst.valid = true;
-    return true;
+    return mode;
 }
 
 }  // namespace qb

@@ -95,22 +95,38 @@ def test_multishift_mixed_every_shift_converges(gpu, inner):
         assert orc.true_residual(dims, links, x, src, m, "even") < 1e-20
 
 
-@pytest.mark.parametrize("parity", ["odd", "evenodd"])
-def test_multishift_mixed_both_parities(gpu, parity):
+def _crossed(v, V):
+    """The reference's multi-shift with EVENODD solves the even half with the
+    odd-checkerboard operator and then the odd half with the even one
+    (parity = parity0 & 1 = 1 first, ks_multicg_offset.cpp:294, then
+    :533-537).  Moving each half to the other parity turns that into the
+    ordinary system the oracle checks."""
+    h = 3 * V
+    return np.concatenate([v[h:], v[:h]])
+
+
+@pytest.mark.parametrize("parity,inner", [("odd", "single"), ("evenodd", "single"), ("evenodd", "double")])
+def test_multishift_mixed_both_parities(gpu, parity, inner):
     """The mixed multi-shift on the odd and on both parities: each parity's
     shifted solutions (accumulated in FP32 partial sums between reliable
-    updates and added into FP64) reach the tolerance on the FP64 residual."""
+    updates and added into FP64) reach the tolerance on the FP64 residual of
+    the system the reference solves there (the FP64 path, which follows the
+    reference statement for statement, checks that reading of EVENODD)."""
     dims = (8, 8, 8, 8)
+    V = int(np.prod(dims))
     lib = gpu.use(dims)
     links = fields(dims)
     src = synthetic.gaussian_source(dims, seed=2002, parity="evenodd")
     masses = _masses(0.02, 6)
-    lib.set_inner_precision("single")
+    lib.set_inner_precision(inner)
     try:
         it, xs, res, info = _multi(lib, "D", links, src, masses, parity, max_iter=4000, nrestart=5, resid=1e-20)
     finally:
         lib.set_inner_precision("double")
-    parities = ["even", "odd"] if parity == "evenodd" else [parity]
     for m, x in zip(masses, xs):
-        for p in parities:
-            assert orc.true_residual(dims, links, x, src, m, p) < 1e-20, (m, p)
+        if parity == "odd":
+            assert orc.true_residual(dims, links, x, src, m, "odd") < 1e-20, m
+        else:
+            xc, bc = _crossed(x, V), _crossed(src, V)
+            for p in ("even", "odd"):
+                assert orc.true_residual(dims, links, xc, bc, m, p) < 1e-20, (m, p)

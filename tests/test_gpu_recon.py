@@ -1,10 +1,13 @@
-"""GPU: FP32 inner solves with 12-real Naik links (QPHIX_B200_set_link_compression).
+"""GPU: FP32 inner solves with 12-real and 13-real Naik links
+(QPHIX_B200_set_link_compression).
 
 The rebuilt third rows make the FP32 operator equal to the 18-real one up to
 FP32 rounding, so a mixed-precision solve with compression must take the same
 number of inner iterations to within a few and reach the same FP64 true
-residual (checked by the oracle).  A Naik field that is not SU(3) times one
-real factor must be detected and solved with 18-real links.
+residual (checked by the oracle).  SU(3) Naik links times one real factor
+are 12-real; U(3) links times a real factor per link are 13-real; a Naik
+field with a non-unitary part must be detected and solved with 18-real
+links.
 """
 import numpy as np
 import pytest
@@ -71,16 +74,48 @@ def test_compressed_multishift(gpu):
         assert orc.true_residual(DIMS, links, x, src, m, "even") < 1.5 * RESID
 
 
-def test_non_su3_naik_links_keep_18_reals(gpu):
-    """Naik links scaled by a site-dependent factor have no single magnitude:
-    the check refuses them and the solve runs with 18-real links."""
+def _naik_variant(links, how, seed=5):
+    """Naik links of `links` changed per link: 'phase' multiplies each by a
+    random U(1) phase (U(3) times the Naik factor, the HISQ form), 'scale' by
+    a random real factor per site, 'noise' adds a small non-unitary part."""
+    dims = DIMS
+    V = int(np.prod(dims))
+    rng = np.random.default_rng(seed)
+    lng = links["lng"].reshape(V, 4, 9, 2)
+    z = lng[..., 0] + 1j * lng[..., 1]
+    if how == "phase":
+        z = z * np.exp(1j * rng.uniform(-np.pi, np.pi, (V, 4)))[:, :, None]
+    elif how == "scale":
+        z = z * (1.0 + 0.1 * rng.random(V))[:, None, None]
+    else:
+        z = z + 1e-3 * np.abs(z).max() * (rng.standard_normal(z.shape) + 1j * rng.standard_normal(z.shape))
+    out = dict(links)
+    out["lng"] = np.stack([z.real, z.imag], axis=-1).reshape(-1)
+    out["lngback"] = synthetic.backlinks_raw(dims, out["lng"], 3)
+    return out
+
+
+@pytest.mark.parametrize("how", ["phase", "scale"])
+def test_u3_naik_links_13_real(gpu, how):
+    """Naik links that are U(3) times a real factor per link (a random phase
+    per link, or a factor that varies by site) are not 12-real but are
+    13-real: one complex ratio per link rebuilds the third row exactly.  The
+    compressed FP32 solve matches the 18-real one."""
     lib = gpu.use(DIMS)
-    links = dict(fields(DIMS, seed=21))
-    V = int(np.prod(DIMS))
-    scale = 1.0 + 0.1 * np.random.default_rng(5).random(V)
-    lng = (links["lng"].reshape(V, 72) * scale[:, None]).reshape(-1)
-    links["lng"] = lng
-    links["lngback"] = synthetic.backlinks_raw(DIMS, lng, 3)
+    links = _naik_variant(fields(DIMS, seed=21), how)
+    src = synthetic.gaussian_source(DIMS, seed=2002, parity="even")
+    st0, (x0,) = _solve(lib, links, src, 0.03, False)
+    st1, (x1,) = _solve(lib, links, src, 0.03, True)
+    assert st0.links_compressed == 0 and st1.links_compressed == 2
+    assert abs(st1.iterations - st0.iterations) <= max(20, st0.iterations // 20)
+    assert orc.true_residual(DIMS, links, x1, src, 0.03, "even") < 1.5 * RESID
+
+
+def test_non_unitary_naik_links_keep_18_reals(gpu):
+    """Naik links with a non-unitary part have no ratio that rebuilds their
+    third row: the check refuses them and the solve runs with 18-real links."""
+    lib = gpu.use(DIMS)
+    links = _naik_variant(fields(DIMS, seed=21), "noise")
     src = synthetic.gaussian_source(DIMS, seed=2002, parity="even")
     st, (x,) = _solve(lib, links, src, 0.03, True)
     assert st.links_compressed == 0
