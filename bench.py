@@ -922,7 +922,7 @@ def main():
                          "mixed_cg_half-links, fp64_multishift, mixed_multishift_single, "
                          "mixed_multishift_half-links")
     ap.add_argument("--reps", type=int, default=1)
-    ap.add_argument("--inner", default="single", choices=["single", "half", "double"])
+    ap.add_argument("--inner", default="single", choices=["single", "half", "half-links", "double"])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)

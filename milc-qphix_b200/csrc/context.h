@@ -82,7 +82,7 @@ struct Context {
     cudaEvent_t ev_user[2] = {nullptr, nullptr};
     // settings (qphix_b200.h)
     int inner_mode = QPHIX_B200_PREC_DOUBLE;  // QPHIX_B200_precision_t of D3 solves
-    int link_compression = 0;                 // FP32 inner solves with 12-real Naik links
+    int link_compression = 0;                 // FP32 inner solves with 12-/13-real Naik links
     double reliable_delta = 0.2;
     int kernel_timing = 0;
     int max_chunk = 64;
@@ -146,8 +146,8 @@ struct QPHIX_D3_FermionLinksAsqtad_struct {
     qb::LinkSet links;         // FP64
     qb::LinkSet sloppy_single;  // derived FP32 copy for mixed-precision solves
     qb::LinkSet sloppy_half;    // derived 16-bit copy
-    qb::LinkSet sloppy_recon;   // derived FP32 copy with 12-real Naik links
-    int recon_checked = 0;      // 1: the 12-real form was tried (sloppy_recon valid if it applied)
+    qb::LinkSet sloppy_recon;   // derived FP32 copy with 12-real or 13-real Naik links
+    int recon_checked = 0;      // 1: compression was tried (sloppy_recon valid if it applied)
 };
 struct QPHIX_F3_GaugeField_struct {
     void *geo;

@@ -56,20 +56,32 @@ template <> struct VecView<float> {
     }
 };
 
+// 16-bit fixed point is stored in offset binary, u = q + 32768 in [1, 65535].
+// Two values of a 32-bit word become floats without the conversion pipe
+// (I2F, an eighth of the FP32 rate, bounded the 16-bit Dslash): PRMT places
+// u in the mantissa of 2^23 (0x4B000000 | u = 2^23 + u exactly) and one FADD
+// removes 2^23 + 32768, leaving q exactly.
+__device__ __forceinline__ float2 fx16x2(unsigned w)
+{
+    return make_float2(__int_as_float(__byte_perm(w, 0x4B000000u, 0x7610)) - 8421376.0f,
+                       __int_as_float(__byte_perm(w, 0x4B000000u, 0x7632)) - 8421376.0f);
+}
+
 // 16-bit storage: per-site norm = max |component| of the site (float), each
 // component stored as 16-bit fixed point q = round(32767 v / norm).  Inside a
 // normalised site fixed point keeps 15 bits where FP16 keeps 11.  A site is
-// one 16-byte record {q0|q1, q2|q3, q4|q5, norm}.
+// one 16-byte record {u0|u1, u2|u3, u4|u5, norm} with u = q + 32768.
 template <> struct VecView<__half> {
     int4 *p;
     int vh;
     static __device__ __forceinline__ void unpack(const int4 w, float v[6]) {
         const float n = __int_as_float(w.w) * (1.0f / 32767.0f);
-        const int q[3] = {w.x, w.y, w.z};
+        const unsigned q[3] = {(unsigned)w.x, (unsigned)w.y, (unsigned)w.z};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            v[2 * k] = (float)(short)(q[k] & 0xffff) * n;
-            v[2 * k + 1] = (float)(short)((unsigned)q[k] >> 16) * n;
+            const float2 f = fx16x2(q[k]);
+            v[2 * k] = f.x * n;
+            v[2 * k + 1] = f.y * n;
         }
     }
     __device__ __forceinline__ void load(int j, float v[6]) const { unpack(__ldg(p + j), v); }
@@ -89,9 +101,9 @@ template <> struct VecView<__half> {
             q[k] = __float2int_rn(v[k] * inv);
             v[k] = (float)q[k] * n;
         }
-        p[j] = make_int4((int)(((unsigned)q[0] & 0xffffu) | ((unsigned)q[1] << 16)),
-                         (int)(((unsigned)q[2] & 0xffffu) | ((unsigned)q[3] << 16)),
-                         (int)(((unsigned)q[4] & 0xffffu) | ((unsigned)q[5] << 16)), __float_as_int(m));
+        p[j] = make_int4((int)((unsigned)(q[0] + 32768) | ((unsigned)(q[1] + 32768) << 16)),
+                         (int)((unsigned)(q[2] + 32768) | ((unsigned)(q[3] + 32768) << 16)),
+                         (int)((unsigned)(q[4] + 32768) | ((unsigned)(q[5] + 32768) << 16)), __float_as_int(m));
     }
 };
 
@@ -153,12 +165,17 @@ template <> struct LinkView<__half> {
 #pragma unroll
         for (int c = 0; c < 9; ++c) raw[c] = __ldcs(q + (size_t)c * vh);
     }
-    // matrix of slot s out of the raw chunks
+    // matrix of slot s out of the raw chunks (offset-binary 16-bit values,
+    // two per word: slot s is words 9s .. 9s+8)
     __device__ __forceinline__ void unpack(const int4 raw[9], int s, float u[18]) const {
         const float sc = s < 2 ? scale_fat : scale_long;
-        const short *h = reinterpret_cast<const short *>(raw);
+        const unsigned *w = reinterpret_cast<const unsigned *>(raw);
 #pragma unroll
-        for (int e = 0; e < 18; ++e) u[e] = h[18 * s + e] * sc;
+        for (int k = 0; k < 9; ++k) {
+            const float2 f = fx16x2(w[9 * s + k]);
+            u[2 * k] = f.x * sc;
+            u[2 * k + 1] = f.y * sc;
+        }
     }
 };
 

@@ -21,10 +21,11 @@ namespace qb {
 //                  c2[c*Vh + j]  (double2 / float2).  A warp reading 32
 //                  consecutive sites issues one fully used 512 B / 256 B
 //                  transaction per component.
-// 16-bit vector  : one 16-byte record per site, int4 rec[j] = {q0|q1,
-//                  q2|q3, q4|q5, norm}: the 6 reals as 16-bit fixed point of
-//                  v/norm and the float norm = max |component| of the site
-//                  (per-site scaling), so a neighbour gather is one load.
+// 16-bit vector  : one 16-byte record per site, int4 rec[j] = {u0|u1,
+//                  u2|u3, u4|u5, norm}: the 6 reals as 16-bit fixed point q
+//                  of v/norm, stored offset-binary u = q + 32768, and the
+//                  float norm = max |component| of the site (per-site
+//                  scaling), so a neighbour gather is one load.
 // Link block     : the 16 matrices an output site needs, grouped by
 //                  direction d: slot s = 0 fat forward F_d(x), 1 fat backward
 //                  B_d(x), 2 Naik forward L_d(x), 3 Naik backward LB_d(x);
@@ -36,9 +37,10 @@ namespace qb {
 //                  nothing about links is gathered.  The block for output
 //                  parity cb is built from raw sites cb*Vh + j
 //                  (qphix_f3.cpp:995-1018).
-// Half links     : short2 fixed point per complex, value = q * link_max/32767
-//                  with one range for the fat slots and one for the Naik
-//                  slots (Naik links are ~1/24 the size of fat links).
+// Half links     : 16-bit fixed point per real, value = q * link_max/32767,
+//                  stored offset-binary u = q + 32768, with one range for the
+//                  fat slots and one for the Naik slots (Naik links are ~1/24
+//                  the size of fat links).
 // ----------------------------------------------------------------------------
 constexpr int kMats = 16;
 constexpr int kLinkReals = kMats * 18;  // reals per site in a link block

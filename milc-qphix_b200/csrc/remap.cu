@@ -230,9 +230,10 @@ __global__ void k_links_convert(D *dst, int kd, const S *src, int ks, int vh, fl
     const S z = src[link_cx_index(ks, d, c, j, vh)];
     D q;
     if constexpr (std::is_same<D, short2>::value) {
+        // offset binary u = q + 32768 (see fx16x2 in device_common.cuh)
         const float inv = (c / 9) >= 2 ? inv_long : inv_fat;
-        q.x = (short)__float2int_rn((float)z.x * inv);
-        q.y = (short)__float2int_rn((float)z.y * inv);
+        q.x = (short)(unsigned short)(__float2int_rn((float)z.x * inv) + 32768);
+        q.y = (short)(unsigned short)(__float2int_rn((float)z.y * inv) + 32768);
     } else {
         q.x = z.x;
         q.y = z.y;
