@@ -165,16 +165,16 @@ template <> struct LinkView<__half> {
 #pragma unroll
         for (int c = 0; c < 9; ++c) raw[c] = __ldcs(q + (size_t)c * vh);
     }
-    // matrix of slot s out of the raw chunks (offset-binary 16-bit values,
-    // two per word: slot s is words 9s .. 9s+8)
-    __device__ __forceinline__ void unpack(const int4 raw[9], int s, float u[18]) const {
-        const float sc = s < 2 ? scale_fat : scale_long;
+    // the fixed-point integers q of slot s out of the raw chunks
+    // (offset-binary 16-bit values, two per word: slot s is words 9s .. 9s+8);
+    // the link is q * scale_fat (slots 0, 1) or q * scale_long (slots 2, 3)
+    __device__ __forceinline__ static void unpack_q(const int4 raw[9], int s, float u[18]) {
         const unsigned *w = reinterpret_cast<const unsigned *>(raw);
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
             const float2 f = fx16x2(w[9 * s + k]);
-            u[2 * k] = f.x * sc;
-            u[2 * k + 1] = f.y * sc;
+            u[2 * k] = f.x;
+            u[2 * k + 1] = f.y;
         }
     }
 };

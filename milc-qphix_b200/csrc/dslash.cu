@@ -105,9 +105,15 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
         }
     } else {
         // 16-bit links: the four matrices of a direction, 9 x 16 bytes + 4
-        // neighbours per stage, pipelined over the directions like FP32
+        // neighbours per stage, pipelined over the directions like FP32.
+        // All fat links share one fixed-point range and all Naik links
+        // another, so the fat and Naik terms are summed from the unscaled
+        // integers and each sum is scaled once at the end.
         int4 raw[2][9];
         A v[2][4][6];
+        A accl[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) accl[i] = A(0);
         auto issue = [&](int d, int b) {
 #pragma unroll
             for (int sl = 0; sl < 4; ++sl)
@@ -122,11 +128,14 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
 #pragma unroll
             for (int sl = 0; sl < 4; ++sl) {
                 A u[18];
-                a.links.unpack(raw[b], sl, u);
-                if (sl & 1) mv_adj_sub(acc, u, v[b][sl]);
-                else mv_add(acc, u, v[b][sl]);
+                a.links.unpack_q(raw[b], sl, u);
+                A *t = sl < 2 ? acc : accl;
+                if (sl & 1) mv_adj_sub(t, u, v[b][sl]);
+                else mv_add(t, u, v[b][sl]);
             }
         }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) acc[i] = acc[i] * a.links.scale_fat + accl[i] * a.links.scale_long;
     }
 }
 
@@ -293,7 +302,10 @@ __device__ __forceinline__ void tma_direction(const DslashArgs<SV, SL> &a, const
 #pragma unroll
         for (int sl = 0; sl < 4; ++sl) {
             A u[18];
-            a.links.unpack(raw, sl, u);
+            a.links.unpack_q(raw, sl, u);
+            const A sc = sl < 2 ? a.links.scale_fat : a.links.scale_long;
+#pragma unroll
+            for (int e = 0; e < 18; ++e) u[e] *= sc;
             if (sl & 1) mv_adj_sub(acc, u, v[sl]);
             else mv_add(acc, u, v[sl]);
         }
