@@ -429,8 +429,9 @@ __device__ __forceinline__ void bdslash_s_item(int item, int cb, float2 *out, co
     bstore<G>(out + sg.voff, sg.g.vh, sg.nrhs, j, q, a);
 }
 
-// GMAX: largest G of the table's segments.  With G <= 2 the kernel fits in
-// 80 registers (3 blocks of 256 per SM); G = 3, 4 need 128 (2 blocks).
+// GMAX: largest G of the table's segments.  With G = 1 the kernel fits in
+// 64 registers (4 blocks of 256 per SM), with G = 2 in 80 (3 blocks); G = 3,
+// 4 need 128 (2 blocks).
 template <bool MDAGM, int GMAX>
 __global__ void __launch_bounds__(kBlock, GMAX == 1 ? 4 : (GMAX == 2 ? 3 : 2)) k_bdslash_s(const BTable *tab, BState *st, float2 *out,
                                                          const float2 *in, const float2 *pv, int cb,
