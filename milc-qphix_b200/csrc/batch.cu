@@ -223,13 +223,40 @@ __device__ __forceinline__ void b_masks(BState *st)
 }
 
 // ------------------------------------------------- multi-RHS vector loads --
+// 32-byte loads and stores (sm_100): four right-hand sides of one colour
+// component in one instruction, so the four threads of a site move a whole
+// 128-byte line each time.  The addresses are 32-byte aligned: segments of
+// four or more systems start on multiples of 24 * Vh * nrhs bytes and Vh is
+// a multiple of 128.  Read-only data of the launch only (non-coherent path).
+__device__ __forceinline__ void ld_nc_v8(const float2 *p, float w[8])
+{
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(w[0]), "=f"(w[1]), "=f"(w[2]), "=f"(w[3]), "=f"(w[4]), "=f"(w[5]), "=f"(w[6]), "=f"(w[7])
+        : "l"(p));
+}
+
+__device__ __forceinline__ void st_v8(float2 *p, const float w[8])
+{
+    asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(w[0]), "f"(w[1]), "f"(w[2]),
+                 "f"(w[3]), "f"(w[4]), "f"(w[5]), "f"(w[6]), "f"(w[7])
+                 : "memory");
+}
+
 template <int G>
 __device__ __forceinline__ void bload(const float2 *f, int vh, int nrhs, int j, int q, float v[G][6])
 {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const float2 *p = f + ((size_t)(c * vh + j) * nrhs + q * G);
-        if constexpr (G % 2 == 1) {
+        if constexpr (G == 4) {
+            float w[8];
+            ld_nc_v8(p, w);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                v[e][2 * c] = w[2 * e];
+                v[e][2 * c + 1] = w[2 * e + 1];
+            }
+        } else if constexpr (G % 2 == 1) {
 #pragma unroll
             for (int e = 0; e < G; ++e) {
                 const float2 z = __ldg(p + e);
@@ -252,7 +279,15 @@ __device__ __forceinline__ void bstore(float2 *f, int vh, int nrhs, int j, int q
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float2 *p = f + ((size_t)(c * vh + j) * nrhs + q * G);
-        if constexpr (G % 2 == 1) {
+        if constexpr (G == 4) {
+            float w[8];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                w[2 * e] = v[e][2 * c];
+                w[2 * e + 1] = v[e][2 * c + 1];
+            }
+            st_v8(p, w);
+        } else if constexpr (G % 2 == 1) {
 #pragma unroll
             for (int e = 0; e < G; ++e) p[e] = make_float2(v[e][2 * c], v[e][2 * c + 1]);
         } else {
