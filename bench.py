@@ -421,6 +421,27 @@ def ref_iteration_sample(links, src, n_iter, dims=DIMS, mass=MASS):
     return dt, res.final_iter
 
 
+def ref_multishift_sample(links, src, n_iter, dims, masses):
+    """Time n_iter FP64 multi-shift iterations of the reference's own solver
+    (ks_multicg_offset.cpp, OpenMP on all host cores) on the full lattice."""
+    import orc
+
+    ref = capi.QphixLib(orc.REF_LIB)
+    ref.init(dims)
+    L = ref.create_L("D", links)
+    b = ref.create_V("D", src, "even")
+    xs = [ref.create_V("D", np.zeros_like(src), "even") for _ in masses]
+    t0 = time.perf_counter()
+    it, info, res = ref.invert_multi("D", L, xs, b, masses, parity="even", max_iter=n_iter, nrestart=1, resid=RESID)
+    dt = time.perf_counter() - t0
+    for x in xs:
+        ref.destroy_V("D", x)
+    ref.destroy_V("D", b)
+    ref.destroy_L("D", L)
+    ref.finalize()
+    return dt, it
+
+
 class _StdoutToStderr:
     """The reference host code prints progress lines to stdout; while it runs
     inside the GPU arm they go to stderr, so stdout carries only the JSON line."""
@@ -494,12 +515,47 @@ def run_reference(args):
 FP64_ITERATIONS = 808
 
 
+def run_reference_dslash(args, dims, links):
+    """--mode dslash --impl reference: the reference's own Dslash
+    (qphix_ks_dslash, ks_long_dslash.cpp:564-668, with the restated per-site
+    kernel; OpenMP on all host cores), wall-clock timed over --reps calls
+    after one warm-up call, GB/s by the same algorithmic bytes."""
+    import orc
+
+    V = int(np.prod(dims))
+    ref = capi.QphixLib(orc.REF_LIB)
+    out = {}
+    with _StdoutToStderr():
+        assert ref.init(dims) == 0
+        for prec in ("F", "D"):
+            L = ref.create_L(prec, links)
+            vin = ref.create_V(prec, np.random.default_rng(1).standard_normal(V * 6))
+            vout = ref.create_V(prec, np.zeros(V * 6))
+            ref.dslash(prec, L, vout, vin, "even")
+            t0 = time.perf_counter()
+            for _ in range(args.reps):
+                ref.dslash(prec, L, vout, vin, "even")
+            dt = (time.perf_counter() - t0) / args.reps
+            nbytes = (DSLASH_BYTES_F32 if prec == "F" else DSLASH_BYTES_F64) * (V // 2)
+            out[prec] = {"us": dt * 1e6, "gbs": nbytes / dt / 1e9}
+            ref.destroy_V(prec, vin)
+            ref.destroy_V(prec, vout)
+            ref.destroy_L(prec, L)
+        ref.finalize()
+    print(json.dumps({"mode": "dslash", "impl": "reference", "lattice": "x".join(map(str, dims)), "reps": args.reps,
+                      "cores": os.cpu_count(), **out}))
+
+
 def run_profile_dslash(args):
     """--mode dslash: one FP32 and one FP64 Dslash launch after a warm-up
-    (small-lattice capture target for ncu)."""
+    (small-lattice capture target for ncu); with --impl reference the
+    reference's host Dslash on the same lattice instead."""
     dims = tuple(int(v) for v in (args.lattice or "16x16x16x32").split("x"))
     links = synthetic.asqtad_links(dims, seed=LINK_SEED)
     V = int(np.prod(dims))
+    if args.impl == "reference":
+        run_reference_dslash(args, dims, links)
+        return
     lib = capi.QphixLib(LIB_PATH)
     assert lib.init(dims) == 0, lib.last_error()
     out = {}
@@ -706,6 +762,14 @@ def run_multishift(args):
                 "s": dt / max(done, 1) * out["fp64_cg"]["iterations"], "cores": os.cpu_count(), "kind": "reference",
                 "sample": f"{done} FP64 CG iterations of the reference solver on the full lattice ({dt:.1f} s), "
                           f"scaled to the {out['fp64_cg']['iterations']} iterations of the FP64 solve"}
+            if "fp64_multishift" in out:
+                with _StdoutToStderr():
+                    dt, done = ref_multishift_sample(links, src, 6, dims, masses)
+                full = out["fp64_multishift"]["iterations"]
+                out["cpu_baseline_fp64_multishift"] = {
+                    "s": dt / max(done, 1) * full, "cores": os.cpu_count(), "kind": "reference",
+                    "sample": f"{done} FP64 multi-shift iterations (12 shifts) of the reference solver on the full "
+                              f"lattice ({dt:.1f} s), scaled to the {full} iterations of the FP64 multi-shift"}
     print(json.dumps(out))
 
 

@@ -41,7 +41,7 @@ QPHIX_B200_precision_t QPHIX_B200_get_inner_precision(void);
 /* Reliable-update threshold of the mixed-precision solvers: the FP64 true
  * residual is recomputed when the sloppy residual norm has dropped by this
  * factor since the last update (default 0.2).  The per-shift refinements
- * that end a mixed multi-shift use a quarter of it. */
+ * that end a mixed multi-shift with FP32 links use a quarter of it. */
 QPHIX_status_t QPHIX_B200_set_reliable_delta(double delta);
 
 /* Compressed Naik links for the FP32 inner solves of QPHIX_D3_asqtad_invert /

@@ -875,15 +875,17 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
         total += r.iteration;
         last = r.iteration;
         // refinement of every shift to its own tolerance from the sloppy
-        // solution.  The refinements take their reliable updates at a quarter
-        // of the CG threshold: at 32^3x64 the iteration counts are the same
-        // for 0.05, 0.1 and 0.2 while the updates drop from 65 to 40
-        // (0.826 -> 0.801 s for the whole multi-shift).
+        // solution.  With FP32 links the refinements take their reliable
+        // updates at a quarter of the CG threshold: at 32^3x64 the iteration
+        // counts are the same for 0.05, 0.1 and 0.2 while the updates drop
+        // from 65 to 40 (0.826 -> 0.801 s for the whole multi-shift).  With
+        // 16-bit links the updates also detect a stalled refinement (which
+        // then continues in FP32), so they keep the CG threshold.
         struct DeltaScope {  // restores the threshold on every exit path
             double &d, keep;
             DeltaScope(double &v, double f) : d(v), keep(v) { d = f * v; }
             ~DeltaScope() { d = keep; }
-        } refine_delta(c.reliable_delta, kRefineDeltaFactor);
+        } refine_delta(c.reliable_delta, base_ru_on ? kRefineDeltaFactor : 1.0);
         for (int j = 0; j < n; ++j) {
             const double tol = A.res[j]->resid > 0 ? A.res[j]->resid : A.res[0]->resid;
             MixedResult m = mixed_pass(ps, ls64, lss, ls_up, x[j], src, parity, A.mass[j], tol, max_cg, tl);
