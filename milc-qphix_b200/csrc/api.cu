@@ -115,6 +115,7 @@ void finalize_context()
     }
     for (auto e : c.ktimer.ev) cudaEventDestroy(e);
     c.ktimer.ev.clear();
+    free_staging();
     cudaStreamDestroy(c.stream);
     c.stream = nullptr;
     c.d_state = nullptr;
@@ -233,11 +234,12 @@ typename Api<Real>::FL *create_L(Real *fat, Real *lng, Real *fatback, Real *lngb
         for (int slot = 0; slot < 4; ++slot) {
             QB_CUDA(cudaMemsetAsync(stage, 0, 2 * nhalf * sizeof(Real), c.stream));
             // only the parities asked for are read, as in qphix_f3.cpp:976-1063
-            if (evenodd & QPHIX_EVEN)
-                QB_CUDA(cudaMemcpyAsync(stage, raw[slot], nhalf * sizeof(Real), cudaMemcpyHostToDevice, c.stream));
-            if (evenodd & QPHIX_ODD)
-                QB_CUDA(cudaMemcpyAsync(stage + nhalf, raw[slot] + nhalf, nhalf * sizeof(Real),
-                                        cudaMemcpyHostToDevice, c.stream));
+            if ((evenodd & QPHIX_EVENODD) == QPHIX_EVENODD) {
+                h2d_copy(stage, raw[slot], 2 * nhalf * sizeof(Real));
+            } else {
+                if (evenodd & QPHIX_EVEN) h2d_copy(stage, raw[slot], nhalf * sizeof(Real));
+                if (evenodd & QPHIX_ODD) h2d_copy(stage + nhalf, raw[slot] + nhalf, nhalf * sizeof(Real));
+            }
             links_from_raw(Api<Real>::prec, H->links, stage, sizeof(Real) == 8, slot, c.launch());
         }
         dev_free(stage);

@@ -1266,7 +1266,7 @@ static QPHIX_B200_Batch *batch_create(int nlat, const int *latsize, double *cons
             void *stage = dev_alloc(nraw * sizeof(double));
             const double *raw[4] = {fat[l], fatback[l], lng[l], lngback[l]};  // slots 0..3
             for (int slot = 0; slot < 4; ++slot) {
-                QB_CUDA(cudaMemcpyAsync(stage, raw[slot], nraw * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+                h2d_copy(stage, raw[slot], nraw * sizeof(double));
                 links_from_raw(Prec::Double, H.l64, stage, true, slot, ln);
             }
             dev_free(stage);

@@ -1,4 +1,9 @@
 // Context, device memory and state transfer helpers.
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <thread>
+
 #include "context.h"
 #include "device_common.cuh"
 
@@ -27,6 +32,89 @@ void *dev_alloc(size_t bytes)
 void dev_free(void *p)
 {
     if (p) cudaFreeAsync(p, ctx().stream);
+}
+
+namespace {
+
+constexpr size_t kStageBytes = 8u << 20;      // one pinned slot
+constexpr size_t kStageMinBytes = 64u << 20;  // smaller copies go in one call
+
+void make_staging(Context &c)
+{
+    HostStaging &h = c.staging;
+    if (h.workers) return;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int w = (int)std::max(1u, std::min(8u, hw / 2));
+    for (int i = 0; i < w; ++i) {
+        cudaStream_t s;
+        QB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        h.streams.push_back(s);
+        for (int k = 0; k < 2; ++k) {
+            void *p = nullptr;
+            QB_CUDA(cudaHostAlloc(&p, kStageBytes, cudaHostAllocDefault));
+            h.slots.push_back(static_cast<char *>(p));
+            cudaEvent_t e;
+            QB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            h.done.push_back(e);
+        }
+        h.workers = i + 1;
+    }
+}
+
+}  // namespace
+
+void free_staging()
+{
+    HostStaging &h = ctx().staging;
+    for (auto s : h.streams) cudaStreamDestroy(s);
+    for (auto p : h.slots) cudaFreeHost(p);
+    for (auto e : h.done) cudaEventDestroy(e);
+    h = HostStaging{};
+}
+
+void h2d_copy(void *dst, const void *src, size_t bytes)
+{
+    Context &c = ctx();
+    if (bytes == 0) return;
+    cudaPointerAttributes at{};
+    const bool pinned = cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // an unregistered pointer is not an error here
+    if (pinned || bytes < kStageMinBytes) {
+        QB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c.stream));
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+        return;
+    }
+    make_staging(c);
+    // work already queued on the library stream (e.g. a memset of dst)
+    // finishes before the worker streams write dst
+    QB_CUDA(cudaStreamSynchronize(c.stream));
+    HostStaging &h = c.staging;
+    const int W = h.workers;
+    std::atomic<int> failed{0};
+    std::vector<std::thread> th;
+    for (int w = 0; w < W; ++w) {
+        th.emplace_back([&, w] {
+            if (cudaSetDevice(c.device) != cudaSuccess) { failed = 1; return; }
+            // contiguous part of the source, 4 KiB aligned
+            const size_t lo = (bytes * w / W) & ~(size_t)4095, hi = w + 1 == W ? bytes : (bytes * (w + 1) / W) & ~(size_t)4095;
+            int k = 0;
+            for (size_t off = lo; off < hi; off += kStageBytes, ++k) {
+                const size_t n = std::min(kStageBytes, hi - off);
+                const int sl = 2 * w + (k & 1);
+                if (k >= 2 && cudaEventSynchronize(h.done[sl]) != cudaSuccess) { failed = 1; break; }
+                std::memcpy(h.slots[sl], static_cast<const char *>(src) + off, n);
+                if (cudaMemcpyAsync(static_cast<char *>(dst) + off, h.slots[sl], n, cudaMemcpyHostToDevice,
+                                    h.streams[w]) != cudaSuccess ||
+                    cudaEventRecord(h.done[sl], h.streams[w]) != cudaSuccess) {
+                    failed = 1;
+                    break;
+                }
+            }
+            if (cudaStreamSynchronize(h.streams[w]) != cudaSuccess) failed = 1;
+        });
+    }
+    for (auto &t : th) t.join();
+    if (failed) throw Error("host to device copy through pinned staging failed");
 }
 
 void check_lattice(const int L[4], const char *who)

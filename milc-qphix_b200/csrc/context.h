@@ -67,6 +67,15 @@ struct KernelTimer {
     }
 };
 
+// Pinned staging for host -> device copies from pageable memory (h2d_copy):
+// one CUDA stream and two pinned slots per host worker thread.
+struct HostStaging {
+    int workers = 0;
+    std::vector<cudaStream_t> streams;
+    std::vector<char *> slots;
+    std::vector<cudaEvent_t> done;
+};
+
 struct Context {
     bool initialized = false;
     int dims[4] = {0, 0, 0, 0};
@@ -92,6 +101,7 @@ struct Context {
     std::string last_error;
 
     int *d_err = nullptr;            // kernel failure word (bounded waits)
+    HostStaging staging;             // made on the first large pageable upload
 
     Launch launch() const { return Launch{stream, &g, d_err}; }
 };
@@ -101,6 +111,13 @@ Context &ctx();
 // device memory from the stream-ordered pool (cached, no device-wide sync)
 void *dev_alloc(size_t bytes);
 void dev_free(void *p);
+
+// Host -> device copy that has completed on return.  Pinned or small
+// sources go by one cudaMemcpyAsync on the library stream; large pageable
+// ones are split across host threads, each copying its part through two
+// pinned slots while the copy engine moves the previous slot.
+void h2d_copy(void *dst, const void *src, size_t bytes);
+void free_staging();
 
 VecBlock alloc_vec(Prec p);
 void free_vec(VecBlock &b);
