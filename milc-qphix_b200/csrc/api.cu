@@ -157,7 +157,7 @@ typename Api<Real>::CV *create_V(Real *src, QPHIX_evenodd_t evenodd)
             const int want = cb == 0 ? (evenodd & QPHIX_EVEN) : (evenodd & QPHIX_ODD);
             if (!want) continue;
             V->blk[cb] = alloc_vec(Api<Real>::prec);
-            QB_CUDA(cudaMemcpyAsync(stage, src + cb * nblk, nblk * sizeof(Real), cudaMemcpyHostToDevice, c.stream));
+            h2d_copy(stage, src + cb * nblk, nblk * sizeof(Real));
             vec_from_raw(Api<Real>::prec, V->blk[cb], stage, sizeof(Real) == 8, c.launch());
         }
         dev_free(stage);
@@ -187,7 +187,7 @@ void extract_V(Real *dest, typename Api<Real>::CV *V)
             const int have = cb == 0 ? (V->parity & QPHIX_EVEN) : (V->parity & QPHIX_ODD);
             if (!have) continue;
             vec_to_raw(Api<Real>::prec, stage, sizeof(Real) == 8, V->blk[cb], c.launch());
-            QB_CUDA(cudaMemcpyAsync(dest + cb * nblk, stage, nblk * sizeof(Real), cudaMemcpyDeviceToHost, c.stream));
+            d2h_copy(dest + cb * nblk, stage, nblk * sizeof(Real));
         }
         dev_free(stage);
         sync_check();
@@ -271,11 +271,8 @@ void extract_L(Real *fat, Real *lng, typename Api<Real>::FL *H, QPHIX_evenodd_t 
         const int slots[2] = {0, 2};  // forward links only (qphix_f3.cpp:1125-1143)
         for (int f = 0; f < 2; ++f) {
             links_to_raw(Api<Real>::prec, stage, sizeof(Real) == 8, H->links, slots[f], c.launch());
-            if (evenodd & QPHIX_EVEN)
-                QB_CUDA(cudaMemcpyAsync(dst[f], stage, nhalf * sizeof(Real), cudaMemcpyDeviceToHost, c.stream));
-            if (evenodd & QPHIX_ODD)
-                QB_CUDA(cudaMemcpyAsync(dst[f] + nhalf, stage + nhalf, nhalf * sizeof(Real), cudaMemcpyDeviceToHost,
-                                        c.stream));
+            if (evenodd & QPHIX_EVEN) d2h_copy(dst[f], stage, nhalf * sizeof(Real));
+            if (evenodd & QPHIX_ODD) d2h_copy(dst[f] + nhalf, stage + nhalf, nhalf * sizeof(Real));
             sync_check();
         }
         dev_free(stage);

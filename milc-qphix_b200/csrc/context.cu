@@ -37,7 +37,7 @@ void dev_free(void *p)
 namespace {
 
 constexpr size_t kStageBytes = 8u << 20;      // one pinned slot
-constexpr size_t kStageMinBytes = 64u << 20;  // smaller copies go in one call
+constexpr size_t kStageMinBytes = 16u << 20;  // smaller copies go in one call
 
 void make_staging(Context &c)
 {
@@ -115,6 +115,58 @@ void h2d_copy(void *dst, const void *src, size_t bytes)
     }
     for (auto &t : th) t.join();
     if (failed) throw Error("host to device copy through pinned staging failed");
+}
+
+void d2h_copy(void *dst, const void *src, size_t bytes)
+{
+    Context &c = ctx();
+    if (bytes == 0) return;
+    cudaPointerAttributes at{};
+    const bool pinned = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // an unregistered pointer is not an error here
+    if (pinned || bytes < kStageMinBytes) {
+        QB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c.stream));
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+        return;
+    }
+    make_staging(c);
+    // the kernels that produce src finish before the worker streams read it
+    QB_CUDA(cudaStreamSynchronize(c.stream));
+    HostStaging &h = c.staging;
+    const int W = h.workers;
+    std::atomic<int> failed{0};
+    std::vector<std::thread> th;
+    for (int w = 0; w < W; ++w) {
+        th.emplace_back([&, w] {
+            if (cudaSetDevice(c.device) != cudaSuccess) { failed = 1; return; }
+            const size_t lo = (bytes * w / W) & ~(size_t)4095, hi = w + 1 == W ? bytes : (bytes * (w + 1) / W) & ~(size_t)4095;
+            // chunk k goes device -> slot k&1 while the host copies chunk k-1 out of the other slot
+            size_t prev_off = 0, prev_n = 0;
+            int k = 0;
+            auto drain = [&](int slot) {
+                if (cudaEventSynchronize(h.done[slot]) != cudaSuccess) { failed = 1; return false; }
+                std::memcpy(static_cast<char *>(dst) + prev_off, h.slots[slot], prev_n);
+                return true;
+            };
+            for (size_t off = lo; off < hi; off += kStageBytes, ++k) {
+                const size_t n = std::min(kStageBytes, hi - off);
+                const int sl = 2 * w + (k & 1);
+                if (cudaMemcpyAsync(h.slots[sl], static_cast<const char *>(src) + off, n, cudaMemcpyDeviceToHost,
+                                    h.streams[w]) != cudaSuccess ||
+                    cudaEventRecord(h.done[sl], h.streams[w]) != cudaSuccess) {
+                    failed = 1;
+                    break;
+                }
+                if (k > 0 && !drain(2 * w + ((k - 1) & 1))) break;
+                prev_off = off;
+                prev_n = n;
+            }
+            if (!failed && k > 0) drain(2 * w + ((k - 1) & 1));
+            if (cudaStreamSynchronize(h.streams[w]) != cudaSuccess) failed = 1;
+        });
+    }
+    for (auto &t : th) t.join();
+    if (failed) throw Error("device to host copy through pinned staging failed");
 }
 
 void check_lattice(const int L[4], const char *who)

@@ -117,6 +117,8 @@ void dev_free(void *p);
 // ones are split across host threads, each copying its part through two
 // pinned slots while the copy engine moves the previous slot.
 void h2d_copy(void *dst, const void *src, size_t bytes);
+// the same for device -> host (completed on return)
+void d2h_copy(void *dst, const void *src, size_t bytes);
 void free_staging();
 
 VecBlock alloc_vec(Prec p);

@@ -117,8 +117,8 @@ static void force_impl(typename ForceApi<Real>::FL *H, int n, const Real *coef, 
         }
         QB_CUDA(cudaGetLastError());
         QB_CUDA(cudaEventRecord(c.ev_solve[1], c.stream));
-        QB_CUDA(cudaMemcpyAsync(grad_fat, g, nraw * sizeof(Real), cudaMemcpyDeviceToHost, c.stream));
-        QB_CUDA(cudaMemcpyAsync(grad_lng, g + nraw, nraw * sizeof(Real), cudaMemcpyDeviceToHost, c.stream));
+        d2h_copy(grad_fat, g, nraw * sizeof(Real));
+        d2h_copy(grad_lng, g + nraw, nraw * sizeof(Real));
         sync_check();
         float ms = 0.f;
         QB_CUDA(cudaEventElapsedTime(&ms, c.ev_solve[0], c.ev_solve[1]));
