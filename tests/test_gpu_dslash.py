@@ -175,3 +175,36 @@ def test_dslash_fp32_vectors_16bit_links(gpu):
     for h in (b, x):
         lib.destroy_V("D", h)
     lib.destroy_L("D", L)
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_large_round_trips_bit_exact(gpu, pinned):
+    """Round trips large enough for the pinned-staging copies (16 MB and up,
+    split across host threads): 24^3x48 colour vectors (32 MB) and 16^3x32
+    links (75 MB per array), from pageable numpy arrays and from pinned ones
+    (which are copied directly)."""
+    import torch
+
+    def host(a):
+        if not pinned:
+            return a
+        t = torch.empty(a.shape, dtype=torch.float64).pin_memory()
+        t.numpy()[...] = a
+        return t.numpy()
+
+    dims = (24, 24, 24, 48)
+    lib = gpu.use(dims)
+    src = host(np.random.default_rng(7).standard_normal(6 * int(np.prod(dims))))
+    h = lib.create_V("D", src)
+    back = lib.extract_V("D", h)
+    lib.destroy_V("D", h)
+    assert np.array_equal(back, src)
+
+    dims = (16, 16, 16, 32)
+    lib = gpu.use(dims)
+    dev = "cuda" if torch.cuda.is_available() else None
+    links = {k: host(v) for k, v in synthetic.asqtad_links(dims, seed=3, device=dev).items()}
+    L = lib.create_L("D", links)
+    fat, lng = lib.extract_L("D", L)
+    lib.destroy_L("D", L)
+    assert np.array_equal(fat, links["fat"]) and np.array_equal(lng, links["lng"])
