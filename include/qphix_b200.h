@@ -57,7 +57,8 @@ QPHIX_status_t QPHIX_B200_set_reliable_delta(double delta);
  * A field of neither form keeps its 18-real links; QPHIX_B200_get_last_stats
  * reports which was used.  FP64 links and all FP64 arithmetic are
  * unaffected.  Saves 16 % (12-real) or 11 % (13-real) of the FP32 Dslash's
- * bytes. */
+ * bytes.  QPHIX_GPU_LINK_COMPRESSION=1 in the environment sets it at
+ * QPHIX_init. */
 QPHIX_status_t QPHIX_B200_set_link_compression(int on);
 
 /* Diagnostics of the most recent invert / invert_multi / batch_invert call. */

@@ -93,6 +93,9 @@ void init_context(QPHIX_layout_t *layout)
         QB_CUDA(cudaEventCreate(&c.ev_user[i]));
     }
     c.inner_mode = env_precision(QPHIX_B200_PREC_DOUBLE);
+    // compressed Naik links for the FP32 inner solves without code changes
+    const char *lc = std::getenv("QPHIX_GPU_LINK_COMPRESSION");
+    c.link_compression = (lc && lc[0] == '1') ? 1 : 0;
     c.verbose = std::getenv("QPHIX_B200_VERBOSE") ? std::atoi(std::getenv("QPHIX_B200_VERBOSE")) : 0;
     c.initialized = true;
 }

@@ -125,3 +125,40 @@ def test_non_unitary_naik_links_keep_18_reals(gpu):
     st, (x,) = _solve(lib, links, src, 0.03, True)
     assert st.links_compressed == 0
     assert orc.true_residual(DIMS, links, x, src, 0.03, "even") < 1.5 * RESID
+
+
+def test_link_compression_from_environment(gpu, monkeypatch):
+    """QPHIX_GPU_LINK_COMPRESSION=1 turns compression on at QPHIX_init (for
+    MILC builds that call only the reference API); without it the library
+    starts with 18-real links."""
+    lib = gpu.use(DIMS)
+    links = fields(DIMS, seed=21)
+    src = synthetic.gaussian_source(DIMS, seed=2002, parity="even")
+
+    def solve_stats():
+        lib.set_inner_precision("single")
+        try:
+            L = lib.create_L("D", links)
+            b = lib.create_V("D", src, "even")
+            x = lib.create_V("D", np.zeros_like(src), "even")
+            it, info, res = lib.invert("D", L, x, b, 0.03, parity="even", max_iter=4000, nrestart=5, resid=RESID)
+            assert info.status == 0, lib.last_error()
+            st = lib.last_stats()
+            for h in (x, b):
+                lib.destroy_V("D", h)
+            lib.destroy_L("D", L)
+        finally:
+            lib.set_inner_precision("double")
+        return st
+
+    try:
+        monkeypatch.setenv("QPHIX_GPU_LINK_COMPRESSION", "1")
+        lib.finalize()
+        assert lib.init(DIMS) == 0
+        assert solve_stats().links_compressed == 1
+        monkeypatch.delenv("QPHIX_GPU_LINK_COMPRESSION")
+        lib.finalize()
+        assert lib.init(DIMS) == 0
+        assert solve_stats().links_compressed == 0
+    finally:
+        lib.set_link_compression(False)
