@@ -76,11 +76,13 @@ void h2d_copy(void *dst, const void *src, size_t bytes)
 {
     Context &c = ctx();
     if (bytes == 0) return;
+    // only plain pageable host memory is staged; pinned, managed or device
+    // memory goes by one copy (direction from the unified address space)
     cudaPointerAttributes at{};
-    const bool pinned = cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    const bool pageable = cudaPointerGetAttributes(&at, src) != cudaSuccess || at.type == cudaMemoryTypeUnregistered;
     cudaGetLastError();  // an unregistered pointer is not an error here
-    if (pinned || bytes < kStageMinBytes) {
-        QB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c.stream));
+    if (!pageable || bytes < kStageMinBytes) {
+        QB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c.stream));
         QB_CUDA(cudaStreamSynchronize(c.stream));
         return;
     }
@@ -122,10 +124,10 @@ void d2h_copy(void *dst, const void *src, size_t bytes)
     Context &c = ctx();
     if (bytes == 0) return;
     cudaPointerAttributes at{};
-    const bool pinned = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    const bool pageable = cudaPointerGetAttributes(&at, dst) != cudaSuccess || at.type == cudaMemoryTypeUnregistered;
     cudaGetLastError();  // an unregistered pointer is not an error here
-    if (pinned || bytes < kStageMinBytes) {
-        QB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c.stream));
+    if (!pageable || bytes < kStageMinBytes) {
+        QB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c.stream));
         QB_CUDA(cudaStreamSynchronize(c.stream));
         return;
     }
