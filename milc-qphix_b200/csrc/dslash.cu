@@ -140,17 +140,17 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
 }
 
 // blocks of 256 per SM the register allocation must allow.  The pipelined
-// kernels keep one stage in flight in 80 registers at 3 blocks/SM (64 at 4
-// with 16-bit vectors).  24^3x48 mixed solves: 12-real 100.7 ms (4 blocks:
-// 107.8 ms); 18-real 113.9 ms (1 block at 241 registers: 116.7 ms); 16-bit
-// links 93.6 ms (1 block: 118.1 ms); 16-bit vectors and links 101.3 ms (2
-// blocks: 106.7 ms)
+// kernels keep one stage in flight in 80 registers at 3 blocks/SM.
+// 24^3x48 mixed solves: 12-real 100.7 ms (4 blocks: 107.8 ms); 18-real
+// 113.9 ms (1 block at 241 registers: 116.7 ms); 16-bit links 93.6 ms (1
+// block: 118.1 ms); 16-bit vectors and links 88.7 ms (4 blocks at 64
+// registers: 93.0 ms)
 template <typename SV, typename SL> struct MinBlocks { static constexpr int value = 1; };
 template <> struct MinBlocks<float, float> { static constexpr int value = 3; };
 template <> struct MinBlocks<float, Recon12> { static constexpr int value = 3; };
 template <> struct MinBlocks<float, Recon13> { static constexpr int value = 3; };
 template <> struct MinBlocks<float, __half> { static constexpr int value = 3; };
-template <> struct MinBlocks<__half, __half> { static constexpr int value = 4; };
+template <> struct MinBlocks<__half, __half> { static constexpr int value = 3; };
 
 // Scalar step after p.(M^dag M p) is known: CG (mode 0) a = -rsq/pkp;
 // multi-shift (mode 1) the shift recurrences.  Runs in one thread.
