@@ -60,8 +60,6 @@ template <typename R> using cx_t = typename Cx<R>::type;
 
 enum class Prec : int { Half = 0, Single = 1, Double = 2 };
 
-inline size_t prec_real_bytes(Prec p) { return p == Prec::Double ? 8 : (p == Prec::Single ? 4 : 2); }
-
 // One parity block of a colour vector in device memory.
 struct VecBlock {
     void *data = nullptr;   // cx_t<R>[3*Vh]   (16-bit: int4[Vh])
