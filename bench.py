@@ -55,8 +55,18 @@ K1_TRAFFIC_PER_SITE_F32 = 264.33e6 / 221184
 K1_TRAFFIC_PER_SITE_R12 = 332.361728e6 / 331776
 DSLASH_FLOPS = 1146
 METRIC = "time to |r|/|b|<1e-10, mixed vs FP64 CG on 1 B200; Dslash HBM GB/s"
+VARIANTS = ["resident-grid", "full-grid", "tma-pipeline"]
 WORKLOAD = ("asqtad mixed-precision CG 24^3x48 m=0.01 tol 1e-10 (FP32 inner with 12-real Naik links, "
             "FP64 reliable updates)")
+
+
+def bench_config(world, dims=DIMS):
+    """The workload's config object, printed identically by both arms."""
+    return {"workload": WORKLOAD, "lattice": "x".join(map(str, dims)), "mass": MASS, "resid_sq": RESID,
+            "reliable_delta": RU_DELTA, "seeds": {"links": LINK_SEED, "source": SRC_SEED},
+            "parallelism": f"replicas{world}",
+            "l2": "working set (FP32 links 0.64 GB with 12-real Naik links, 0.76 GB with 18; FP64 1.5 GB) exceeds "
+                  "the 126 MB L2"}
 
 
 def peaks():
@@ -280,29 +290,46 @@ def run_gpu(args):
     xsolh = lib.extract_V("D", xh, "even")[: Vh * 6]
     lib.destroy_V("D", xh)
 
-    # end to end through the C ABI with host buffers: create b, x (H2D from
-    # pinned host memory), solve, extract x (D2H), all inside the timed region
+    # end to end through the C ABI with host buffers, as MILC calls it on
+    # every solve: create L from the raw host links (H2D of 4 x 72 reals per
+    # site, the 12-real check and pack happen inside the solve), create b
+    # and x (H2D from pinned host memory), solve, extract x (D2H), destroy.
+    # All of it is inside the timed region.
     pinned_src = torch.from_numpy(src).pin_memory().numpy()
     pinned_zero = torch.zeros(src.shape, dtype=torch.float64).pin_memory().numpy()
     pinned_out = torch.zeros(src.shape, dtype=torch.float64).pin_memory().numpy()
+    pinned_links = {k: torch.from_numpy(links[k]).pin_memory().numpy() for k in ("fat", "lng", "fatback", "lngback")}
     lib.set_inner_precision("single")
     lib.set_link_compression(True)  # as in the timed solves
-    e2e = []
-    for _ in range(max(1, min(args.steps, 3))):
+
+    def e2e_step(with_links):
         barrier(pg)
         t0 = time.perf_counter()
         lib.timer_start()
+        LL = lib.create_L("D", pinned_links) if with_links else L
         bb = lib.create_V("D", pinned_src, "even")
         xx = lib.create_V("D", pinned_zero, "even")
-        it, info, res = lib.invert("D", L, xx, bb, MASS, parity="even", max_iter=MAX_ITER, nrestart=NRESTART,
+        it, info, res = lib.invert("D", LL, xx, bb, MASS, parity="even", max_iter=MAX_ITER, nrestart=NRESTART,
                                    resid=RESID)
         lib.extract_V("D", xx, "even", out=pinned_out)
-        ms_dev = lib.timer_stop()
-        wall = (time.perf_counter() - t0) * 1e3
         lib.destroy_V("D", bb)
         lib.destroy_V("D", xx)
-        e2e.append(max(ms_dev, wall))
+        if with_links:
+            lib.destroy_L("D", LL)
+        ms_dev = lib.timer_stop()
+        wall = (time.perf_counter() - t0) * 1e3
+        assert info.status == 0, lib.last_error()
+        return max(ms_dev, wall), res.final_rsq
+
+    e2e_step(True)  # first upload of this size: pinned staging and pool growth
+    n_e2e = max(1, min(args.steps, 5))
+    e2e_runs = [e2e_step(True) for _ in range(n_e2e)]
+    e2e = [t for t, _ in e2e_runs]
+    e2e_rsq = max(r for _, r in e2e_runs)
     e2e_ms = max_over_ranks(pg, float(np.mean(e2e)))
+    e2e_res = [e2e_step(False)[0] for _ in range(n_e2e)]
+    e2e_res_ms = max_over_ranks(pg, float(np.mean(e2e_res)))
+    link_bytes = 4 * V * 72 * 8
     lib.set_link_compression(False)
 
     # isolated Dslash bandwidth (FP32 and FP64), timed with CUDA events
@@ -320,12 +347,28 @@ def run_gpu(args):
     lib.destroy_V("D", vout)
     lib.destroy_V("D", b)
     lib.destroy_L("D", L)
-    tuning = {name: lib.dslash_variant(name) for name in ("single", "double", "half", "half-links")}
+    tuning = {name: lib.dslash_variant(name) for name in ("single", "single-r12", "double", "half", "half-links")}
+    tuning_k2 = {name: lib.dslash_variant(name, "mdagm")
+                 for name in ("single", "single-r12", "double", "half", "half-links")}
     lib.finalize()
+    # the north-star size in the same run: 32^3x64, HISQ-shaped links,
+    # m = 0.0012 -- FP64 and mixed CG, FP64 and mixed 12-shift multi-shift
+    target = None
+    if not args.no_target:
+        t = multishift_workload(MS_DIMS, 2, {"fp64_cg", "mixed_cg_single", "fp64_multishift",
+                                             "mixed_multishift_single"}, True, False, notes=False)
+        target = {k: t[k] for k in ("workload", "lattice", "mass", "sigmas", "resid_sq", "reliable_delta",
+                                    "fp64_cg", "mixed_cg_single", "fp64_multishift", "mixed_multishift_single")}
+        target["timing"] = ("device time of each solve (CUDA events on the library stream), inputs resident, "
+                            "the second of two solves; true residuals recomputed through the FP64 Dslash")
 
     peak, peak_kind = peaks()
     k1_ms = dslash_ms / max(dslash_n, 1)
     achieved = k1_bytes * Vh / (k1_ms * 1e-3) / 1e9
+    # K2 reads what K1 reads plus p and writes ttt: 24 more bytes per site
+    k2_bytes = k1_bytes + 24
+    k2_ms = mdagm_ms / max(mdagm_n, 1)
+    k2_achieved = k2_bytes * Vh / (k2_ms * 1e-3) / 1e9
     err_vs_fp64 = float(np.abs(xs_last - xsol64).max() / np.abs(xsol64).max())
     err_half = float(np.abs(xsolh - xsol64).max() / np.abs(xsol64).max())
     err_hl = float(np.abs(xsoll - xsol64).max() / np.abs(xsol64).max())
@@ -333,8 +376,7 @@ def run_gpu(args):
         if pg is not None:
             pg.destroy_process_group()
         return
-    cpu = (cpu_baseline_sample(res64.final_iter, links, src)
-           if world == 1 and not args.no_cpu_baseline else None)
+    cpu = cpu_baseline_sample(links, src) if world == 1 and not args.no_cpu_baseline else None
     line = {
         "metric": METRIC,
         "value": ms_step / 1e3,
@@ -348,10 +390,7 @@ def run_gpu(args):
         "vs_baseline": None,
         "dtype": "f32 inner / f64 reliable updates",
         "data": "synthetic (seeded random SU(3) links, Gaussian source)",
-        "config": {"workload": WORKLOAD, "lattice": "24x24x24x48", "mass": MASS, "resid_sq": RESID,
-                   "reliable_delta": RU_DELTA,
-                   "seeds": {"links": LINK_SEED, "source": SRC_SEED}, "parallelism": f"replicas{world}",
-                   "l2": "working set (FP32 links 0.64 GB with 12-real Naik links, 0.76 GB with 18; FP64 1.5 GB) exceeds the 126 MB L2"},
+        "config": bench_config(world),
         "solve": {"ms_each": [round(t, 3) for t in times], "links_compressed": compressed,
                   "iterations": int(np.median(iters)), "reliable_updates": int(np.median(rus)),
                   "true_rsq_rel": float(max(trues)), "err_vs_fp64_solution": err_vs_fp64},
@@ -375,8 +414,10 @@ def run_gpu(args):
                    "f64_us": ms_f64 * 1e3, "f64_gbs": DSLASH_BYTES_F64 * Vh / (ms_f64 * 1e-3) / 1e9,
                    "f32_gflops": DSLASH_FLOPS * Vh / (ms_f32 * 1e-3) / 1e9,
                    "bytes_per_site": {"f32": DSLASH_BYTES_F32, "f64": DSLASH_BYTES_F64},
-                   "autotuner": {k: {"variant": ["resident-grid", "full-grid", "tma-pipeline"][v] if v >= 0 else None,
-                                     "us": [round(x, 2) for x in us]} for k, (v, us) in tuning.items()}},
+                   "autotuner": {k: {"variant": VARIANTS[v] if v >= 0 else None,
+                                     "us": [round(x, 2) for x in us]} for k, (v, us) in tuning.items()},
+                   "autotuner_k2": {k: {"variant": VARIANTS[v] if v >= 0 else None,
+                                        "us": [round(x, 2) for x in us]} for k, (v, us) in tuning_k2.items()}},
         "roofline": {"kernel": ("k_dslash<float, Recon12>" if compressed else "k_dslash<float, float>")
                                + " (K1) in a solve of the timed workload (CUDA events per launch)",
                      "bound": "hbm",
@@ -387,11 +428,25 @@ def run_gpu(args):
                      "traffic": (None if (compressed and K1_TRAFFIC_PER_SITE_R12 is None) else
                                  (K1_TRAFFIC_PER_SITE_R12 if compressed else K1_TRAFFIC_PER_SITE_F32) * Vh),
                      "launches": int(dslash_n), "avg_launch_us": k1_ms * 1e3},
-        "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": 2 * Vh * 6 * 8,
-                "d2h_bytes_per_step": Vh * 6 * 8},
+        "roofline_k2": {"kernel": ("k_dslash_mdagm<float, Recon12>" if compressed else "k_dslash_mdagm<float, float>")
+                                  + " (K2: Dslash + M^dag M epilogue + p.Mp reduction) in a solve of the timed "
+                                    "workload (CUDA events per launch)",
+                        "bound": "hbm", "achieved": k2_achieved, "peak": peak, "unit": "GB/s",
+                        "frac": k2_achieved / peak, "peak_source": peak_kind,
+                        "algorithmic_bytes_per_site": k2_bytes, "launches": int(mdagm_n),
+                        "avg_launch_us": k2_ms * 1e3},
+        "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": link_bytes + 2 * Vh * 6 * 8,
+                "d2h_bytes_per_step": Vh * 6 * 8, "steps": n_e2e, "true_rsq_rel": e2e_rsq,
+                "what": "QPHIX_D3_asqtad_create_L_from_raw (raw FP64 links from pinned host memory), "
+                        "create_V of b and x, invert (mixed, 12-real Naik check and pack included), "
+                        "extract_V, destroy: every step, wall clock and device timer, the larger"},
+        "e2e_links_resident": {"value": e2e_res_ms / 1e3, "unit": "s", "h2d_bytes_per_step": 2 * Vh * 6 * 8,
+                               "d2h_bytes_per_step": Vh * 6 * 8, "steps": n_e2e,
+                               "what": "as e2e with the link handle created once, outside the timed region"},
         "gpu_launches": None,
         "clocks": clk,
         "cpu_baseline": cpu,
+        "target_32x32x32x64": target,
     }
     # our kernel launches per step: 4 per iteration + restart/reliable-update kernels
     line["gpu_launches"] = int(np.median(iters)) * 4 + 8 * int(np.median(rus)) + 8
@@ -401,47 +456,6 @@ def run_gpu(args):
 
 
 # ------------------------------------------------------- reference (CPU) --
-def ref_iteration_sample(links, src, n_iter, dims=DIMS, mass=MASS):
-    """Time n_iter FP64 CG iterations of the reference's own solver
-    (ks_d_congrad_fn.cpp, OpenMP on all host cores) on the full lattice."""
-    import orc
-
-    ref = capi.QphixLib(orc.REF_LIB)
-    ref.init(dims)
-    L = ref.create_L("D", links)
-    b = ref.create_V("D", src, "even")
-    x = ref.create_V("D", np.zeros_like(src), "even")
-    t0 = time.perf_counter()
-    it, info, res = ref.invert("D", L, x, b, mass, parity="even", max_iter=n_iter, nrestart=1, resid=RESID)
-    dt = time.perf_counter() - t0
-    ref.destroy_V("D", b)
-    ref.destroy_V("D", x)
-    ref.destroy_L("D", L)
-    ref.finalize()
-    return dt, res.final_iter
-
-
-def ref_multishift_sample(links, src, n_iter, dims, masses):
-    """Time n_iter FP64 multi-shift iterations of the reference's own solver
-    (ks_multicg_offset.cpp, OpenMP on all host cores) on the full lattice."""
-    import orc
-
-    ref = capi.QphixLib(orc.REF_LIB)
-    ref.init(dims)
-    L = ref.create_L("D", links)
-    b = ref.create_V("D", src, "even")
-    xs = [ref.create_V("D", np.zeros_like(src), "even") for _ in masses]
-    t0 = time.perf_counter()
-    it, info, res = ref.invert_multi("D", L, xs, b, masses, parity="even", max_iter=n_iter, nrestart=1, resid=RESID)
-    dt = time.perf_counter() - t0
-    for x in xs:
-        ref.destroy_V("D", x)
-    ref.destroy_V("D", b)
-    ref.destroy_L("D", L)
-    ref.finalize()
-    return dt, it
-
-
 class _StdoutToStderr:
     """The reference host code prints progress lines to stdout; while it runs
     inside the GPU arm they go to stderr, so stdout carries only the JSON line."""
@@ -459,26 +473,74 @@ class _StdoutToStderr:
         return False
 
 
-def cpu_baseline_sample(full_iters, links=None, src=None, n_iter=12):
-    with _StdoutToStderr():
-        return _cpu_baseline_sample(full_iters, links, src, n_iter)
+class RefSolver:
+    """The reference's own FP64 CG (QPHIX_D3_asqtad_invert of its host code
+    plus the restated per-site kernel, oracle/_ref; OpenMP on all host
+    cores) with the links resident, as the GPU arm's timed solves are."""
+
+    def __init__(self, links, src, dims=DIMS):
+        import orc
+
+        self.ref = capi.QphixLib(orc.REF_LIB)
+        with _StdoutToStderr():
+            assert self.ref.init(dims) == 0
+            self.L = self.ref.create_L("D", links)
+            self.b = self.ref.create_V("D", src, "even")
+        self.src = src
+
+    def solve(self, max_iter=MAX_ITER, nrestart=NRESTART, mass=MASS):
+        """One solve to |r|/|b| < 1e-10 (or max_iter * nrestart iterations):
+        (seconds, iterations, final |r|^2/|b|^2)."""
+        with _StdoutToStderr():
+            x = self.ref.create_V("D", np.zeros_like(self.src), "even")
+            t0 = time.perf_counter()
+            it, info, res = self.ref.invert("D", self.L, x, self.b, mass, parity="even", max_iter=max_iter,
+                                            nrestart=nrestart, resid=RESID)
+            dt = time.perf_counter() - t0
+            self.ref.destroy_V("D", x)
+        return dt, res.final_iter, res.final_rsq
+
+    def close(self):
+        with _StdoutToStderr():
+            self.ref.destroy_V("D", self.b)
+            self.ref.destroy_L("D", self.L)
+            self.ref.finalize()
 
 
-def _cpu_baseline_sample(full_iters, links=None, src=None, n_iter=12):
+def cpu_threads():
+    n = os.environ.get("OMP_NUM_THREADS")
+    return int(n) if n and n.isdigit() else os.cpu_count()
+
+
+def cpu_baseline_sample(links=None, src=None):
+    """One full FP64 CG solve of the reference solver on the benchmark input
+    (measured, 10-30 s on 16 host cores)."""
     import orc
 
     if not os.path.exists(orc.REF_LIB):
         return None
     if links is None:
         links, src = make_inputs(None)
-    dt, done = ref_iteration_sample(links, src, n_iter)
-    per_iter = dt / max(done, 1)
-    return {"value": per_iter * full_iters, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
-            "sample": f"{done} FP64 CG iterations of the reference solver on the full 24^3x48 lattice "
-                      f"({dt:.1f} s), scaled to the {full_iters} iterations the FP64 solve needs"}
+    r = RefSolver(links, src)
+    try:
+        dt, iters, rsq = r.solve()
+    finally:
+        r.close()
+    return {"value": dt, "unit": "s", "cores": cpu_threads(), "kind": "reference",
+            "sample": f"one full FP64 CG solve of the reference solver (its host code + the restated per-site "
+                      f"kernel, OpenMP) on the full 24^3x48 lattice to |r|^2/|b|^2 = {rsq:.2e}: {iters} iterations "
+                      f"in {dt:.1f} s, measured (not scaled)",
+            "iterations": iters, "true_rsq_rel": rsq}
 
 
 def run_reference(args):
+    """--impl reference: the reference's CPU implementation of the path on
+    the host cores.  Every timed step is one full FP64 CG solve of the
+    benchmark input to |r|/|b| < 1e-10 by the reference's own solver
+    (ks_d_congrad_fn.cpp:221-619); warm-up steps are bounded samples of
+    --ref-iters iterations (they only warm the caches and the thread pool).
+    Same metric, unit and config object as the GPU arm; the solver it runs
+    (FP64 CG) is named in "solver"."""
     world, rank, local, pg = dist_setup()
     if rank != 0:
         return
@@ -487,32 +549,32 @@ def run_reference(args):
     if not os.path.exists(orc.REF_LIB):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libqphix_ref.so was not built"}))
         return
-    links, src = make_inputs(None)
-    full_iters = FP64_ITERATIONS
-    samples = []
-    for k in range(args.warmup + args.steps):
-        with _StdoutToStderr():
-            dt, done = ref_iteration_sample(links, src, args.ref_iters)
-        if k >= args.warmup:
-            samples.append(dt / max(done, 1) * full_iters)
-    v = float(np.mean(samples))
-    sample = (f"{args.ref_iters} FP64 CG iterations per step of the reference solver (its host code + restated "
-              f"kernel, OpenMP) on the full 24^3x48 lattice, scaled to the {full_iters} iterations of the "
-              f"FP64 solve")
+    dims = tuple(int(v) for v in args.lattice.split("x")) if args.lattice else DIMS
+    links = synthetic.asqtad_links(dims, seed=LINK_SEED)
+    src = synthetic.gaussian_source(dims, seed=SRC_SEED, parity="even")
+    r = RefSolver(links, src, dims)
+    try:
+        for _ in range(args.warmup):
+            r.solve(max_iter=args.ref_iters, nrestart=1)
+        runs = [r.solve() for _ in range(args.steps)]
+    finally:
+        r.close()
+    v = float(np.mean([t for t, _, _ in runs]))
+    iters = [i for _, i, _ in runs]
+    sample = (f"every step one full FP64 CG solve of the reference solver (its host code + restated kernel, "
+              f"OpenMP on {cpu_threads()} threads) on the full {'x'.join(map(str, dims))} lattice to |r|/|b| < 1e-10: "
+              f"{iters[0]} iterations, measured (not scaled)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random SU(3) links, Gaussian source)",
-        "config": {"workload": WORKLOAD, "lattice": "24x24x24x48", "mass": MASS, "resid_sq": RESID},
-        "cpu_baseline": {"value": v, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
-                         "sample": sample},
+        "config": bench_config(world, dims),
+        "solver": "FP64 CG with the reference's control flow (the reference has no mixed-precision solver)",
+        "solve": {"s_each": [round(t, 3) for t, _, _ in runs], "iterations": iters,
+                  "true_rsq_rel": max(q for _, _, q in runs)},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": cpu_threads(), "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
-
-
-# iterations the FP64 CG (reference control flow) needs on this workload; the
-# GPU arm measures it on every run and reports it as fp64_cg.iterations
-FP64_ITERATIONS = 808
 
 
 def run_reference_dslash(args, dims, links):
@@ -627,29 +689,31 @@ def _true_rel_rsq(lib, L, x_raw, src, mass, V):
     return float(np.dot(r, r) / np.dot(src[e], src[e]))
 
 
-def run_multishift(args):
-    """--mode multishift: the 32^3x64 workload.  Times, on one GPU and on the
-    same input: the FP64 CG (reference control flow), the mixed CG with FP32
-    and with 16-bit-link inner solves, the FP64 multi-shift CG with 12 shifts
-    and the mixed multi-shift CG; checks every solution's FP64 true residual
-    through the FP64 Dslash and its error against the FP64 solution.  Prints
-    one JSON line."""
+def multishift_workload(dims=MS_DIMS, reps=2, which=None, compress=True, cpu_baseline=False, notes=True):
+    """The 32^3x64 workload on one GPU, same input for every solve: the FP64
+    CG (reference control flow), the mixed CG with FP32 and with 16-bit-link
+    inner solves, the FP64 multi-shift CG with 12 shifts and the mixed
+    multi-shift CG.  Every solution's FP64 true residual is recomputed
+    through the FP64 Dslash, and its error against the FP64 solution
+    reported.  `which`: subset of the solve names (None: all); the last of
+    `reps` solves of each kind is reported.  Returns a dict."""
     import torch
 
-    dims = tuple(int(v) for v in args.lattice.split("x")) if args.lattice else MS_DIMS
     V = int(np.prod(dims))
+    Vh = V // 2
     dev = "cuda" if torch.cuda.is_available() else None
     t0 = time.perf_counter()
     links = synthetic.asqtad_links(dims, seed=LINK_SEED, eps_fat=0.2, eps_long=0.3, fat_scale=0.9,
                                    smear=True, device=dev)
     src = synthetic.gaussian_source(dims, seed=SRC_SEED, parity="even")
     gen_s = time.perf_counter() - t0
-    torch.cuda.empty_cache()
+    if dev:
+        torch.cuda.empty_cache()
     masses = np.sqrt(MS_MASS ** 2 + MS_SIGMAS / 4)
     lib = capi.QphixLib(LIB_PATH)
     assert lib.init(dims) == 0, lib.last_error()
     lib.set_reliable_delta(0.2)
-    lib.set_link_compression(not args.no_compress)  # FP32 inner solves with 12-real Naik links
+    lib.set_link_compression(compress)  # FP32 inner solves with 12-real Naik links
     L = lib.create_L("D", links)
     b = lib.create_V("D", src, "even")
     assert L and b, lib.last_error()
@@ -658,14 +722,13 @@ def run_multishift(args):
            "mass": MS_MASS, "sigmas": [float(s) for s in MS_SIGMAS], "resid_sq": RESID,
            "reliable_delta": 0.2,
            "seeds": {"links": LINK_SEED, "source": SRC_SEED}, "field_generation_s": gen_s}
-    which = set(args.solves.split(",")) if args.solves else None
 
     def want(name):
         return which is None or name in which
 
-    def cg(inner, reps):
+    def cg(inner, n):
         lib.set_inner_precision(inner)
-        for k in range(reps):
+        for k in range(n):
             x = lib.create_V("D", zeros, "even")
             lib.timer_start()
             it, info, res = lib.invert("D", L, x, b, MS_MASS, parity="even", max_iter=MAX_ITER,
@@ -677,9 +740,9 @@ def run_multishift(args):
             lib.destroy_V("D", x)
         return ms, st, res, sol
 
-    def multi(inner, reps):
+    def multi(inner, n):
         lib.set_inner_precision(inner)
-        for k in range(reps):
+        for k in range(n):
             xs = [lib.create_V("D", zeros, "even") for _ in masses]
             lib.timer_start()
             it, info, res = lib.invert_multi("D", L, xs, b, masses, parity="even", max_iter=MAX_ITER,
@@ -697,10 +760,10 @@ def run_multishift(args):
         return float(np.abs(a[e] - ref[e]).max() / np.abs(ref[e]).max())
 
     def note(name):
-        print(json.dumps({name: out[name]}), file=sys.stderr, flush=True)
+        if notes:
+            print(json.dumps({name: out[name]}), file=sys.stderr, flush=True)
 
     note("field_generation_s")
-    reps = 1 + max(0, min(args.steps, 2) - 1)  # the last of `reps` solves is reported
     x64 = xs64 = None
     ms64 = ms64m = None
     if want("fp64_cg"):
@@ -726,6 +789,13 @@ def run_multishift(args):
             d["k1_us"] = sti.dslash_ms / max(sti.dslash_launches, 1) * 1e3
             d["k2_us"] = sti.mdagm_ms / max(sti.mdagm_launches, 1) * 1e3
             d["k1_launches"] = sti.dslash_launches
+            k1_bytes = DSLASH_BYTES_R12 if sti.links_compressed == 1 else DSLASH_BYTES_F32
+            peak, kind = peaks()
+            d["k1_gbs"] = k1_bytes * Vh / (d["k1_us"] * 1e-6) / 1e9
+            d["k1_frac"] = d["k1_gbs"] / peak
+            d["k2_gbs"] = (k1_bytes + 24) * Vh / (d["k2_us"] * 1e-6) / 1e9
+            d["k2_frac"] = d["k2_gbs"] / peak
+            d["peak_source"] = kind
         out[f"mixed_cg_{inner}"] = d
         note(f"mixed_cg_{inner}")
     if want("fp64_multishift"):
@@ -750,27 +820,52 @@ def run_multishift(args):
         note(f"mixed_multishift_{inner}")
     lib.destroy_V("D", b)
     lib.destroy_L("D", L)
-    out["autotuner"] = {k: lib.dslash_variant(k) for k in ("single", "double", "half-links")}
+    out["autotuner"] = {k: lib.dslash_variant(k) for k in ("single", "single-r12", "double", "half-links")}
     lib.finalize()
-    if not args.no_cpu_baseline and "fp64_cg" in out:
+    if cpu_baseline and "fp64_cg" in out:
         import orc
 
         if os.path.exists(orc.REF_LIB):
-            with _StdoutToStderr():
-                dt, done = ref_iteration_sample(links, src, 8, dims, MS_MASS)
+            # full FP64 solves of the reference solver on the host cores, measured
+            r = RefSolver(links, src, dims)
+            try:
+                dt, iters, rsq = r.solve(mass=MS_MASS)
+            finally:
+                r.close()
             out["cpu_baseline_fp64_cg"] = {
-                "s": dt / max(done, 1) * out["fp64_cg"]["iterations"], "cores": os.cpu_count(), "kind": "reference",
-                "sample": f"{done} FP64 CG iterations of the reference solver on the full lattice ({dt:.1f} s), "
-                          f"scaled to the {out['fp64_cg']['iterations']} iterations of the FP64 solve"}
+                "s": dt, "iterations": iters, "true_rsq_rel": rsq, "cores": cpu_threads(), "kind": "reference",
+                "sample": "one full FP64 CG solve of the reference solver on the full lattice, measured"}
+            note("cpu_baseline_fp64_cg")
             if "fp64_multishift" in out:
+                ref = capi.QphixLib(orc.REF_LIB)
                 with _StdoutToStderr():
-                    dt, done = ref_multishift_sample(links, src, 6, dims, masses)
-                full = out["fp64_multishift"]["iterations"]
+                    ref.init(dims)
+                    RL = ref.create_L("D", links)
+                    rb = ref.create_V("D", src, "even")
+                    rxs = [ref.create_V("D", np.zeros_like(src), "even") for _ in masses]
+                    t0 = time.perf_counter()
+                    it, info, res = ref.invert_multi("D", RL, rxs, rb, masses, parity="even", max_iter=MAX_ITER,
+                                                     nrestart=NRESTART, resid=RESID)
+                    dt = time.perf_counter() - t0
+                    for x in rxs:
+                        ref.destroy_V("D", x)
+                    ref.destroy_V("D", rb)
+                    ref.destroy_L("D", RL)
+                    ref.finalize()
                 out["cpu_baseline_fp64_multishift"] = {
-                    "s": dt / max(done, 1) * full, "cores": os.cpu_count(), "kind": "reference",
-                    "sample": f"{done} FP64 multi-shift iterations (12 shifts) of the reference solver on the full "
-                              f"lattice ({dt:.1f} s), scaled to the {full} iterations of the FP64 multi-shift"}
-    print(json.dumps(out))
+                    "s": dt, "iterations": it, "cores": cpu_threads(), "kind": "reference",
+                    "sample": "one full FP64 multi-shift solve (12 shifts) of the reference solver on the full "
+                              "lattice, measured"}
+    return out
+
+
+def run_multishift(args):
+    """--mode multishift: multishift_workload on --lattice (default 32^3x64)
+    with every solve and the measured CPU baselines; prints one JSON line."""
+    dims = tuple(int(v) for v in args.lattice.split("x")) if args.lattice else MS_DIMS
+    which = set(args.solves.split(",")) if args.solves else None
+    reps = 1 + max(0, min(args.steps, 2) - 1)
+    print(json.dumps(multishift_workload(dims, reps, which, not args.no_compress, not args.no_cpu_baseline)))
 
 
 BATCH_BIG = (24, 24, 24, 48)
@@ -993,6 +1088,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-target", action="store_true",
+                    help="bench mode: skip the 32^3x64 solves reported beside the headline")
     ap.add_argument("--no-compress", action="store_true",
                     help="multishift mode: 18-real links in the FP32 inner solves")
     ap.add_argument("--compress", action="store_true",

@@ -98,14 +98,68 @@ QPHIX_status_t QPHIX_B200_D3_dslash_timed(void *links, void *out, void *in,
                                           double *ms_per_call);
 
 /* Dslash kernel variant chosen by the library's autotuner for precision p
- * (HALF_LINKS: FP32 vectors with 16-bit links):
+ * (HALF_LINKS: FP32 vectors with 16-bit links; QPHIX_B200_TUNE_F32_R12 /
+ * _R13: FP32 vectors with 12-real / 13-real Naik links):
  * 0 register streaming over a resident grid, 1 register streaming with one
  * thread per site, 2 TMA bulk-copy pipeline.  The first Dslash of each
  * precision and lattice times all three on scratch vectors and keeps the
  * fastest; us[3] receives those timings (microseconds per launch).  Returns
  * -1 before the first Dslash in that precision.  QPHIX_B200_DSLASH=plain|
- * full|tma in the environment forces a variant. */
-int QPHIX_B200_dslash_variant(QPHIX_B200_precision_t p, double us[3]);
+ * full|tma in the environment forces a variant.  QPHIX_B200_mdagm_variant
+ * reports the same for the fused Dslash + M^dag M kernel of the solvers,
+ * which is tuned on its own.  With QPHIX_B200_TUNECACHE=<file> in the
+ * environment the choices are kept in that file (one line per lattice
+ * volume, precision and link storage, tagged with the GPU model) and later
+ * processes read them instead of timing again. */
+#define QPHIX_B200_TUNE_F32_R12 4
+#define QPHIX_B200_TUNE_F32_R13 5
+int QPHIX_B200_dslash_variant(int p, double us[3]);
+int QPHIX_B200_mdagm_variant(int p, double us[3]);
+
+/* Forces the Dslash variant of every precision (0, 1 or 2 as above) or,
+ * with -1 (the default), lets the autotuner choose.  Same effect as
+ * QPHIX_B200_DSLASH=plain|full|tma, which sets the value at load. */
+QPHIX_status_t QPHIX_B200_set_dslash_variant(int variant);
+
+/* Poll limit of the bounded mbarrier waits of the TMA-pipeline Dslash
+ * (variant 2).  A wait that reaches the limit stops the kernel, which lets
+ * the copies it issued land, records the failure in a device error word and
+ * returns; the call then reports QPHIX_FAIL and QPHIX_B200_last_error says
+ * so.  polls < 0 restores the default (2^22 polls, far longer than any copy
+ * takes); 0 gives up at the first wait, which exercises the failure path. */
+QPHIX_status_t QPHIX_B200_set_wait_limit(long polls);
+
+/* ---- Operators of the inner solves (no counterpart in the reference) ------
+ * The mixed-precision solvers apply the Dslash with lower-precision copies
+ * of the links and vectors.  These entry points apply exactly those
+ * kernels to FP64 handles, so the inner operators can be compared with
+ * the FP64 one element by element:
+ *   in[1-parity] is rounded to the storage's vector format, the operator
+ *   runs on the storage's link copy, and the result is widened to FP64.
+ * QPHIX_B200_STORE_F32_R12 / _R13 need Naik links of that form (see
+ * QPHIX_B200_set_link_compression); QPHIX_FAIL otherwise. */
+typedef enum {
+  QPHIX_B200_STORE_F32 = 0,         /* FP32 vectors, 18-real FP32 links */
+  QPHIX_B200_STORE_F32_R12 = 1,     /* FP32 vectors, 12-real Naik links */
+  QPHIX_B200_STORE_F32_R13 = 2,     /* FP32 vectors, 13-real Naik links */
+  QPHIX_B200_STORE_HALF_LINKS = 3,  /* FP32 vectors, 16-bit fixed-point links */
+  QPHIX_B200_STORE_HALF = 4         /* 16-bit vectors (per-site norm) and links */
+} QPHIX_B200_storage_t;
+
+/* out[parity] = D in[1-parity] with the inner kernel of `storage`
+ * (QPHIX_D3_asqtad_dslash's operator, qphix_f3.cpp:1233-1245). */
+QPHIX_status_t QPHIX_B200_D3_asqtad_dslash_inner(QPHIX_D3_FermionLinksAsqtad *L, QPHIX_D3_ColorVector *out,
+                                                 QPHIX_D3_ColorVector *in, QPHIX_evenodd_t parity,
+                                                 QPHIX_B200_storage_t storage);
+/* out[parity] = D D in[parity] - 4 mass^2 in[parity] through the inner
+ * solve's two kernels (the plain Dslash, then the fused Dslash with the
+ * M^dag M epilogue), *in_dot_out = in . out reduced on the device: the
+ * vector and the scalar calc_pkp forms in the reference CG
+ * (ks_d_congrad_fn.cpp:159-171). */
+QPHIX_status_t QPHIX_B200_D3_asqtad_mdagm_inner(QPHIX_D3_FermionLinksAsqtad *L, QPHIX_D3_ColorVector *out,
+                                                QPHIX_D3_ColorVector *in, QPHIX_D_Real mass,
+                                                QPHIX_evenodd_t parity, QPHIX_B200_storage_t storage,
+                                                double *in_dot_out);
 
 /* Allocation-free application of the CG operator (no counterpart in the
  * reference).  For callers that cannot allocate GPU memory at the point of
@@ -154,6 +208,21 @@ void QPHIX_B200_D3_batch_destroy_L(QPHIX_B200_Batch *B);
 int QPHIX_B200_D3_batch_invert(QPHIX_info_t *info, QPHIX_B200_Batch *B, QPHIX_invert_arg_t *inv_arg,
                                QPHIX_resid_arg_t **res_arg, int nsys, const int *lat,
                                const double *mass, double *const *out, double *const *in);
+
+/* Applies the batched solver's Dslash kernels to nsys systems in one launch
+ * (the operators QPHIX_B200_D3_batch_invert runs), system k on lattice
+ * lat[k] of the batch, raw MILC vectors in and out (6 reals per site, even
+ * sites first, both parities in the arrays):
+ *   op 0: out_k[parity] = D in_k[1-parity]
+ *   op 1: out_k[parity] = 4 mass[k]^2 in_k[parity] - D D in_k[parity]
+ *         (the inner CG's M p; FP32 only)
+ * prec QPHIX_B200_PREC_SINGLE runs the FP32 inner kernels on the batch's
+ * FP32 links with `rhs_per_thread` = 4, 2 or 1 systems per thread (0: 4);
+ * QPHIX_B200_PREC_DOUBLE the FP64 reliable-update kernel.  The parity of
+ * out_k that the operator does not write is left as it was. */
+QPHIX_status_t QPHIX_B200_D3_batch_dslash(QPHIX_B200_Batch *B, int nsys, const int *lat, const double *mass,
+                                          QPHIX_evenodd_t parity, int op, QPHIX_B200_precision_t prec,
+                                          int rhs_per_thread, double *const *out, double *const *in);
 
 /* ---- Fermion force (no counterpart in the reference) -----------------------
  * Gradient of S = sum_k coef[k] phi_k^dag (4 m_k^2 - D_pq D_qp)^{-1} phi_k

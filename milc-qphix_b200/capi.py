@@ -85,6 +85,11 @@ class Stats(C.Structure):
 
 
 PRECISION = {"half": 0, "single": 1, "double": 2, "half-links": 3}
+# QPHIX_B200_dslash_variant precision codes: PRECISION plus FP32 vectors with
+# 12-real / 13-real Naik links
+TUNE_CODE = dict(PRECISION, **{"single-r12": 4, "single-r13": 5})
+# QPHIX_B200_storage_t: vector and link format of an inner-solve operator
+STORAGE = {"single": 0, "single-r12": 1, "single-r13": 2, "half-links": 3, "half": 4}
 
 
 class QphixLib:
@@ -141,6 +146,20 @@ class QphixLib:
                                                              C.c_int, C.POINTER(C.c_double)]
             L.QPHIX_B200_dslash_variant.restype = C.c_int
             L.QPHIX_B200_dslash_variant.argtypes = [C.c_int, C.POINTER(C.c_double)]
+            L.QPHIX_B200_mdagm_variant.restype = C.c_int
+            L.QPHIX_B200_mdagm_variant.argtypes = [C.c_int, C.POINTER(C.c_double)]
+            L.QPHIX_B200_set_dslash_variant.argtypes = [C.c_int]
+            L.QPHIX_B200_set_wait_limit.argtypes = [C.c_long]
+            L.QPHIX_B200_D3_asqtad_dslash_inner.restype = C.c_int
+            L.QPHIX_B200_D3_asqtad_dslash_inner.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+            L.QPHIX_B200_D3_asqtad_mdagm_inner.restype = C.c_int
+            L.QPHIX_B200_D3_asqtad_mdagm_inner.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                                           C.c_int, C.c_int, C.POINTER(C.c_double)]
+            L.QPHIX_B200_D3_batch_dslash.restype = C.c_int
+            L.QPHIX_B200_D3_batch_dslash.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                                     C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int,
+                                                     C.POINTER(C.POINTER(C.c_double)),
+                                                     C.POINTER(C.POINTER(C.c_double))]
             dpp = C.POINTER(C.POINTER(C.c_double))
             L.QPHIX_B200_D3_batch_create_L.restype = C.c_void_p
             L.QPHIX_B200_D3_batch_create_L.argtypes = [C.c_int, C.POINTER(C.c_int), dpp, dpp, dpp, dpp]
@@ -262,10 +281,47 @@ class QphixLib:
         rc = self.lib.QPHIX_B200_D3_asqtad_mdagm_noalloc(L, out, inp, mass, PARITY[parity], C.byref(dot))
         return rc, dot.value
 
-    def dslash_variant(self, prec_name):
+    def dslash_variant(self, prec_name, kernel="dslash"):
+        """(variant, [us per variant]) the autotuner chose for the Dslash
+        (kernel='dslash') or the fused M^dag M kernel (kernel='mdagm');
+        prec_name: a PRECISION name, 'single-r12' or 'single-r13'."""
         us = (C.c_double * 3)()
-        v = self.lib.QPHIX_B200_dslash_variant(PRECISION[prec_name], us)
+        f = self.lib.QPHIX_B200_dslash_variant if kernel == "dslash" else self.lib.QPHIX_B200_mdagm_variant
+        v = f(TUNE_CODE[prec_name], us)
         return v, list(us)
+
+    def set_dslash_variant(self, variant):
+        """Force Dslash variant 0, 1 or 2 everywhere; -1 returns to the autotuner."""
+        return self.lib.QPHIX_B200_set_dslash_variant(int(variant))
+
+    def set_wait_limit(self, polls):
+        """Poll limit of the TMA pipeline's bounded waits (< 0: the default)."""
+        return self.lib.QPHIX_B200_set_wait_limit(int(polls))
+
+    def dslash_inner(self, L, out, inp, parity, storage):
+        """QPHIX_B200_D3_asqtad_dslash_inner: the inner solve's Dslash for
+        ``storage`` (a STORAGE name) on FP64 handles; returns the status."""
+        return self.lib.QPHIX_B200_D3_asqtad_dslash_inner(L, out, inp, PARITY[parity], STORAGE[storage])
+
+    def mdagm_inner(self, L, out, inp, mass, parity, storage):
+        """QPHIX_B200_D3_asqtad_mdagm_inner: (status, in . out)."""
+        dot = C.c_double()
+        rc = self.lib.QPHIX_B200_D3_asqtad_mdagm_inner(L, out, inp, mass, PARITY[parity], STORAGE[storage],
+                                                      C.byref(dot))
+        return rc, dot.value
+
+    def batch_dslash(self, B, systems, parity="even", op=0, prec="single", rhs_per_thread=0):
+        """QPHIX_B200_D3_batch_dslash.  ``systems``: list of (lattice index,
+        mass, raw input vector).  Returns (status, [raw outputs])."""
+        n = len(systems)
+        lat = (C.c_int * n)(*[int(s[0]) for s in systems])
+        mass = (C.c_double * n)(*[float(s[1]) for s in systems])
+        pin, keep = self._dptrs([s[2] for s in systems])
+        outs = [np.zeros_like(k) for k in keep]
+        pout = (C.POINTER(C.c_double) * n)(*[o.ctypes.data_as(C.POINTER(C.c_double)) for o in outs])
+        rc = self.lib.QPHIX_B200_D3_batch_dslash(B, n, lat, mass, PARITY[parity], int(op), PRECISION[prec],
+                                                 int(rhs_per_thread), pout, pin)
+        return rc, outs
 
     def neighbor_index(self, dims, cb, site, k):
         Ld = (C.c_int * 4)(*dims)

@@ -6,9 +6,11 @@
 // QPHIX_FAIL (through the return value or info->status), or NULL from a
 // create call, and records a message for QPHIX_B200_last_error().  Nothing
 // exits, aborts or traps.
+#include <climits>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "context.h"
 #include "device_common.cuh"
@@ -372,6 +374,124 @@ SloppyCfg sloppy_cfg(QPHIX_D3_FermionLinksAsqtad *H, int mode)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Inner-solve operators on FP64 handles (QPHIX_B200_D3_*_inner)
+// ---------------------------------------------------------------------------
+// vector precision and link copy of an inner-operator storage; a compressed
+// copy of a form the solver has not cached is made for the call only
+struct InnerOp {
+    Prec vec = Prec::Single;
+    const LinkSet *links = nullptr;
+    LinkSet temp;
+    std::vector<VecBlock> vecs;
+    InnerOp() = default;
+    InnerOp(const InnerOp &) = delete;
+    InnerOp &operator=(const InnerOp &) = delete;
+    ~InnerOp()
+    {
+        for (auto &v : vecs) free_vec(v);
+        if (temp.valid) free_links(temp);
+    }
+    VecBlock vec_tmp()
+    {
+        vecs.push_back(alloc_vec(vec));
+        return vecs.back();
+    }
+};
+
+void inner_setup(QPHIX_D3_FermionLinksAsqtad *H, int storage, InnerOp &op)
+{
+    Context &c = ctx();
+    switch (storage) {
+    case QPHIX_B200_STORE_F32:
+        op.vec = Prec::Single;
+        op.links = &single_links(H);
+        break;
+    case QPHIX_B200_STORE_F32_R12:
+    case QPHIX_B200_STORE_F32_R13: {
+        const int want = storage == QPHIX_B200_STORE_F32_R12 ? 1 : 2;
+        op.vec = Prec::Single;
+        if (H->recon_checked && H->sloppy_recon.valid && H->sloppy_recon.recon == want) {
+            op.links = &H->sloppy_recon;  // the copy the solvers use
+        } else {
+            double dev[5];
+            if (links_compress(op.temp, H->links, c.launch(), dev, want) != want)
+                throw Error(std::string("inner operator: the Naik links do not have the ") +
+                            (want == 1 ? "12-real" : "13-real") + " form");
+            op.links = &op.temp;
+        }
+        break;
+    }
+    case QPHIX_B200_STORE_HALF_LINKS:
+        op.vec = Prec::Single;
+        op.links = &half_links(H);
+        break;
+    case QPHIX_B200_STORE_HALF:
+        op.vec = Prec::Half;
+        op.links = &half_links(H);
+        break;
+    default: throw Error("inner operator: unknown storage");
+    }
+}
+
+QPHIX_status_t dslash_inner(QPHIX_D3_FermionLinksAsqtad *H, QPHIX_D3_ColorVector *out, QPHIX_D3_ColorVector *in,
+                            QPHIX_evenodd_t parity, int storage)
+{
+    return guarded([&] {
+        require_init();
+        Context &c = ctx();
+        if (!H || !out || !in) throw Error("asqtad_dslash_inner: NULL argument");
+        if (parity != QPHIX_EVEN && parity != QPHIX_ODD)
+            throw Error("asqtad_dslash_inner: parity must be EVEN or ODD");
+        const int cb = parity == QPHIX_EVEN ? 0 : 1;
+        if (!out->blk[cb].data || !in->blk[1 - cb].data)
+            throw Error("asqtad_dslash_inner: vectors lack the parities the operator needs");
+        InnerOp op;
+        inner_setup(H, storage, op);
+        const Launch L = c.launch();
+        VecBlock tin = op.vec_tmp(), tout = op.vec_tmp();
+        vec_copy(op.vec, tin, Prec::Double, in->blk[1 - cb], L);
+        dslash(op.vec, L, tout, tin, *op.links, cb);
+        vec_copy(Prec::Double, out->blk[cb], op.vec, tout, L);
+        sync_check();
+        QB_CUDA(cudaGetLastError());
+    });
+}
+
+QPHIX_status_t mdagm_inner(QPHIX_D3_FermionLinksAsqtad *H, QPHIX_D3_ColorVector *out, QPHIX_D3_ColorVector *in,
+                           double mass, QPHIX_evenodd_t parity, int storage, double *in_dot_out)
+{
+    return guarded([&] {
+        require_init();
+        Context &c = ctx();
+        if (!H || !out || !in) throw Error("asqtad_mdagm_inner: NULL argument");
+        if (parity != QPHIX_EVEN && parity != QPHIX_ODD)
+            throw Error("asqtad_mdagm_inner: parity must be EVEN or ODD");
+        const int cb = parity == QPHIX_EVEN ? 0 : 1;
+        if (!out->blk[cb].data || !in->blk[cb].data)
+            throw Error("asqtad_mdagm_inner: in and out must hold the requested parity");
+        InnerOp op;
+        inner_setup(H, storage, op);
+        const Launch L = c.launch();
+        VecBlock p = op.vec_tmp(), tmp = op.vec_tmp(), ttt = op.vec_tmp();
+        vec_copy(op.vec, p, Prec::Double, in->blk[cb], L);
+        // the inner CG's K1 and K2: tmp = D p; ttt = D tmp - 4 m^2 p, p.ttt
+        SolverState &S = *c.h_state;
+        S.counter = S.counter2 = 0;
+        S.stop_at = INT_MAX;
+        S.iteration = 0;
+        S.rsq = 1.0;
+        S.prec_single = 0;
+        upload_state();
+        dslash_gated(op.vec, L, tmp, p, *op.links, 1 - cb, c.d_state, -1);
+        dslash_mdagm_dot(op.vec, L, ttt, tmp, *op.links, p, -4.0 * mass * mass, cb, c.d_state, c.d_partials, -1, 0);
+        vec_copy(Prec::Double, out->blk[cb], op.vec, ttt, L);
+        download_state();
+        if (in_dot_out) *in_dot_out = S.pkp;
+        QB_CUDA(cudaGetLastError());
+    });
+}
+
 template <typename Real>
 int asqtad_invert(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_invert_arg_t *inv, QPHIX_resid_arg_t *res,
                   Real mass, typename Api<Real>::CV *out, typename Api<Real>::CV *in)
@@ -490,6 +610,28 @@ QPHIX_status_t dslash_timed(void *links, void *out, void *in, QPHIX_evenodd_t pa
         *ms = t / reps;
         QB_CUDA(cudaGetLastError());
     });
+}
+
+// autotuner report of kernel 0 (Dslash) / 1 (fused M^dag M) for the
+// precision codes of QPHIX_B200_dslash_variant
+int variant_report(int kernel, int p, double us[3])
+{
+    Prec pv;
+    int slot;
+    switch (p) {
+    case QPHIX_B200_PREC_HALF: pv = Prec::Half; slot = (int)Prec::Half; break;
+    case QPHIX_B200_PREC_SINGLE: pv = Prec::Single; slot = (int)Prec::Single; break;
+    case QPHIX_B200_PREC_DOUBLE: pv = Prec::Double; slot = (int)Prec::Double; break;
+    case QPHIX_B200_PREC_HALF_LINKS: pv = Prec::Single; slot = (int)Prec::Half; break;
+    case QPHIX_B200_TUNE_F32_R12: pv = Prec::Single; slot = 3; break;
+    case QPHIX_B200_TUNE_F32_R13: pv = Prec::Single; slot = 4; break;
+    default: return -1;
+    }
+    float t[3] = {0, 0, 0};
+    const int v = dslash_variant(kernel, pv, slot, t);
+    if (us)
+        for (int i = 0; i < 3; ++i) us[i] = t[i];
+    return v;
 }
 
 void not_on_path(QPHIX_info_t *info, const char *what)
@@ -677,22 +819,22 @@ long QPHIX_B200_neighbor_index(const int L[4], int cb, long site, int k)
     const SiteCoords s = decode(g, cb, (int)site);
     return neighbor(g, s, k);
 }
-int QPHIX_B200_dslash_variant(QPHIX_B200_precision_t p, double us[3])
+QPHIX_status_t QPHIX_B200_D3_asqtad_dslash_inner(QPHIX_D3_FermionLinksAsqtad *L, QPHIX_D3_ColorVector *out,
+                                                 QPHIX_D3_ColorVector *in, QPHIX_evenodd_t parity,
+                                                 QPHIX_B200_storage_t storage)
 {
-    Prec pv, pl;
-    switch (p) {
-    case QPHIX_B200_PREC_HALF: pv = pl = Prec::Half; break;
-    case QPHIX_B200_PREC_SINGLE: pv = pl = Prec::Single; break;
-    case QPHIX_B200_PREC_DOUBLE: pv = pl = Prec::Double; break;
-    case QPHIX_B200_PREC_HALF_LINKS: pv = Prec::Single; pl = Prec::Half; break;
-    default: return -1;
-    }
-    float t[3] = {0, 0, 0};
-    const int v = dslash_variant(pv, pl, t);
-    if (us)
-        for (int i = 0; i < 3; ++i) us[i] = t[i];
-    return v;
+    return dslash_inner(L, out, in, parity, (int)storage);
 }
+QPHIX_status_t QPHIX_B200_D3_asqtad_mdagm_inner(QPHIX_D3_FermionLinksAsqtad *L, QPHIX_D3_ColorVector *out,
+                                                QPHIX_D3_ColorVector *in, QPHIX_D_Real mass, QPHIX_evenodd_t parity,
+                                                QPHIX_B200_storage_t storage, double *in_dot_out)
+{
+    return mdagm_inner(L, out, in, mass, parity, (int)storage, in_dot_out);
+}
+int QPHIX_B200_dslash_variant(int p, double us[3]) { return variant_report(0, p, us); }
+int QPHIX_B200_mdagm_variant(int p, double us[3]) { return variant_report(1, p, us); }
+QPHIX_status_t QPHIX_B200_set_dslash_variant(int variant) { return guarded([&] { set_forced_variant(variant); }); }
+QPHIX_status_t QPHIX_B200_set_wait_limit(long polls) { return guarded([&] { set_wait_limit(polls); }); }
 
 const char *QPHIX_B200_last_error(void) { return ctx().last_error.c_str(); }
 int QPHIX_B200_version(void) { return 100; }

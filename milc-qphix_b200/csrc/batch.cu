@@ -512,6 +512,12 @@ __global__ void __launch_bounds__(kBlock, GMAX == 1 ? 4 : (GMAX == 2 ? 3 : 2)) k
                 if (!y.active) return;
                 y.pkp = t[0];
                 y.a = t[0] > 0.0 ? y.rsq / t[0] : 0.0;
+                // p.(M p) <= 0 or not finite: breakdown of system k (M is
+                // positive definite for m > 0); the whole batch stops
+                if (!(t[0] > 0.0) || !isfinite(t[0])) {
+                    st->nonfinite = isfinite(t[0]) ? 2 : 1;
+                    st->stop = 1;
+                }
             },
             [&] {});
     }
@@ -715,11 +721,12 @@ __global__ void __launch_bounds__(kBlock) k_bvec(const BTable *tab, BState *st, 
                     y.rsqstop = y.resid * t[0];
                     y.active = t[0] > 0.0;
                     y.flag = y.active;
+                    if (!isfinite(t[0])) st->nonfinite = 1;  // a source with NaN or Inf
                 },
                 [&] {
                     b_masks(st);
                     st->any_flag = st->flag_mask != 0;
-                    st->stop = st->active_mask == 0;
+                    st->stop = st->active_mask == 0 || st->nonfinite;
                 });
         } else {
             b_finish<1>(
@@ -732,13 +739,14 @@ __global__ void __launch_bounds__(kBlock) k_bvec(const BTable *tab, BState *st, 
                     y.b = y.rsq_old > 0.0 ? t[0] / y.rsq_old : 0.0;
                     y.iterations += 1;
                     y.flag = (t[0] < st->delta2 * y.rsq_ru || t[0] <= y.rsqstop || !(t[0] == t[0])) ? 1 : 0;
+                    if (!isfinite(t[0])) st->nonfinite = 1;
                 },
                 [&] {
                     b_masks(st);
                     st->any_flag = st->flag_mask != 0;
                     st->iteration += 1;
                     if (st->use_cond) cudaGraphSetConditional(st->cond_ru, st->any_flag ? 1u : 0u);
-                    if (st->iteration >= st->iter_cap) st->stop = 1;
+                    if (st->iteration >= st->iter_cap || st->nonfinite) st->stop = 1;
                 });
         }
     } else if constexpr (OP == kBAxpyRu) {
@@ -780,6 +788,18 @@ __global__ void k_b_to_raw(double *raw, const double2 *f, long long voff, int vh
 }
 
 }  // namespace qb
+
+// FP64 <-> FP32 copy of a whole batched field (n complex numbers)
+__global__ void k_b_narrow(float2 *dst, const double2 *src, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = make_float2((float)src[i].x, (float)src[i].y);
+}
+__global__ void k_b_widen(double2 *dst, const float2 *src, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = make_double2((double)src[i].x, (double)src[i].y);
+}
 
 // ------------------------------------------------------------------ host --
 struct QPHIX_B200_Batch_struct {
@@ -1223,7 +1243,8 @@ void run_batch(const std::vector<LatRef> &lats, const std::vector<SegPlan> &plan
             download(h, d_st, c.stream);
         }
     }
-    if (h->nonfinite) throw Error("batch: non-finite residual");
+    if (h->nonfinite == 2) throw Error("batch_invert: CG breakdown (p.Ap <= 0) in a system");
+    if (h->nonfinite) throw Error("batch_invert: non-finite source or residual in a system");
     store(f, tabs[2], h, mem);
     sync_check();
     c.stats = Stats{};
@@ -1366,6 +1387,115 @@ static int batch_invert(QPHIX_info_t *info, QPHIX_B200_Batch *B, QPHIX_invert_ar
     return max_iter;
 }
 
+// The batched solver's Dslash kernels on caller vectors, one launch each
+// (QPHIX_B200_D3_batch_dslash): op 0 out = D in, op 1 out = m4 in - D D in
+// (FP32 only); prec 1 FP32 kernels with g systems per thread, 2 the FP64
+// kernel of the reliable update.
+static void batch_dslash(QPHIX_B200_Batch *B, int nsys, const int *lat, const double *mass, QPHIX_evenodd_t parity,
+                         int op, int prec, int g, double *const *out, double *const *in)
+{
+    Context &c = ctx();
+    if (!c.initialized) throw Error("batch_dslash: QPhiX library used before QPHIX_init");
+    if (!B || !lat || !out || !in || (op == 1 && !mass)) throw Error("batch_dslash: NULL argument");
+    if (nsys < 1 || nsys > kBMaxSys) throw Error("batch_dslash: nsys must be 1.." + std::to_string(kBMaxSys));
+    if (parity != QPHIX_EVEN && parity != QPHIX_ODD) throw Error("batch_dslash: parity must be EVEN or ODD");
+    if (op != 0 && op != 1) throw Error("batch_dslash: op must be 0 (D) or 1 (4m^2 - D D)");
+    if (prec != QPHIX_B200_PREC_SINGLE && prec != QPHIX_B200_PREC_DOUBLE)
+        throw Error("batch_dslash: prec must be QPHIX_B200_PREC_SINGLE or _DOUBLE");
+    if (prec == QPHIX_B200_PREC_DOUBLE && op != 0) throw Error("batch_dslash: the FP64 batched kernel applies D only");
+    if (g == 0) g = 4;
+    if (g != 1 && g != 2 && g != 4) throw Error("batch_dslash: rhs_per_thread must be 0, 1, 2 or 4");
+    for (int k = 0; k < nsys; ++k) {
+        if (lat[k] < 0 || lat[k] >= (int)B->lats.size()) throw Error("batch_dslash: lattice index out of range");
+        if (!out[k] || !in[k]) throw Error("batch_dslash: NULL system vector");
+    }
+    const int cb = parity == QPHIX_EVEN ? 0 : 1;
+    const int in_cb = op == 0 ? 1 - cb : cb;
+    std::vector<int> slot_of;
+    const std::vector<SegPlan> plan = plan_segments((int)B->lats.size(), nsys, lat, slot_of);
+    std::vector<LatRef> lats;
+    for (const auto &L : B->lats) lats.push_back(LatRef{&L.g, &L.l64, &L.l32});
+    const bool dbl = prec == QPHIX_B200_PREC_DOUBLE;
+    const BTable tab = make_table(plan, lats, dbl ? 1 : 0, g);
+    const BTable vt = make_table(plan, lats, 2);
+    long long ncx = 0;
+    for (const auto &p : plan) ncx += 3LL * lats[p.lat].g->vh * p.nrhs;
+
+    BatchMem mem;
+    BTable *d_tab = static_cast<BTable *>(mem.get(sizeof(BTable)));
+    BState *d_st = static_cast<BState *>(mem.get(sizeof(BState)));
+    double2 *in64 = static_cast<double2 *>(mem.get((size_t)ncx * 16));
+    double2 *out64 = static_cast<double2 *>(mem.get((size_t)ncx * 16));
+    QB_CUDA(cudaMemsetAsync(in64, 0, (size_t)ncx * 16, c.stream));
+    QB_CUDA(cudaMemsetAsync(out64, 0, (size_t)ncx * 16, c.stream));
+    QB_CUDA(cudaMemcpyAsync(d_tab, &tab, sizeof(BTable), cudaMemcpyHostToDevice, c.stream));
+    for (size_t s = 0; s < plan.size(); ++s) {
+        const SegPlan &p = plan[s];
+        const Geom &gm = *lats[p.lat].g;
+        const size_t n = (size_t)6 * gm.vh;
+        double *stage = static_cast<double *>(mem.get(sizeof(double) * n));
+        for (int r = 0; r < p.nrhs; ++r) {
+            QB_CUDA(cudaMemcpyAsync(stage, in[p.user[r]] + in_cb * n, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                    c.stream));
+            k_b_from_raw<<<grid_for(gm.vh), kBlock, 0, c.stream>>>(in64, vt.seg[s].voff, gm.vh, p.nrhs, r, stage);
+        }
+    }
+    BState *h = pinned_state();
+    std::memset(h, 0, sizeof(BState));
+    h->nsys = nsys;
+    h->active_mask = h->flag_mask = nsys >= 64 ? ~0ull : ((1ull << nsys) - 1ull);
+    h->any_flag = 1;
+    for (int k = 0; k < nsys; ++k) {
+        h->sys[slot_of[k]].m4 = op == 1 ? 4.0 * mass[k] * mass[k] : 0.0;
+        h->sys[slot_of[k]].active = 1;
+        h->sys[slot_of[k]].flag = 1;
+    }
+    upload(d_st, h, c.stream);
+    auto grid = [&](int res_blocks) { return std::max(1, std::min(res_blocks, tab.ntiles)); };
+    double *partials = static_cast<double *>(mem.get(sizeof(double) * kBMaxSys * tab.ntiles));
+    const unsigned nb = (unsigned)((ncx + kBlock - 1) / kBlock);
+    if (dbl) {
+        k_bdslash_d<false><<<grid(resident_blocks(k_bdslash_d<false>)), kBlock, 0, c.stream>>>(
+            d_tab, d_st, out64, in64, BFields{}, cb, partials);
+    } else {
+        float2 *in32 = static_cast<float2 *>(mem.get((size_t)ncx * 8));
+        float2 *t32 = static_cast<float2 *>(mem.get((size_t)ncx * 8));
+        float2 *out32 = static_cast<float2 *>(mem.get((size_t)ncx * 8));
+        QB_CUDA(cudaMemsetAsync(t32, 0, (size_t)ncx * 8, c.stream));
+        QB_CUDA(cudaMemsetAsync(out32, 0, (size_t)ncx * 8, c.stream));
+        k_b_narrow<<<nb, kBlock, 0, c.stream>>>(in32, in64, ncx);
+        int gmax = 1;
+        for (int k = 0; k < tab.nseg; ++k) gmax = std::max(gmax, tab.seg[k].G);
+        auto run = [&](auto k0, auto k1) {
+            if (op == 0) {
+                k0<<<grid(resident_blocks(k0)), kBlock, 0, c.stream>>>(d_tab, d_st, out32, in32, in32, cb, partials);
+            } else {
+                k0<<<grid(resident_blocks(k0)), kBlock, 0, c.stream>>>(d_tab, d_st, t32, in32, in32, 1 - cb,
+                                                                        partials);
+                k1<<<grid(resident_blocks(k1)), kBlock, 0, c.stream>>>(d_tab, d_st, out32, t32, in32, cb, partials);
+            }
+        };
+        if (gmax > 2) run(k_bdslash_s<false, 4>, k_bdslash_s<true, 4>);
+        else if (gmax == 2) run(k_bdslash_s<false, 2>, k_bdslash_s<true, 2>);
+        else run(k_bdslash_s<false, 1>, k_bdslash_s<true, 1>);
+        k_b_widen<<<nb, kBlock, 0, c.stream>>>(out64, out32, ncx);
+    }
+    QB_CUDA(cudaGetLastError());
+    for (size_t s = 0; s < plan.size(); ++s) {
+        const SegPlan &p = plan[s];
+        const Geom &gm = *lats[p.lat].g;
+        const size_t n = (size_t)6 * gm.vh;
+        double *stage = static_cast<double *>(mem.get(sizeof(double) * n));
+        for (int r = 0; r < p.nrhs; ++r) {
+            k_b_to_raw<<<grid_for(gm.vh), kBlock, 0, c.stream>>>(stage, out64, vt.seg[s].voff, gm.vh, p.nrhs, r);
+            QB_CUDA(cudaMemcpyAsync(out[p.user[r]] + cb * n, stage, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                    c.stream));
+            sync_check();
+        }
+    }
+    sync_check();
+}
+
 }  // namespace qb
 
 // ------------------------------------------------------------- C ABI --
@@ -1412,6 +1542,14 @@ int QPHIX_B200_D3_batch_invert(QPHIX_info_t *info, QPHIX_B200_Batch *B, QPHIX_in
         batch_guarded([&] { it = qb::batch_invert(info, B, inv_arg, res_arg, nsys, lat, mass, out, in); });
     if (s != QPHIX_SUCCESS && info) info->status = s;
     return it;
+}
+
+QPHIX_status_t QPHIX_B200_D3_batch_dslash(QPHIX_B200_Batch *B, int nsys, const int *lat, const double *mass,
+                                          QPHIX_evenodd_t parity, int op, QPHIX_B200_precision_t prec,
+                                          int rhs_per_thread, double *const *out, double *const *in)
+{
+    return batch_guarded(
+        [&] { qb::batch_dslash(B, nsys, lat, mass, parity, op, (int)prec, rhs_per_thread, out, in); });
 }
 
 }  // extern "C"

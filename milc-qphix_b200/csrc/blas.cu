@@ -139,7 +139,8 @@ k_cg_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverSta
         st->b = round_to(round_to(rsq, single) / oldrsq, single);
         const bool conv = (st->rsqmin <= 0 || st->rsqmin > st->size_r) &&
                           (st->relrsqmin <= 0 || st->relrsqmin > st->size_relr);
-        if ((st->iteration % st->niter == 0) || conv || run_guard(st)) stop_run(st, gate);
+        if (!isfinite(rsq) && !st->error) st->error = 1;  // non-finite residual: breakdown
+        if ((st->iteration % st->niter == 0) || conv || st->error || run_guard(st)) stop_run(st, gate);
     });
 }
 
@@ -177,8 +178,9 @@ __device__ __forceinline__ void mx_finish(SolverState *st, double rsq, int gate,
         stalled = true;
         st->ru_stalled = 1;
     }
+    if (!isfinite(rsq) && !st->error) st->error = 1;  // non-finite residual: breakdown
     const bool ru = (rsq < delta2 * st->rsq_ru) || (rsq <= st->rsqstop) || stalled ||
-                    (st->iteration >= st->max_cg) || !(rsq == rsq) || run_guard(st);
+                    (st->iteration >= st->max_cg) || st->error || run_guard(st);
     if (ru) {
         st->skip_axpy = 1;  // this iteration's p update waits for the true residual
         stop_run(st, gate);
@@ -294,6 +296,11 @@ k_ms_residual(VecView<S> r, VecView<S> ttt, SolverState *st, double *partials, i
         const double rsq = t[0];
         st->oldrsq = oldrsq;
         st->rsq = rsq;
+        if (!isfinite(rsq) && !st->error) st->error = 1;  // non-finite residual: breakdown
+        if (st->error) {  // (or a zero p.Ap in the Dslash kernel before)
+            stop_run(st, gate);
+            return;
+        }
         if (rsq <= st->rsqstop) {
             st->converged = 1;
             stop_run(st, gate);

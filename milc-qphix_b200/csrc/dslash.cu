@@ -14,11 +14,14 @@
 //
 // Roofline: 1146 flop per site against >= 1200 B (FP32, 18-real links):
 // memory bound on HBM.
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <stdexcept>
+#include <string>
 
 #include "device_common.cuh"
+#include "tunecache.h"
 
 namespace qb {
 
@@ -154,10 +157,19 @@ template <> struct MinBlocks<__half, __half> { static constexpr int value = 3; }
 
 // Scalar step after p.(M^dag M p) is known: CG (mode 0) a = -rsq/pkp;
 // multi-shift (mode 1) the shift recurrences.  Runs in one thread.
+// A zero or non-finite p.(M p) is a breakdown (M is positive definite for
+// m > 0; the reference divides by it unchecked, ks_d_congrad_fn.cpp:511):
+// the step is set to zero, st->error = 2 and the update kernel that follows
+// ends the device run, so the host returns QPHIX_FAIL.
 __device__ __forceinline__ void mdagm_finalize(SolverState *st, double pkp, int mode)
 {
     st->pkp = pkp;
     st->iteration += 1;
+    if (!(pkp != 0.0) || !isfinite(pkp)) {
+        st->error = 2;
+        st->a = 0.0;
+        return;
+    }
     if (mode == 0) {
         st->a = round_to(-st->rsq / pkp, st->prec_single);
     } else {
@@ -251,6 +263,11 @@ template <> struct TmaCfg<double> { static constexpr int C = 36, T = 128, NS = 2
 template <> struct TmaCfg<float> { static constexpr int C = 18, T = 128, NS = 3; };
 template <> struct TmaCfg<__half> { static constexpr int C = 9, T = 128, NS = 4; };
 
+constexpr unsigned kDefaultWaitPolls = 1u << 22;  // far longer than any copy takes
+constexpr unsigned kDrainPolls = 1u << 22;
+// poll limit of the pipeline's waits (QPHIX_B200_set_wait_limit)
+static unsigned g_wait_limit = kDefaultWaitPolls;
+
 template <typename S>
 constexpr size_t tma_smem_bytes()
 {
@@ -314,10 +331,15 @@ __device__ __forceinline__ void tma_direction(const DslashArgs<SV, SL> &a, const
 
 // MODE 0: out = D in.  MODE 1: out = D in + m4 p, p.out reduced, then the
 // solver's scalar step (mdagm_finalize).
+// Every mbarrier wait gives up after `wait_limit` polls.  The CTA then
+// stops as a whole (the failure is OR-ed over the CTA at the end of the
+// stage), thread 0 waits -- with a generous limit -- for every copy still
+// in flight, so nothing lands in shared memory after the CTA has left,
+// records the failure in *err and the CTA returns.
 template <typename SV, typename SL, int MODE>
 __global__ void __launch_bounds__(TmaCfg<SL>::T)
 k_dslash_tma(DslashArgs<SV, SL> a, const char *links, VecView<SV> pv, double m4, SolverState *st,
-             double *partials, int gate, int mode, int *err)
+             double *partials, int gate, int mode, int *err, unsigned wait_limit)
 {
     using A = typename Acc<SV>::type;
     constexpr int C = TmaCfg<SL>::C, T = TmaCfg<SL>::T, NS = TmaCfg<SL>::NS;
@@ -325,7 +347,6 @@ k_dslash_tma(DslashArgs<SV, SL> a, const char *links, VecView<SV> pv, double m4,
     extern __shared__ __align__(128) unsigned char smem[];
     uint4 *buf = reinterpret_cast<uint4 *>(smem);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)NS * C * T * 16);
-    __shared__ int s_fail;
     const int tid = threadIdx.x;
     const int vh = a.g.vh;
     const int ntiles = (vh + T - 1) / T;
@@ -334,7 +355,6 @@ k_dslash_tma(DslashArgs<SV, SL> a, const char *links, VecView<SV> pv, double m4,
     if (tid == 0) {
         for (int b = 0; b < NS; ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
-        s_fail = 0;
     }
     __syncthreads();
     const uint64_t policy = policy_evict_first();
@@ -357,6 +377,7 @@ k_dslash_tma(DslashArgs<SV, SL> a, const char *links, VecView<SV> pv, double m4,
     double dot[1] = {0.0};
     A acc[6];
     int g = 0;
+    bool failed = false;
     for (; g < total; ++g) {
         if (tid == 0 && g + NS - 1 < total) {
             fence_proxy_async_smem();
@@ -370,8 +391,8 @@ k_dslash_tma(DslashArgs<SV, SL> a, const char *links, VecView<SV> pv, double m4,
 #pragma unroll
             for (int i = 0; i < 6; ++i) acc[i] = A(0);
         }
-        if (!mbar_wait_bounded(&bars[b], (uint32_t)((g / NS) & 1))) s_fail = 1;
-        if (j < vh) {
+        const bool ok = mbar_wait_bounded(&bars[b], (uint32_t)((g / NS) & 1), wait_limit);
+        if (ok && j < vh) {
             const SiteCoords s = decode(a.g, a.cb, j);
             tma_direction<SV, SL, A>(a, s, d, buf + (size_t)b * C * T + tid, acc);
             if (d == 3) {
@@ -389,14 +410,20 @@ k_dslash_tma(DslashArgs<SV, SL> a, const char *links, VecView<SV> pv, double m4,
                 }
             }
         }
-        __syncthreads();
-        if (s_fail) break;
+        // the barrier also keeps buffer b alive until every thread is done
+        // with it (the next stage's copy into it is issued after this point)
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
     }
-    if (s_fail) {
+    if (failed) {
         if (tid == 0) {
             atomicExch(err, 1);
-            // let copies still in flight land before the CTA's shared memory is released
-            for (int b = 0; b < NS; ++b) (void)mbar_wait_bounded(&bars[b], (uint32_t)(((g + b) / NS) & 1), 1u << 16);
+            // stages g .. g+NS-1 may still be in flight, one per barrier
+            const int last = min(g + NS - 1, total - 1);
+            for (int s2 = g; s2 <= last; ++s2)
+                (void)mbar_wait_bounded(&bars[s2 % NS], (uint32_t)((s2 / NS) & 1), kDrainPolls);
         }
         return;
     }
@@ -477,17 +504,30 @@ static int tma_grid(int vh)
 // ---------------------------------------------------------------------------
 constexpr int kVariants = 3;
 
+// -1: tuned; 0..2 forced (QPHIX_B200_DSLASH at load, QPHIX_B200_set_dslash_variant)
+static int g_forced = -2;
+
 static int forced_variant()
 {
-    static int v = -2;
-    if (v == -2) {
+    if (g_forced == -2) {
         const char *e = std::getenv("QPHIX_B200_DSLASH");
-        v = -1;
-        if (e && !std::strcmp(e, "plain")) v = 0;
-        if (e && !std::strcmp(e, "full")) v = 1;
-        if (e && !std::strcmp(e, "tma")) v = 2;
+        g_forced = -1;
+        if (e && !std::strcmp(e, "plain")) g_forced = 0;
+        if (e && !std::strcmp(e, "full")) g_forced = 1;
+        if (e && !std::strcmp(e, "tma")) g_forced = 2;
     }
-    return v;
+    return g_forced;
+}
+
+void set_forced_variant(int v)
+{
+    if (v < -1 || v >= 3) throw std::runtime_error("set_dslash_variant: variant must be -1, 0, 1 or 2");
+    g_forced = v;
+}
+
+void set_wait_limit(long polls)
+{
+    g_wait_limit = polls < 0 ? kDefaultWaitPolls : (unsigned)std::min<long>(polls, 0x7fffffffL);
 }
 
 struct TuneEntry {
@@ -504,6 +544,38 @@ static int link_slot(Prec pl)
     return std::is_same<SL, Recon12>::value ? 3 : std::is_same<SL, Recon13>::value ? 4 : (int)pl;
 }
 
+// key of a tuning result in the persistent cache
+static std::string tune_key(const char *kernel, int vh, Prec pv, int slot)
+{
+    return std::string(kernel) + ":" + tune_device_tag() + ":vh" + std::to_string(vh) + ":v" +
+           std::to_string((int)pv) + ":l" + std::to_string(slot);
+}
+
+// a cached choice for this (kernel, volume, precisions), if the cache has one
+static bool tune_from_cache(TuneEntry &t, const std::string &key, int vh, int nvariants)
+{
+    std::vector<double> v;
+    if (!tune_cache_get(key, v) || v.size() != 1 + kVariants) return false;
+    const int variant = (int)v[0];
+    if (variant < 0 || variant >= nvariants) return false;
+    t.vh = vh;
+    t.variant = variant;
+    for (int i = 0; i < kVariants; ++i) t.us[i] = (float)v[1 + i];
+    return true;
+}
+
+static void tune_to_cache(const TuneEntry &t, const std::string &key)
+{
+    tune_cache_put(key, {(double)t.variant, t.us[0], t.us[1], t.us[2]});
+}
+
+// the tuner times the pipeline with the default wait limit
+struct DefaultWaitLimit {
+    unsigned keep;
+    DefaultWaitLimit() : keep(g_wait_limit) { g_wait_limit = kDefaultWaitPolls; }
+    ~DefaultWaitLimit() { g_wait_limit = keep; }
+};
+
 // the TMA pipeline stages 18-real FP32 pairs; compressed Naik links run the
 // register variants only
 template <typename SL>
@@ -518,7 +590,7 @@ static void launch_variant(int variant, const DslashArgs<SV, SL> &a, const LinkS
     } else if (variant == 2) {
         k_dslash_tma<SV, SL, 0><<<tma_grid<SV, SL, 0>(L.g->vh), TmaCfg<SL>::T, tma_smem_bytes<SL>(), L.stream>>>(
             a, static_cast<const char *>(ls.blk[cb]), a.out, 0.0, const_cast<SolverState *>(st), nullptr, gate, 0,
-            L.err);
+            L.err, g_wait_limit);
         return;
     }
     if (variant == 1) {
@@ -535,6 +607,9 @@ static int tuned_variant(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV,
     if (f >= 0) return f;
     TuneEntry &t = g_tune[(int)pv][link_slot<SL>(pl)];
     if (t.vh == L.g->vh) return t.variant;
+    const std::string key = tune_key("dslash", L.g->vh, pv, link_slot<SL>(pl));
+    if (tune_from_cache(t, key, L.g->vh, has_tma<SL>() ? kVariants : 2)) return t.variant;
+    DefaultWaitLimit wl;
     // time the variants on scratch vectors so no caller data is touched twice
     const size_t vb = vec_bytes(pv, L.g->vh);
     void *vin = nullptr, *vout = nullptr;
@@ -565,6 +640,7 @@ static int tuned_variant(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV,
     cudaFreeAsync(vout, L.stream);
     t.vh = L.g->vh;
     t.variant = best;
+    tune_to_cache(t, key);
     return best;
 }
 
@@ -603,13 +679,6 @@ void dslash_gated(Prec p, const Launch &L, VecBlock out, VecBlock in, const Link
     QB_DISPATCH_VL(p, ls, launch_dslash, L, out, in, ls, cb, st, gate, p);
 }
 
-int dslash_variant(Prec pv, Prec pl, float us[3])
-{
-    const TuneEntry &t = g_tune[(int)pv][(int)pl];
-    for (int v = 0; v < kVariants; ++v) us[v] = t.us[v];
-    if (forced_variant() >= 0) return forced_variant();
-    return t.vh < 0 ? -1 : t.variant;
-}
 
 
 template <typename SV, typename SL>
@@ -621,7 +690,7 @@ static void launch_mdagm_variant(int variant, const DslashArgs<SV, SL> &a, const
         if (variant == 2) variant = 1;
     } else if (variant == 2) {
         k_dslash_tma<SV, SL, 1><<<tma_grid<SV, SL, 1>(L.g->vh), TmaCfg<SL>::T, tma_smem_bytes<SL>(), L.stream>>>(
-            a, static_cast<const char *>(ls.blk[cb]), pv, m4, st, partials, gate, mode, L.err);
+            a, static_cast<const char *>(ls.blk[cb]), pv, m4, st, partials, gate, mode, L.err, g_wait_limit);
         return;
     }
     if (variant == 1) {
@@ -644,6 +713,9 @@ static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashAr
     if (f >= 0) return f;
     TuneEntry &t = g_tune_mdagm[(int)pv][link_slot<SL>(pl)];
     if (t.vh == L.g->vh) return t.variant;
+    const std::string key = tune_key("mdagm", L.g->vh, pv, link_slot<SL>(pl));
+    if (tune_from_cache(t, key, L.g->vh, has_tma<SL>() ? kVariants : 2)) return t.variant;
+    DefaultWaitLimit wl;
     // scratch vectors, solver state and partials: no caller data is touched
     const size_t vb = vec_bytes(pv, L.g->vh);
     void *vin = nullptr, *vout = nullptr, *vp = nullptr;
@@ -682,7 +754,19 @@ static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashAr
         if (q) cudaFreeAsync(q, L.stream);
     t.vh = L.g->vh;
     t.variant = best;
+    tune_to_cache(t, key);
     return best;
+}
+
+// kernel 0: the Dslash (K1), 1: the fused M^dag M kernel (K2); slot: link
+// storage (Prec, or 3 / 4 for 12-real / 13-real Naik links)
+int dslash_variant(int kernel, Prec pv, int slot, float us[3])
+{
+    if (slot < 0 || slot > 4) return -1;
+    const TuneEntry &t = (kernel == 0 ? g_tune : g_tune_mdagm)[(int)pv][slot];
+    for (int v = 0; v < kVariants; ++v) us[v] = t.us[v];
+    if (forced_variant() >= 0) return forced_variant();
+    return t.vh < 0 ? -1 : t.variant;
 }
 
 template <typename SV, typename SL>

@@ -187,8 +187,14 @@ void dslash_mdagm_fixed_d(const Launch &L, VecBlock ttt, VecBlock tmp, const Lin
 // (required before a stream capture, which must not synchronise)
 void dslash_prepare(Prec pv, const LinkSet &ls, const Launch &L);
 
-// variant chosen by the Dslash autotuner for precision p; us = its timings
-int dslash_variant(Prec pv, Prec pl, float us[3]);
+// variant chosen by the autotuner for kernel 0 (Dslash) or 1 (fused M^dag M)
+// with vectors in pv and link storage `slot` (Prec, or 3 / 4 = 12-real /
+// 13-real Naik links); us = its timings; -1 before the first tuning
+int dslash_variant(int kernel, Prec pv, int slot, float us[3]);
+// -1: autotuned variants; 0..2: that variant everywhere
+void set_forced_variant(int v);
+// poll limit of the TMA pipeline's waits (< 0: the default)
+void set_wait_limit(long polls);
 
 // BLAS (blas.cu) ---------------------------------------------------------------
 // state->source_norm = |v|^2
@@ -244,10 +250,12 @@ void links_convert(Prec dst_p, LinkSet &dst, Prec src_p, const LinkSet &src, con
 // 12-real when lambda = sign * s with one magnitude s for all links, else
 // 13-real when each link has its own complex lambda; fills dst (allocated
 // here) and returns its recon mode (1 or 2), or leaves dst empty and returns
-// 0 when neither holds.  dev[0..4] receive the check's statistics (mean
+// 0 when neither holds.  want = 0 takes 12-real where it holds, else
+// 13-real; want = 1 or 2 asks for that form only (a 12-real field also has
+// the 13-real form).  dev[0..4] receive the check's statistics (mean
 // |ratio|, relative spread of |ratio|, relative imaginary part, relative
 // residual of the rows rebuilt with a real ratio, and with a complex one).
-int links_compress(LinkSet &dst, const LinkSet &src64, const Launch &L, double dev[5]);
+int links_compress(LinkSet &dst, const LinkSet &src64, const Launch &L, double dev[5], int want = 0);
 // fills ls_half.link_max[] from the ranges of `src` (fat and Naik slots)
 void links_absmax(Prec p, const LinkSet &src, LinkSet &ls_half, const Launch &L, double *scratch);
 

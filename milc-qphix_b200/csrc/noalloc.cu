@@ -18,10 +18,14 @@
 //    contents; the reduction counter is cleared at the start of each call.
 //    Calls whose work overlaps on the GPU (from several host threads or
 //    several streams) race on the array and give wrong results;
+//  * the call runs on the library's device (QPHIX_GPU_DEVICE at QPHIX_init)
+//    whatever device the calling thread has current, and restores the
+//    caller's current device before it returns;
 //  * the device address of the array is looked up (cudaGetSymbolAddress)
-//    on the first call made on each device, with that device current; make
+//    on the first call made for each device, with that device current; make
 //    that first call before any stream capture begins.
 #include <cstring>
+#include <mutex>
 
 #include "context.h"
 #include "device_common.cuh"
@@ -44,12 +48,14 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 unsigned char *g_scratch_addr[kMaxDevices] = {nullptr};
+std::mutex g_scratch_mu;  // first lookups from several host threads
 
-unsigned char *scratch_for_current_device()
+// Device address of the scratch on `dev`, which must be the current device
+// (a symbol's address is per device).
+unsigned char *scratch_for_device(int dev)
 {
-    int dev = 0;
-    QB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) throw Error("mdagm_noalloc: device index out of range");
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
     if (!g_scratch_addr[dev]) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -59,6 +65,21 @@ unsigned char *scratch_for_current_device()
     }
     return g_scratch_addr[dev];
 }
+
+// makes `dev` current for the scope and restores the caller's device
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int dev)
+    {
+        QB_CUDA(cudaGetDevice(&prev));
+        if (prev != dev) QB_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceScope()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
 
 }  // namespace
 }  // namespace qb
@@ -83,7 +104,9 @@ extern "C" QPHIX_status_t QPHIX_B200_D3_asqtad_mdagm_noalloc(QPHIX_D3_FermionLin
         const int cb = parity == QPHIX_EVEN ? 0 : 1;
         if (!(out->parity & parity) || !(in->parity & parity) || !in->blk[cb].data || !out->blk[cb].data)
             throw Error("mdagm_noalloc: in and out must hold the requested parity");
-        unsigned char *base = scratch_for_current_device();
+        // the stream and the links belong to the library's device
+        DeviceScope on_device(c.device);
+        unsigned char *base = scratch_for_device(c.device);
         SolverState *st = reinterpret_cast<SolverState *>(base);
         double *partials = reinterpret_cast<double *>(base + kStateBytes);
         VecBlock tmp{base + kStateBytes + kPartialBytes};

@@ -18,6 +18,9 @@
 // Bytes per output site of the FP32 Dslash: 8 fat x 72 + 8 Naik x 48 + 48
 // (vectors) + 4 (12-real sign word) = 1012 or + 64 (13-real ratios) = 1072,
 // instead of 1200.
+#include <algorithm>
+#include <cmath>
+
 #include "context.h"
 #include "device_common.cuh"
 
@@ -25,7 +28,8 @@ namespace qb {
 
 namespace {
 
-constexpr int kProbeNV = 5;
+constexpr int kProbeNV = 5;  // sums of the probe
+constexpr int kProbeNM = 2;  // maxima of the probe
 
 __device__ __forceinline__ void load_link64(const double2 *blk, int d, int slot, int j, int vh, double2 u[9])
 {
@@ -62,12 +66,16 @@ __device__ __forceinline__ double2 ratio(const double2 u[9], const double2 c[3],
 }
 
 // pass 0: sums of |rho|, (Im rho)^2, |row2 - Re(rho) c|^2, |row2|^2,
-//         |row2 - rho c|^2
-// pass 1: sum of (|rho| - mean)^2
+//         |row2 - rho c|^2, and the largest per-link relative residuals
+//         |row2 - Re(rho) c| / |row2| and |row2 - rho c| / |row2|
+// pass 1: sum of (|rho| - mean)^2 and the largest ||rho| - mean| / mean
+// A field-wide RMS alone would let a few links whose rows rebuild to only
+// ~1e-6 through; the maxima hold every link to the same bound.
 __global__ void __launch_bounds__(kBlock) k_recon_probe(const double2 *blk, int vh, int pass, double mean,
                                                         double *partials)
 {
     double s[kProbeNV] = {0, 0, 0, 0, 0};
+    double mx[kProbeNM] = {0, 0};
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < vh * 8; t += gridDim.x * blockDim.x) {
         const int j = t >> 3, d = (t >> 1) & 3, slot = 2 + (t & 1);
         double2 u[9], c[3];
@@ -77,32 +85,48 @@ __global__ void __launch_bounds__(kBlock) k_recon_probe(const double2 *blk, int 
         const double2 rho = ratio(u, c, &c2);
         const double mag = fabs(rho.x);
         if (pass == 0) {
-            s[0] += mag;
-            s[1] += rho.y * rho.y;
+            double e_re = 0, e_cx = 0, n2 = 0;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const double dr = u[6 + k].x - rho.x * c[k].x, di = u[6 + k].y - rho.x * c[k].y;
-                s[2] += dr * dr + di * di;
-                s[3] += u[6 + k].x * u[6 + k].x + u[6 + k].y * u[6 + k].y;
+                e_re += dr * dr + di * di;
+                n2 += u[6 + k].x * u[6 + k].x + u[6 + k].y * u[6 + k].y;
                 const double er = u[6 + k].x - (rho.x * c[k].x - rho.y * c[k].y);
                 const double ei = u[6 + k].y - (rho.x * c[k].y + rho.y * c[k].x);
-                s[4] += er * er + ei * ei;
+                e_cx += er * er + ei * ei;
             }
+            s[0] += mag;
+            s[1] += rho.y * rho.y;
+            s[2] += e_re;
+            s[3] += n2;
+            s[4] += e_cx;
+            // a link with a zero third row rebuilds only if row0 x row1 is zero too
+            mx[0] = fmax(mx[0], n2 > 0 ? sqrt(e_re / n2) : (e_re > 0 ? 1.0 : 0.0));
+            mx[1] = fmax(mx[1], n2 > 0 ? sqrt(e_cx / n2) : (e_cx > 0 ? 1.0 : 0.0));
         } else {
             s[0] += (mag - mean) * (mag - mean);
+            mx[0] = fmax(mx[0], mean > 0 ? fabs(mag - mean) / mean : 1.0);
         }
     }
-    __shared__ double sm[kProbeNV][kBlock / 32];
+    __shared__ double sm[kProbeNV + kProbeNM][kBlock / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int i = 0; i < kProbeNV; ++i) {
         const double v = warp_sum(s[i]);
         if (lane == 0) sm[i][w] = v;
     }
+#pragma unroll
+    for (int i = 0; i < kProbeNM; ++i) {
+        double v = mx[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+        if (lane == 0) sm[kProbeNV + i][w] = v;
+    }
     __syncthreads();
-    if (threadIdx.x < kProbeNV) {
+    if (threadIdx.x < kProbeNV + kProbeNM) {
+        const bool is_max = threadIdx.x >= kProbeNV;
         double v = 0;
-        for (int k = 0; k < kBlock / 32; ++k) v += sm[threadIdx.x][k];
+        for (int k = 0; k < kBlock / 32; ++k) v = is_max ? fmax(v, sm[threadIdx.x][k]) : v + sm[threadIdx.x][k];
         partials[threadIdx.x * gridDim.x + blockIdx.x] = v;
     }
 }
@@ -110,9 +134,9 @@ __global__ void __launch_bounds__(kBlock) k_recon_probe(const double2 *blk, int 
 __global__ void k_sum_partials(const double *partials, int nb, double *out)
 {
     const int i = threadIdx.x;
-    if (i >= kProbeNV) return;
+    if (i >= kProbeNV + kProbeNM) return;
     double v = 0;
-    for (int b = 0; b < nb; ++b) v += partials[i * nb + b];
+    for (int b = 0; b < nb; ++b) v = i >= kProbeNV ? fmax(v, partials[i * nb + b]) : v + partials[i * nb + b];
     out[i] = v;
 }
 
@@ -161,17 +185,18 @@ __global__ void __launch_bounds__(kBlock) k_recon_pack(float4 *dst, unsigned *si
 
 }  // namespace
 
-int links_compress(LinkSet &dst, const LinkSet &src64, const Launch &L, double dev[5])
+int links_compress(LinkSet &dst, const LinkSet &src64, const Launch &L, double dev[5], int want)
 {
     const int vh = L.g->vh;
     if (src64.prec != Prec::Double || !src64.valid) throw Error("links_compress: needs FP64 links");
+    constexpr int NT = kProbeNV + kProbeNM;
     const int nb = 296;
-    double *part = static_cast<double *>(dev_alloc(sizeof(double) * (kProbeNV * nb + kProbeNV)));
-    double *sums = part + kProbeNV * nb;
-    double h[kProbeNV], tot[kProbeNV] = {0, 0, 0, 0, 0};
-    double mean = 0, spread = 0;
+    double *part = static_cast<double *>(dev_alloc(sizeof(double) * (NT * nb + NT)));
+    double *sums = part + NT * nb;
+    double h[NT], tot[NT] = {0, 0, 0, 0, 0, 0, 0};
+    double mean = 0, spread = 0, spread_max = 0;
     for (int pass = 0; pass < 2; ++pass) {
-        double acc[kProbeNV] = {0, 0, 0, 0, 0};
+        double acc[NT] = {0, 0, 0, 0, 0, 0, 0};
         for (int cb = 0; cb < 2; ++cb) {
             k_recon_probe<<<nb, kBlock, 0, L.stream>>>(static_cast<const double2 *>(src64.blk[cb]), vh, pass, mean,
                                                       part);
@@ -179,13 +204,15 @@ int links_compress(LinkSet &dst, const LinkSet &src64, const Launch &L, double d
             QB_CUDA(cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, L.stream));
             sync_check();
             for (int i = 0; i < kProbeNV; ++i) acc[i] += h[i];
+            for (int i = kProbeNV; i < NT; ++i) acc[i] = std::max(acc[i], h[i]);
         }
         const double n = 2.0 * vh * 8;
         if (pass == 0) {
-            for (int i = 0; i < kProbeNV; ++i) tot[i] = acc[i];
+            for (int i = 0; i < NT; ++i) tot[i] = acc[i];
             mean = tot[0] / n;
         } else {
             spread = std::sqrt(acc[0] / n) / (mean > 0 ? mean : 1.0);
+            spread_max = acc[kProbeNV];
         }
     }
     dev_free(part);
@@ -195,10 +222,17 @@ int links_compress(LinkSet &dst, const LinkSet &src64, const Launch &L, double d
     dev[2] = mean > 0 ? std::sqrt(tot[1] / n) / mean : 1.0;
     dev[3] = tot[3] > 0 ? std::sqrt(tot[2] / tot[3]) : 1.0;
     dev[4] = tot[3] > 0 ? std::sqrt(tot[4] / tot[3]) : 1.0;
-    // the rebuilt rows must be exact far below FP32 rounding
+    // The rebuilt rows must be exact far below FP32 rounding, field-wide and
+    // link by link: 12-real needs one magnitude for every link and a real
+    // ratio rebuilding every third row; 13-real a complex ratio per link.
+    const double max_re = tot[kProbeNV], max_cx = tot[kProbeNV + 1];
+    const bool ok12 = mean > 0 && spread < 1e-9 && spread_max < 1e-9 && dev[2] < 1e-9 && dev[3] < 1e-9 &&
+                      max_re < 1e-9;
+    const bool ok13 = mean > 0 && dev[4] < 1e-9 && max_cx < 1e-9;
     int mode = 0;
-    if (mean > 0 && spread < 1e-9 && dev[2] < 1e-9 && dev[3] < 1e-9) mode = 1;
-    else if (mean > 0 && dev[4] < 1e-9) mode = 2;
+    if (want == 1) mode = ok12 ? 1 : 0;
+    else if (want == 2) mode = ok13 ? 2 : 0;
+    else mode = ok12 ? 1 : (ok13 ? 2 : 0);
     if (!mode) return 0;
     dst = LinkSet{};
     for (int cb = 0; cb < 2; ++cb) {

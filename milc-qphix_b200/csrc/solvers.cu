@@ -93,6 +93,23 @@ struct TimedLaunches {
     }
 };
 
+// The reference CG and multi-shift divide by p.Ap and |r|^2 unchecked
+// (ks_d_congrad_fn.cpp:511, ks_multicg_offset.cpp:475-520): a NaN or Inf in
+// the source or the links, or a zero p.Ap, runs on to the iteration limit
+// and returns garbage as success.  Here the device records the breakdown in
+// SolverState::error (1: non-finite residual, 2: zero or non-finite p.Ap)
+// and ends the run; the call returns QPHIX_FAIL with this message.
+[[noreturn]] void breakdown(const char *who, int code, int iteration)
+{
+    throw Error(std::string(who) + ": CG breakdown at iteration " + std::to_string(iteration) +
+                (code == 2 ? " (p.Ap is zero or not finite)" : " (the residual is not finite)"));
+}
+
+void require_finite(const char *who, double v, const char *what)
+{
+    if (!std::isfinite(v)) throw Error(std::string(who) + ": " + what + " is not finite");
+}
+
 int next_chunk(int current, double size_prev, double size_now, int done, double target, int cap)
 {
     Context &c = ctx();
@@ -263,9 +280,11 @@ int cg_reference(Prec P, const LinkSet &ls, SolveArgs &A)
     int total_iters = 0, iteration = 0, nrestart = 0;
     double rsq = 0, relrsq = 0, source_norm = 0;
     bool finished = false;
+    S.error = 0;
     while (!finished) {
         // start: (:309-350)
         source_norm = norm2_sync(P, t_src);
+        require_finite("asqtad_invert", source_norm, "|source|^2");
         nrestart = 0;
         total_iters += iteration;
         iteration = 0;
@@ -297,6 +316,7 @@ int cg_reference(Prec P, const LinkSet &ls, SolveArgs &A)
                 download_state();
                 tl.collect(INT_MAX);
                 rsq = S.rsq;
+                require_finite("asqtad_invert", rsq, "the restart residual |b - M x|^2");
                 if (relres) relrsq = R(std::sqrt(2 * S.relrsq / V));
                 res->final_rsq = R(rsq) / source_norm;
                 res->final_rel = R(relrsq);
@@ -345,6 +365,7 @@ int cg_reference(Prec P, const LinkSet &ls, SolveArgs &A)
                     return n;
                 },
                 tl, niter - (iteration % niter) + 1);
+            if (S.error) breakdown("asqtad_invert", S.error, S.iteration);
             iteration = S.iteration;
             rsq = S.rsq;
             relrsq = S.relrsq;
@@ -409,6 +430,8 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
     MixedResult out;
 
     const double bnorm = norm2_sync(Prec::Double, b);
+    require_finite("asqtad_invert", bnorm, "|source|^2");
+    S.error = 0;
     if (bnorm == 0.0) {
         vec_zero(Prec::Double, x, L);
         sync_check();
@@ -432,6 +455,7 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
     };
 
     double rsq = true_residual();
+    require_finite("asqtad_invert", rsq, "the true residual |b - M x|^2");
     out.true_rsq_rel = rsq / bnorm;
     if (out.true_rsq_rel < tol) return out;
 
@@ -470,6 +494,7 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
                 return n;
             },
             tl, max_cg - S.iteration + 1);
+        if (S.error) breakdown("asqtad_invert (mixed precision)", S.error, S.iteration);
         out.iterations = S.iteration;
         const double oldrsq = S.oldrsq;
         const double sloppy_rsq = S.rsq;
@@ -478,12 +503,13 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
         vec_zero(inner_x_prec(ps), xs, L);
         const double prev_true = rsq;
         rsq = true_residual();
+        require_finite("asqtad_invert (mixed precision)", rsq, "the true residual |b - M x|^2");
         out.reliable_updates++;
         out.true_rsq_rel = rsq / bnorm;
         if (c.verbose)
             std::fprintf(stderr, "qphix_b200 mixed CG: iter %d RU %d prec %d sloppy %.3e true %.3e\n",
                          S.iteration, out.reliable_updates, (int)ps, sloppy_rsq / bnorm, rsq / bnorm);
-        if (out.true_rsq_rel < tol || S.iteration >= max_cg || !std::isfinite(rsq)) break;
+        if (out.true_rsq_rel < tol || S.iteration >= max_cg) break;
         // A 16-bit inner solve perturbs the operator by ~1e-4 relative; once
         // the residual lives in the lowest modes of an ill-conditioned system
         // the corrections stop reducing the true residual, or the inner CG
@@ -603,6 +629,8 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
     const int other = 1 - parity;
     MsPass out;
     out.source_norm = norm2_sync(p, src);
+    require_finite("asqtad_invert_multi", out.source_norm, "|source|^2");
+    S.error = 0;
     for (int j = 0; j < n; ++j) vec_zero(xp, x[j], L);
     for (int j = 0; j < n; ++j) vec_copy(p, pm[j], p, src, L);
     vec_copy(p, resid, p, src, L);
@@ -653,10 +681,12 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
                 return m;
             },
             tl, max_cg + 1);
+        if (S.error) breakdown("asqtad_invert_multi", S.error, S.iteration);
         if (S.converged || !S.ms_ru || S.iteration >= max_cg) break;
         // reliable update of the base shift: r = b - (A + sigma_low) x_low in FP64
         const double prev = S.rsq_ru;
         const double rsq = reliable_update();
+        require_finite("asqtad_invert_multi", rsq, "the base shift's true residual");
         S.rsq = rsq;
         S.rsq_ru = rsq;
         ++out.reliable_updates;

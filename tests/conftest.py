@@ -41,7 +41,7 @@ def ref_lib():
     """The reference's own host code + restated kernel (oracle/_ref)."""
     if not os.path.exists(orc.REF_LIB):
         # the oracle recipe builds oracle/_ref only where the reference sources are
-        entry._make(os.path.join(ROOT, "oracle"))
+        entry.make_oracle()
         if not os.path.exists(orc.REF_LIB):
             pytest.skip("reference host-code oracle not built (reference sources absent)")
     return capi.QphixLib(orc.REF_LIB)

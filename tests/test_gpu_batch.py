@@ -3,9 +3,12 @@
 Several lattices of different sizes, several right-hand sides per lattice
 (segments of 6 + 1, 2 and 1 systems: register groups of G = 3, 2 and 1),
 different masses, one device run.  Every
-system must reach its FP64 true-residual tolerance as measured by the oracle
-(the reference's own host code with the restated Dslash), agree with the
-oracle's FP64 CG solution, and be bit-reproducible run to run.
+system must reach its FP64 true-residual tolerance as measured by the oracle,
+agree with the oracle's FP64 CG solution, and be bit-reproducible run to run.
+The oracle here is the plain-C restatement (oracle/qphix_oracle.c, built as
+oracle/_build/liboracle.so); it is tied to the reference's own host code by
+the CPU pin tests (tests/test_oracle_pin.py, tests/test_golden.py), not
+called here.
 """
 import os
 
