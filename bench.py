@@ -1068,9 +1068,91 @@ def run_force(args):
     }))
 
 
+DD_WORKLOAD = ("domain-decomposed asqtad CG: the lattice cut into t slabs, one per GPU, faces over NCCL "
+               "send/recv into each GPU's ghost buffer, FP64 sums by ncclAllReduce")
+
+
+def run_dd(args):
+    """--mode dd: the domain-decomposed path.  Under torchrun with N > 1 the
+    --lattice (default 32^3x64) is cut into N t slabs, one per GPU; every
+    rank solves its slab of the same system (FP64 CG, then mixed CG with
+    12-real Naik links); device time per solve, max over ranks (strong
+    scaling).  On one GPU: the headline mixed solve through the periodic
+    path and through the loopback halo path, to measure the halo's cost."""
+    import torch
+
+    world, rank, local, pg = dist_setup()
+    os.environ["QPHIX_GPU_DEVICE"] = str(local)
+    torch.cuda.set_device(local)
+    dims = tuple(int(v) for v in args.lattice.split("x")) if args.lattice else (MS_DIMS if world > 1 else DIMS)
+    mass = MS_MASS if dims == MS_DIMS else MASS
+    links = synthetic.asqtad_links(dims, seed=LINK_SEED, smear=dims == MS_DIMS,
+                                   eps_fat=0.2 if dims == MS_DIMS else 0.3,
+                                   device="cuda" if max(dims) > 16 else None)
+    src = synthetic.gaussian_source(dims, seed=SRC_SEED, parity="even")
+    lib = capi.QphixLib(LIB_PATH)
+    if world > 1:
+        from milc_qphix_b200 import decomp
+
+        uid = [lib.comm_unique_id() if rank == 0 else None]
+        pg.broadcast_object_list(uid, src=0)
+        assert lib.comm_init(uid[0], world, rank) == 0, lib.last_error()
+        assert lib.init(dims, (1, 1, 1, world), rank) == 0, lib.last_error()
+        links = {k: decomp.scatter(dims, v, world, rank, 72) for k, v in links.items()}
+        src = decomp.scatter(dims, src, world, rank, 6)
+    else:
+        assert lib.init(dims) == 0, lib.last_error()
+    lib.set_reliable_delta(0.2 if dims == MS_DIMS else RU_DELTA)
+    lib.set_link_compression(True)
+    L = lib.create_L("D", links)
+    b = lib.create_V("D", src, "even")
+    zeros = np.zeros_like(src)
+
+    def solve(inner, n):
+        lib.set_inner_precision(inner)
+        out = []
+        for _ in range(n):
+            x = lib.create_V("D", zeros, "even")
+            barrier(pg)
+            lib.timer_start()
+            it, info, res = lib.invert("D", L, x, b, mass, parity="even", max_iter=MAX_ITER, nrestart=NRESTART,
+                                       resid=RESID)
+            ms = lib.timer_stop()
+            assert info.status == 0, lib.last_error()
+            st = lib.last_stats()
+            out.append((max_over_ranks(pg, ms), st.iterations, res.final_rsq))
+            lib.destroy_V("D", x)
+        return out
+
+    result = {"mode": "dd", "workload": DD_WORKLOAD, "lattice": "x".join(map(str, dims)), "mass": mass,
+              "n_gpus": world, "scaling": "strong", "resid_sq": RESID}
+    paths = [("decomposed", False)] if world > 1 else [("periodic", False), ("loopback_halo", True)]
+    for name, loop in paths:
+        if world == 1:
+            lib.set_loopback_halo(loop)
+        r64 = solve("double", 2)[-1]
+        rmx = solve("single", 1 + max(1, args.steps))[1:]
+        result[name] = {"fp64_cg": {"s": r64[0] / 1e3, "iterations": r64[1], "true_rsq_rel": r64[2]},
+                        "mixed_cg": {"s": float(np.mean([t for t, _, _ in rmx])) / 1e3, "iterations": rmx[0][1],
+                                     "true_rsq_rel": max(q for _, _, q in rmx)}}
+    if world == 1:
+        lib.set_loopback_halo(False)
+        result["halo_cost_mixed"] = result["loopback_halo"]["mixed_cg"]["s"] / result["periodic"]["mixed_cg"]["s"]
+    lib.destroy_V("D", b)
+    lib.destroy_L("D", L)
+    lib.finalize()
+    if world > 1:
+        lib.comm_finalize()
+    if rank == 0:
+        print(json.dumps(result))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", default="bench", choices=["bench", "dslash", "mixed", "multishift", "batch", "force"],
+    ap.add_argument("--mode", default="bench",
+                    choices=["bench", "dslash", "mixed", "multishift", "batch", "force", "dd"],
                     help="bench: the benchmark line; dslash/mixed: small profiling targets; "
                          "multishift: the 32^3x64 CG and 12-shift multi-shift workload; "
                          "batch: 24 systems on 9 lattices in one batched solve; "
@@ -1113,6 +1195,9 @@ def main():
         return
     if args.mode == "force":
         run_force(args)
+        return
+    if args.mode == "dd":
+        run_dd(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -244,6 +244,41 @@ QPHIX_status_t QPHIX_B200_F3_asqtad_force(QPHIX_F3_FermionLinksAsqtad *L, int n,
                                           QPHIX_F3_ColorVector **x, QPHIX_evenodd_t parity,
                                           float *grad_fat, float *grad_lng);
 
+/* ---- Domain decomposition over several GPUs (no counterpart in this form
+ * in the reference) ---------------------------------------------------------
+ * The reference runs one MPI rank per node, exchanges the depth-3 faces of
+ * the Dslash input before each application (ks_boundary.cpp:185-825) and
+ * sums every dot product over the ranks (g_doublesum,
+ * ks_blas_utils_c.cpp:101-107).  Here one process drives one GPU and the
+ * lattice is cut into slabs along t only: faces go over NVLink with NCCL
+ * send/recv into each GPU's own ghost buffer while the interior of the
+ * Dslash runs, and the FP64 sums are ncclAllReduce calls.  NCCL is loaded
+ * at run time (libnccl.so.2); a single-GPU build needs none.
+ * Set-up: rank 0 calls QPHIX_B200_comm_unique_id and hands the 128 bytes to
+ * every rank (MPI_Bcast, a shared file, ...); every rank calls
+ * QPHIX_B200_comm_init(id, nranks, rank) with QPHIX_GPU_DEVICE naming its
+ * GPU, then QPHIX_init with the global latsize, machsize {1, 1, 1, nranks}
+ * and this_node = rank.  Nt / nranks must satisfy the QPHIX_init lattice
+ * checks (a multiple of 4).  The raw arrays of create/extract are then the
+ * rank's own sites in MILC's node-local even-first order, and
+ * fatback / lngback are the backward links of those sites (MILC gathers
+ * them).  The Dslash, CG and multi-shift CG (FP64 and mixed) run
+ * decomposed; the fermion force and the allocation-free operator refuse
+ * more than one rank.  QPHIX_B200_comm_finalize after QPHIX_finalize. */
+QPHIX_status_t QPHIX_B200_comm_unique_id(void *id128);
+QPHIX_status_t QPHIX_B200_comm_init(const void *id128, int nranks, int rank);
+QPHIX_status_t QPHIX_B200_comm_finalize(void);
+
+/* One GPU through the decomposed path: with on = 1 every Dslash packs its
+ * first and last three t-slices into the ghost buffer and reads its t
+ * neighbours beyond the slab from there -- the rank is its own t neighbour,
+ * each send buffer being the matching receive buffer, like the
+ * reference's ASSUME_MULTINODE (ks_boundary.cpp:196-200, 250-256) -- and
+ * every reduction goes through the split (sum over ranks, then finish)
+ * path.  Results equal the periodic single-GPU path to rounding.  For
+ * testing the decomposition on one GPU. */
+QPHIX_status_t QPHIX_B200_set_loopback_halo(int on);
+
 /* Host-side neighbour arithmetic used by the Dslash kernels (no GPU
  * needed): block index, in the opposite parity, of neighbour k of site
  * `site` of parity cb on lattice L[4] = {Nx,Ny,Nz,Nt}.  k follows the

@@ -66,12 +66,13 @@ _NODE_NUMBER = NODE_NUMBER_FN(_node_number)
 _NODE_INDEX = NODE_INDEX_FN(_node_index)
 
 
-def make_layout(dims):
-    """Single-node layout for lattice ``dims`` = [Nx, Ny, Nz, Nt]."""
+def make_layout(dims, machsize=(1, 1, 1, 1), this_node=0):
+    """Layout for the lattice ``dims`` = [Nx, Ny, Nz, Nt] cut into
+    ``machsize`` nodes; this process is node ``this_node``."""
     lat = (C.c_int * 4)(*dims)
-    mach = (C.c_int * 4)(1, 1, 1, 1)
-    V = int(np.prod(dims))
-    lay = Layout(_NODE_NUMBER, _NODE_INDEX, 4, lat, 4, mach, 0, V, V // 2, None)
+    mach = (C.c_int * 4)(*machsize)
+    V = int(np.prod(dims)) // int(np.prod(machsize))
+    lay = Layout(_NODE_NUMBER, _NODE_INDEX, 4, lat, 4, mach, int(this_node), V, V // 2, None)
     lay._keep = (lat, mach)
     return lay
 
@@ -149,6 +150,9 @@ class QphixLib:
             L.QPHIX_B200_mdagm_variant.restype = C.c_int
             L.QPHIX_B200_mdagm_variant.argtypes = [C.c_int, C.POINTER(C.c_double)]
             L.QPHIX_B200_set_dslash_variant.argtypes = [C.c_int]
+            L.QPHIX_B200_comm_unique_id.argtypes = [C.c_void_p]
+            L.QPHIX_B200_comm_init.argtypes = [C.c_void_p, C.c_int, C.c_int]
+            L.QPHIX_B200_set_loopback_halo.argtypes = [C.c_int]
             L.QPHIX_B200_set_wait_limit.argtypes = [C.c_long]
             L.QPHIX_B200_D3_asqtad_dslash_inner.restype = C.c_int
             L.QPHIX_B200_D3_asqtad_dslash_inner.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
@@ -290,6 +294,25 @@ class QphixLib:
         v = f(TUNE_CODE[prec_name], us)
         return v, list(us)
 
+    def comm_unique_id(self):
+        """128-byte NCCL unique id (rank 0 makes it, every rank gets a copy)."""
+        buf = C.create_string_buffer(128)
+        rc = self.lib.QPHIX_B200_comm_unique_id(buf)
+        if rc != 0:
+            raise RuntimeError("comm_unique_id failed: " + self.last_error())
+        return bytes(buf.raw)
+
+    def comm_init(self, uid, nranks, rank):
+        buf = C.create_string_buffer(bytes(uid), 128)
+        return self.lib.QPHIX_B200_comm_init(buf, int(nranks), int(rank))
+
+    def comm_finalize(self):
+        return self.lib.QPHIX_B200_comm_finalize()
+
+    def set_loopback_halo(self, on):
+        """Run one GPU through the decomposed (halo) path."""
+        return self.lib.QPHIX_B200_set_loopback_halo(1 if on else 0)
+
     def set_dslash_variant(self, variant):
         """Force Dslash variant 0, 1 or 2 everywhere; -1 returns to the autotuner."""
         return self.lib.QPHIX_B200_set_dslash_variant(int(variant))
@@ -336,9 +359,11 @@ class QphixLib:
         return getattr(self.lib, f"QPHIX_{prec}3_{name}")
 
     # -- API ---------------------------------------------------------------
-    def init(self, dims):
-        self._layout = make_layout(dims)
-        self.dims = tuple(dims)
+    def init(self, dims, machsize=(1, 1, 1, 1), this_node=0):
+        """QPHIX_init for the global lattice ``dims``; with several nodes
+        ``self.dims`` is this node's slab (the size of its raw arrays)."""
+        self._layout = make_layout(dims, machsize, this_node)
+        self.dims = tuple(int(d) // int(m) for d, m in zip(dims, machsize))
         return self.lib.QPHIX_init(C.byref(self._layout))
 
     def finalize(self):

@@ -58,17 +58,34 @@ void init_context(QPHIX_layout_t *layout)
     if (!layout || !layout->latsize) throw Error("QPHIX_init: layout or latsize is NULL");
     if (layout->machdim != layout->latdim) throw Error("QPHIX_init: machine dimension must equal lattice dimension");
     if (layout->latdim != 4) throw Error("QPHIX_init: only 4-dimensional lattices are supported");
-    int nranks = 1;
-    for (int i = 0; i < layout->machdim; ++i) nranks *= layout->machsize ? layout->machsize[i] : 1;
-    if (nranks != 1) throw Error("QPHIX_init: one lattice per GPU; machsize must be all ones");
-    const int *L = layout->latsize;
+    // Decomposition: t slabs only, one per process and GPU
+    // (QPHIX_B200_comm_init); machsize = {1, 1, 1, P}
+    int P = 1;
+    if (layout->machsize) {
+        for (int i = 0; i < 3; ++i)
+            if (layout->machsize[i] != 1)
+                throw Error("QPHIX_init: the lattice may be cut along t only (machsize {1,1,1,P})");
+        P = layout->machsize[3];
+    }
+    if (P < 1) throw Error("QPHIX_init: bad machsize");
+    if (P != comm_nranks())
+        throw Error("QPHIX_init: machsize[3] = " + std::to_string(P) + " but the communicator has " +
+                    std::to_string(comm_nranks()) + " ranks (QPHIX_B200_comm_init)");
+    if (P > 1 && layout->this_node != comm_rank())
+        throw Error("QPHIX_init: this_node differs from the communicator's rank");
+    const int *G = layout->latsize;
+    if (G[3] % P) throw Error("QPHIX_init: Nt is not a multiple of machsize[3]");
+    const int Lloc[4] = {G[0], G[1], G[2], G[3] / P};
+    const int *L = Lloc;
     check_lattice(L, "QPHIX_init");
     if (layout->node_number) {
         const int orig[4] = {0, 0, 0, 0};
         (void)layout->node_number(orig);  // the reference calls it (qphix_misc.cpp:489)
     }
     if (c.initialized) {
-        if (c.dims[0] == L[0] && c.dims[1] == L[1] && c.dims[2] == L[2] && c.dims[3] == L[3]) return;
+        if (c.dims[0] == L[0] && c.dims[1] == L[1] && c.dims[2] == L[2] && c.dims[3] == L[3] &&
+            c.global_dims[3] == G[3])
+            return;
         throw Error("QPHIX_init: already initialised with another lattice; call QPHIX_finalize first");
     }
     const char *dev = std::getenv("QPHIX_GPU_DEVICE");
@@ -80,7 +97,9 @@ void init_context(QPHIX_layout_t *layout)
     uint64_t thr = UINT64_MAX;
     QB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     for (int i = 0; i < 4; ++i) c.dims[i] = L[i];
+    for (int i = 0; i < 4; ++i) c.global_dims[i] = G[i];
     c.g = make_geom(L[0], L[1], L[2], L[3]);
+    halo_setup(c, P, comm_rank(), 2LL * c.g.vh * P);
     QB_CUDA(cudaMalloc(&c.d_state, sizeof(SolverState)));
     QB_CUDA(cudaMemset(c.d_state, 0, sizeof(SolverState)));
     QB_CUDA(cudaMallocHost(&c.h_state, sizeof(SolverState)));
@@ -121,12 +140,13 @@ void finalize_context()
     for (auto e : c.ktimer.ev) cudaEventDestroy(e);
     c.ktimer.ev.clear();
     free_staging();
+    halo_free(c);
     cudaStreamDestroy(c.stream);
     c.stream = nullptr;
     c.d_state = nullptr;
     c.h_state = nullptr;
     c.initialized = false;
-    for (int i = 0; i < 4; ++i) c.dims[i] = 0;
+    for (int i = 0; i < 4; ++i) c.dims[i] = c.global_dims[i] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -830,6 +850,30 @@ QPHIX_status_t QPHIX_B200_D3_asqtad_mdagm_inner(QPHIX_D3_FermionLinksAsqtad *L, 
                                                 QPHIX_B200_storage_t storage, double *in_dot_out)
 {
     return mdagm_inner(L, out, in, mass, parity, (int)storage, in_dot_out);
+}
+QPHIX_status_t QPHIX_B200_comm_unique_id(void *id128)
+{
+    return guarded([&] {
+        if (!id128) throw Error("comm_unique_id: NULL");
+        nccl_unique_id(id128);
+    });
+}
+QPHIX_status_t QPHIX_B200_comm_init(const void *id128, int nranks, int rank)
+{
+    return guarded([&] { comm_init(id128, nranks, rank); });
+}
+QPHIX_status_t QPHIX_B200_comm_finalize(void) { return guarded([&] { comm_finalize(); }); }
+QPHIX_status_t QPHIX_B200_set_loopback_halo(int on)
+{
+    return guarded([&] {
+        Context &c = ctx();
+        if (c.initialized && c.halo.nranks > 1) throw Error("set_loopback_halo: several ranks are in use");
+        set_loopback(on != 0);
+        if (c.initialized) {
+            QB_CUDA(cudaStreamSynchronize(c.stream));
+            halo_setup(c, 1, 0, 2LL * c.g.vh);
+        }
+    });
 }
 int QPHIX_B200_dslash_variant(int p, double us[3]) { return variant_report(0, p, us); }
 int QPHIX_B200_mdagm_variant(int p, double us[3]) { return variant_report(1, p, us); }

@@ -12,13 +12,28 @@
 #include <type_traits>
 
 #include "device_common.cuh"
+#include "halo.h"
 
 namespace qb {
 
 // ------------------------------------------------------------------ norms --
+// Finishing steps of the reductions, as functors so a domain-decomposed
+// solve can run them after the sum over GPUs (k_dd_fin).
+struct FinNorm2 {
+    SolverState *st;
+    int which;
+    double *out;
+    __device__ void operator()(const double *t) const
+    {
+        if (which == 0) st->source_norm = t[0];
+        else if (which == 1) st->rsq = t[0];
+        if (out) *out = t[0];
+    }
+};
+
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
-k_norm2(VecView<S> v, SolverState *st, double *partials, int which, double *out)
+k_norm2(VecView<S> v, SolverState *st, double *partials, int which, double *out, SolverState *split)
 {
     using A = typename Acc<S>::type;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -29,11 +44,7 @@ k_norm2(VecView<S> v, SolverState *st, double *partials, int which, double *out)
 #pragma unroll
         for (int i = 0; i < 6; ++i) s[0] += (double)(a[i] * a[i]);
     }
-    grid_reduce<1>(s, partials, &st->counter2, [&](const double *t) {
-        if (which == 0) st->source_norm = t[0];
-        else if (which == 1) st->rsq = t[0];
-        if (out) *out = t[0];
-    });
+    grid_reduce<1>(s, partials, &st->counter2, FinNorm2{st, which, out}, split);
 }
 
 // per-site |r|^2/|x|^2 term of relative_residue (ks_blas_utils_c.cpp:110-134)
@@ -53,10 +64,24 @@ __device__ __forceinline__ double relres_term(const A r[6], const A x[6])
 // ---------------------------------------------------------- CG restart --
 // calc_rsq (ks_d_congrad_fn.cpp:82-99): ttt += (-m4) x; r = b + ttt; p = r;
 // rsq = |r|^2 (+ relative residue sum when requested)
+struct FinRestart {
+    SolverState *st;
+    double *out;
+    __device__ void operator()(const double *t) const
+    {
+        if (out) {
+            out[0] = t[0];
+        } else {
+            st->rsq = t[0];
+            st->relrsq = t[1];
+        }
+    }
+};
+
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
 k_cg_restart(VecView<S> ttt, VecView<S> x, VecView<S> b, VecView<S> r, VecView<S> pv, bool setp,
-             SolverState *st, double *partials, bool relres, double *out)
+             SolverState *st, double *partials, bool relres, double *out, SolverState *split)
 {
     using A = typename Acc<S>::type;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -84,24 +109,44 @@ k_cg_restart(VecView<S> ttt, VecView<S> x, VecView<S> b, VecView<S> r, VecView<S
         for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
         if (relres) s[1] = relres_term(rv, xv);
     }
-    grid_reduce<2>(s, partials, &st->counter2, [&](const double *t) {
-        if (out) {
-            out[0] = t[0];
-        } else {
-            st->rsq = t[0];
-            st->relrsq = t[1];
-        }
-    });
+    grid_reduce<2>(s, partials, &st->counter2, FinRestart{st, out}, split);
 }
 
 // --------------------------------------------------------- CG iteration --
 // calc_rsq2 (ks_d_congrad_fn.cpp:131-147): x += a p; r += a ttt; rsq = |r|^2
 // followed by the scalar bookkeeping of :543-566 and the completion test at
 // the top of the loop (:360-363), evaluated on the device.
+// V: sites of the whole lattice (relative_residue divides by the global
+// volume, ks_blas_utils_c.cpp:148)
+struct FinCgUpdate {
+    SolverState *st;
+    int gate;
+    bool relres;
+    double V;
+    __device__ void operator()(const double *t) const
+    {
+        const int single = st->prec_single;
+        const double oldrsq = st->rsq;
+        const double rsq = t[0];
+        st->oldrsq = oldrsq;
+        st->rsq = rsq;
+        double relrsq = st->relrsq;
+        if (relres) relrsq = round_to(sqrt(2.0 * t[1] / V), single);
+        st->relrsq = relrsq;
+        st->size_r = round_to(rsq, single) / st->source_norm;
+        st->size_relr = round_to(relrsq, single);
+        st->b = round_to(round_to(rsq, single) / oldrsq, single);
+        const bool conv = (st->rsqmin <= 0 || st->rsqmin > st->size_r) &&
+                          (st->relrsqmin <= 0 || st->relrsqmin > st->size_relr);
+        if (!isfinite(rsq) && !st->error) st->error = 1;  // non-finite residual: breakdown
+        if ((st->iteration % st->niter == 0) || conv || st->error || run_guard(st)) stop_run(st, gate);
+    }
+};
+
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
 k_cg_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverState *st,
-            double *partials, int gate, bool relres, int V)
+            double *partials, int gate, bool relres, double V, SolverState *split)
 {
     using A = typename Acc<S>::type;
     if (gated_off(st, gate)) return;
@@ -125,23 +170,7 @@ k_cg_update(VecView<S> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverSta
         for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
         if (relres) s[1] = relres_term(rv, xv);
     }
-    grid_reduce<2>(s, partials, &st->counter, [&](const double *t) {
-        const int single = st->prec_single;
-        const double oldrsq = st->rsq;
-        const double rsq = t[0];
-        st->oldrsq = oldrsq;
-        st->rsq = rsq;
-        double relrsq = st->relrsq;
-        if (relres) relrsq = round_to(sqrt(2.0 * t[1] / (double)V), single);
-        st->relrsq = relrsq;
-        st->size_r = round_to(rsq, single) / st->source_norm;
-        st->size_relr = round_to(relrsq, single);
-        st->b = round_to(round_to(rsq, single) / oldrsq, single);
-        const bool conv = (st->rsqmin <= 0 || st->rsqmin > st->size_r) &&
-                          (st->relrsqmin <= 0 || st->relrsqmin > st->size_relr);
-        if (!isfinite(rsq) && !st->error) st->error = 1;  // non-finite residual: breakdown
-        if ((st->iteration % st->niter == 0) || conv || st->error || run_guard(st)) stop_run(st, gate);
-    });
+    grid_reduce<2>(s, partials, &st->counter, FinCgUpdate{st, gate, relres, V}, split);
 }
 
 // axpy (ks_d_congrad_fn.cpp:178-188): p = r + b p
@@ -186,6 +215,13 @@ __device__ __forceinline__ void mx_finish(SolverState *st, double rsq, int gate,
         stop_run(st, gate);
     }
 }
+
+struct FinMx {
+    SolverState *st;
+    int gate;
+    double delta2;
+    __device__ void operator()(const double *t) const { mx_finish(st, t[0], gate, delta2); }
+};
 
 // ------------------------------------------- flat vectorised p / x, r updates --
 // In FP32 and FP64 a parity block is one contiguous array of 6 Vh reals
@@ -239,7 +275,7 @@ template <typename R>
 __global__ void __launch_bounds__(kBlock)
 k_mx_update_flat(typename Wide<R>::type *x, const typename Wide<R>::type *p, typename Wide<R>::type *r,
                  const typename Wide<R>::type *ttt, long long n, SolverState *st, double *partials, int gate,
-                 double delta2)
+                 double delta2, SolverState *split)
 {
     if (gated_off(st, gate)) return;
     constexpr int W = Wide<R>::n;
@@ -265,32 +301,17 @@ k_mx_update_flat(typename Wide<R>::type *x, const typename Wide<R>::type *p, typ
         x[i] = wide_make(xv);
         r[i] = wide_make(rv);
     }
-    grid_reduce<1>(s, partials, &st->counter, [&](const double *tot) { mx_finish(st, tot[0], gate, delta2); });
+    grid_reduce<1>(s, partials, &st->counter, FinMx{st, gate, delta2}, split);
 }
 
 // ------------------------------------------------------------ multi-shift --
 // calc_rsq2 (ks_multicg_offset.cpp:124-140) + the convergence test (:520)
 // + the alpha recurrences (:587-598), evaluated on the device.
-template <typename S>
-__global__ void __launch_bounds__(kBlock)
-k_ms_residual(VecView<S> r, VecView<S> ttt, SolverState *st, double *partials, int gate)
-{
-    using A = typename Acc<S>::type;
-    if (gated_off(st, gate)) return;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    double s[1] = {0.0};
-    if (j < r.vh) {
-        A rv[6], t[6];
-        r.load_cg(j, rv);
-        ttt.load_cg(j, t);
-        const A bl = (A)st->beta_i[st->j_low];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) rv[i] = rv[i] + bl * t[i];
-        r.store(j, rv);
-#pragma unroll
-        for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
-    }
-    grid_reduce<1>(s, partials, &st->counter, [&](const double *t) {
+struct FinMsResidual {
+    SolverState *st;
+    int gate;
+    __device__ void operator()(const double *t) const
+    {
         const int single = st->prec_single;
         const double oldrsq = st->rsq;
         const double rsq = t[0];
@@ -330,7 +351,29 @@ k_ms_residual(VecView<S> r, VecView<S> ttt, SolverState *st, double *partials, i
             stop_run(st, gate);
         }
         if (st->iteration >= st->max_cg || run_guard(st)) stop_run(st, gate);
-    });
+    }
+};
+
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+k_ms_residual(VecView<S> r, VecView<S> ttt, SolverState *st, double *partials, int gate, SolverState *split)
+{
+    using A = typename Acc<S>::type;
+    if (gated_off(st, gate)) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    double s[1] = {0.0};
+    if (j < r.vh) {
+        A rv[6], t[6];
+        r.load_cg(j, rv);
+        ttt.load_cg(j, t);
+        const A bl = (A)st->beta_i[st->j_low];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) rv[i] = rv[i] + bl * t[i];
+        r.store(j, rv);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
+    }
+    grid_reduce<1>(s, partials, &st->counter, FinMsResidual{st, gate}, split);
 }
 
 // update_pm / update_dest (ks_multicg_offset.cpp:142-184) for every active
@@ -396,7 +439,7 @@ k_ms_update(VecBlock *xs, VecBlock *ps, VecView<S> r, int n, SolverState *st, in
 template <typename SX, typename S>
 __global__ void __launch_bounds__(kBlock)
 k_mx_update(VecView<SX> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverState *st,
-            double *partials, int gate, double delta2)
+            double *partials, int gate, double delta2, SolverState *split)
 {
     using A = typename Acc<S>::type;
     if (gated_off(st, gate)) return;
@@ -419,7 +462,7 @@ k_mx_update(VecView<SX> x, VecView<S> pv, VecView<S> r, VecView<S> ttt, SolverSt
 #pragma unroll
         for (int i = 0; i < 6; ++i) s[0] += (double)(rv[i] * rv[i]);
     }
-    grid_reduce<1>(s, partials, &st->counter, [&](const double *t) { mx_finish(st, t[0], gate, delta2); });
+    grid_reduce<1>(s, partials, &st->counter, FinMx{st, gate, delta2}, split);
 }
 
 // -------------------------------------------------------------- elementwise --
@@ -455,6 +498,23 @@ __global__ void __launch_bounds__(kBlock) k_add(VecView<Y> y, VecView<X> x)
 }
 
 // --------------------------------------------------------------- dispatch --
+// A domain-decomposed solve (L.halo set) splits every reduction: the
+// reducing kernel leaves this GPU's totals in st->dd_red, they are summed
+// over the GPUs in place (one ncclAllReduce; nothing with one GPU), and a
+// one-thread kernel takes the finishing step.
+inline SolverState *split_of(const Launch &L, SolverState *st) { return L.halo ? st : nullptr; }
+
+template <int NV, typename Fin>
+void dd_finish(const Launch &L, SolverState *st, int gate, Fin fin)
+{
+    if (!L.halo) return;
+    if (L.halo->nranks > 1) nccl_allreduce_sum(L.halo->comm, st->dd_red, NV, L.stream);
+    k_dd_fin<NV, Fin><<<1, 32, 0, L.stream>>>(st, gate, fin);
+}
+
+// sites of the whole lattice (all GPUs)
+inline double global_sites(const Launch &L) { return L.halo ? (double)L.halo->global_sites : 2.0 * L.g->vh; }
+
 #define QB_DISPATCH(p, F, ...)                               \
     switch (p) {                                             \
     case Prec::Double: F<double>(__VA_ARGS__); break;        \
@@ -465,7 +525,9 @@ __global__ void __launch_bounds__(kBlock) k_add(VecView<Y> y, VecView<X> x)
 template <typename S>
 static void norm2_impl(const Launch &L, VecBlock v, SolverState *st, double *partials, int which, double *out)
 {
-    k_norm2<S><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(view<S>(v, L.g->vh), st, partials, which, out);
+    k_norm2<S><<<grid_for(L.g->vh), kBlock, 0, L.stream>>>(view<S>(v, L.g->vh), st, partials, which, out,
+                                                          split_of(L, st));
+    dd_finish<1>(L, st, -1, FinNorm2{st, which, out});
 }
 
 void norm2_to_state(Prec p, const Launch &L, VecBlock v, SolverState *st, double *partials, int which)
@@ -481,7 +543,8 @@ static void restart_impl(const Launch &L, VecBlock ttt, VecBlock x, VecBlock b, 
     const int vh = L.g->vh;
     k_cg_restart<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(ttt, vh), view<S>(x, vh), view<S>(b, vh),
                                                            view<S>(r, vh), view<S>(pv, vh), setp, st,
-                                                           partials, relres, out);
+                                                           partials, relres, out, split_of(L, st));
+    dd_finish<2>(L, st, -1, FinRestart{st, out});
 }
 
 void cg_restart_residual(Prec p, const Launch &L, VecBlock ttt, VecBlock x, VecBlock b, VecBlock r,
@@ -495,9 +558,11 @@ static void update_impl(const Launch &L, VecBlock x, VecBlock pv, VecBlock r, Ve
                         SolverState *st, double *partials, int gate, bool relres)
 {
     const int vh = L.g->vh;
+    const double V = global_sites(L);
     k_cg_update<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(x, vh), view<S>(pv, vh), view<S>(r, vh),
-                                                          view<S>(ttt, vh), st, partials, gate, relres,
-                                                          2 * vh);
+                                                          view<S>(ttt, vh), st, partials, gate, relres, V,
+                                                          split_of(L, st));
+    dd_finish<2>(L, st, gate, FinCgUpdate{st, gate, relres, V});
 }
 
 void cg_update(Prec p, const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlock ttt,
@@ -530,7 +595,9 @@ template <typename S>
 static void msres_impl(const Launch &L, VecBlock r, VecBlock ttt, SolverState *st, double *partials, int gate)
 {
     const int vh = L.g->vh;
-    k_ms_residual<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(r, vh), view<S>(ttt, vh), st, partials, gate);
+    k_ms_residual<S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<S>(r, vh), view<S>(ttt, vh), st, partials, gate,
+                                                            split_of(L, st));
+    dd_finish<1>(L, st, gate, FinMsResidual{st, gate});
 }
 
 void ms_residual(Prec p, const Launch &L, VecBlock r, VecBlock ttt, SolverState *st, double *partials, int gate)
@@ -563,15 +630,16 @@ static void mx_impl(const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlo
     if constexpr (std::is_same<S, __half>::value) {
         k_mx_update<float, S><<<grid_for(vh), kBlock, 0, L.stream>>>(view<float>(x, vh), view<S>(pv, vh),
                                                                      view<S>(r, vh), view<S>(ttt, vh), st,
-                                                                     partials, gate, delta2);
+                                                                     partials, gate, delta2, split_of(L, st));
     } else {
         using V = typename Wide<S>::type;
         const long long n = 6LL * vh / Wide<S>::n;
         const int grid = (int)(((n + 1) / 2 + kBlock - 1) / kBlock);
         k_mx_update_flat<S><<<grid, kBlock, 0, L.stream>>>(static_cast<V *>(x.data), static_cast<const V *>(pv.data),
                                                            static_cast<V *>(r.data), static_cast<const V *>(ttt.data),
-                                                           n, st, partials, gate, delta2);
+                                                           n, st, partials, gate, delta2, split_of(L, st));
     }
+    dd_finish<1>(L, st, gate, FinMx{st, gate, delta2});
 }
 
 void mx_update(Prec p, const Launch &L, VecBlock x, VecBlock pv, VecBlock r, VecBlock ttt,

@@ -6,6 +6,7 @@
 #include <dlfcn.h>
 #include <nccl.h>
 
+#include <cstring>
 #include <mutex>
 #include <string>
 

@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "halo.h"
 #include "internal.h"
 #include "qphix.h"
 #include "qphix_b200.h"
@@ -102,11 +103,23 @@ struct Context {
 
     int *d_err = nullptr;            // kernel failure word (bounded waits)
     HostStaging staging;             // made on the first large pageable upload
+    Halo halo;                       // domain decomposition along t (halo.h)
+    int global_dims[4] = {0, 0, 0, 0};  // the whole lattice (dims: this GPU's slab)
 
-    Launch launch() const { return Launch{stream, &g, d_err}; }
+    Launch launch() const { return Launch{stream, &g, d_err, halo.on ? &halo : nullptr}; }
 };
 
 Context &ctx();
+
+// domain decomposition (halo.cu)
+void comm_init(const void *id128, int nranks, int rank);
+void comm_finalize();
+int comm_nranks();
+int comm_rank();
+void set_loopback(bool on);
+bool loopback();
+void halo_setup(Context &c, int nranks, int rank, long long global_sites);
+void halo_free(Context &c);
 
 // device memory from the stream-ordered pool (cached, no device-wide sync)
 void *dev_alloc(size_t bytes);

@@ -309,11 +309,14 @@ __device__ __forceinline__ double warp_sum(double v)
 
 // Reduce NV doubles over the grid.  Every block writes its partial sums to
 // partials[i*gridDim.x + blockIdx.x]; the last block to arrive sums them in
-// block order (deterministic) and calls fin(totals) from thread 0.
+// block order (deterministic) and calls fin(totals) from thread 0 -- or,
+// when `split` is given (a domain-decomposed solve), stores the totals of
+// this GPU in split->dd_red[] for the sum over GPUs, after which a
+// one-thread kernel calls fin (k_dd_fin).
 // Must be called by every thread of every block (uniform control flow).
 template <int NV, typename F>
 __device__ __forceinline__ void grid_reduce(double (&v)[NV], double *partials,
-                                            unsigned int *counter, F fin)
+                                            unsigned int *counter, F fin, SolverState *split = nullptr)
 {
     __shared__ double sm[NV][kBlock / 32];
     __shared__ bool am_last;
@@ -356,7 +359,12 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NV], double *partials,
             for (int k = 0; k < nw; ++k) s += sm[i][k];
             t[i] = s;
         }
-        fin(t);
+        if (split) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) split->dd_red[i] = t[i];
+        } else {
+            fin(t);
+        }
         *counter = 0;
         __threadfence();
     }
@@ -371,6 +379,19 @@ __device__ __forceinline__ bool gated_off(const SolverState *st, int gate)
 }
 
 inline int grid_for(int n) { return (n + kBlock - 1) / kBlock; }
+
+// Second half of a split reduction: after the totals in st->dd_red have been
+// summed over the GPUs, one thread applies the reduction's finishing step.
+// Gated like the reducing kernel.
+template <int NV, typename Fin>
+__global__ void k_dd_fin(SolverState *st, int gate, Fin fin)
+{
+    if (threadIdx.x || (gate >= 0 && gate > *(volatile const int *)&st->stop_at)) return;
+    double t[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) t[i] = st->dd_red[i];
+    fin(t);
+}
 
 // Ends the device run of a solver phase: records the stopping iteration for
 // the chunked launcher and, inside a CUDA-graph while loop, clears the loop

@@ -21,6 +21,7 @@
 #include <string>
 
 #include "device_common.cuh"
+#include "halo.h"
 #include "tunecache.h"
 
 namespace qb {
@@ -34,11 +35,37 @@ struct DslashArgs {
     LinkView<SL> links;
     Geom g;
     int cb;
+    // domain decomposition: the input parity's t-slices -3..-1 and Nt..Nt+2
+    // of the neighbouring slabs (component stride 3 * g.st, index
+    // slice * g.st + face site)
+    VecView<SV> gback, gfwd;
 };
+
+// Gathers neighbour k of output site s.  Without the halo (DD = false) every
+// neighbour is inside the lattice with periodic wrap.  With it the t
+// direction does not wrap: t - 1, t - 3 below 0 and t + 1, t + 3 at or
+// beyond Nt come from the ghost slices.  A t hop keeps xh (the parity flip
+// and the odd hop cancel in x = 2 xh + ((y+z+t+cb) & 1)).
+template <bool DD, typename SV, typename SL, typename A>
+__device__ __forceinline__ void load_nb(const DslashArgs<SV, SL> &a, const SiteCoords &s, int k, A v[6])
+{
+    if constexpr (DD) {
+        if (((k & 7) >> 1) == 3) {
+            const int hop = k < 8 ? 1 : 3;
+            const int t = s.t + ((k & 1) ? hop : -hop);
+            const int face = s.z * a.g.sz + s.y * a.g.sy + s.xh;
+            if (t < 0) a.gback.load((t + 3) * a.g.st + face, v);
+            else if (t >= a.g.nt) a.gfwd.load((t - a.g.nt) * a.g.st + face, v);
+            else a.in.load(t * a.g.st + face, v);
+            return;
+        }
+    }
+    a.in.load(neighbor(a.g, s, k), v);
+}
 
 // Neighbour k of output site s: one hop 2*d (backward) / 2*d+1 (forward),
 // three hops 8+2*d / 9+2*d (the reference's NeighTable order).
-template <typename SV, typename SL, typename A>
+template <typename SV, typename SL, typename A, bool DD = false>
 __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, A acc[6])
 {
     const SiteCoords s = decode(a.g, a.cb, j);
@@ -52,7 +79,7 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
             for (int sl = 0; sl < 4; ++sl) {
                 const int k = (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1);
                 A u[18], v[6];
-                a.in.load(neighbor(a.g, s, k), v);
+                load_nb<DD>(a, s, k, v);
                 a.links.load_mat(d, sl, j, u);
                 if (sl & 1) mv_adj_sub(acc, u, v);
                 else mv_add(acc, u, v);
@@ -75,8 +102,8 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
         A v[2][2][6];
         auto issue = [&](int st, int b) {
             const int d = st >> 1, h = st & 1;
-            a.in.load(neighbor(a.g, s, 8 * h + 2 * d + 1), v[b][0]);
-            a.in.load(neighbor(a.g, s, 8 * h + 2 * d), v[b][1]);
+            load_nb<DD>(a, s, 8 * h + 2 * d + 1, v[b][0]);
+            load_nb<DD>(a, s, 8 * h + 2 * d, v[b][1]);
             if constexpr (RN) {
                 if (h) {
                     a.links.fetch_naik(d, j, c[b]);
@@ -120,7 +147,7 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
         auto issue = [&](int d, int b) {
 #pragma unroll
             for (int sl = 0; sl < 4; ++sl)
-                a.in.load(neighbor(a.g, s, (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1)), v[b][sl]);
+                load_nb<DD>(a, s, (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1), v[b][sl]);
             a.links.load_quad(d, j, raw[b]);
         };
         issue(0, 0);
@@ -246,6 +273,89 @@ k_dslash_mdagm(DslashArgs<SV, SL> a, VecView<SV> pv, double m4, SolverState *st,
     }
     grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) { mdagm_finalize(st, tot[0], mode); });
 }
+
+// ---------------------------------------------------------------------------
+// Domain-decomposed Dslash (halo.h): sites of a range of t-slices, the t
+// neighbours beyond the slab read from the ghost slices.  Site i of the
+// launch is j = i + off_a for i < split, else i + off_b, so one launch
+// covers the interior (3 <= t < Nt-3) or both boundary bands (t < 3 and
+// t >= Nt-3).  With pv set the M^dag M epilogue out = D in + m4 pv is
+// applied (its dot product is reduced by k_dd_dot).
+// ---------------------------------------------------------------------------
+struct SiteRange {
+    int n, split, off_a, off_b;
+    __device__ __forceinline__ int site(int i) const { return i < split ? i + off_a : i + off_b; }
+};
+
+template <typename SV, typename SL>
+__global__ void __launch_bounds__(kBlock, MinBlocks<SV, SL>::value)
+k_dslash_dd(DslashArgs<SV, SL> a, SiteRange r, VecView<SV> pv, double m4, const SolverState *st, int gate)
+{
+    using A = typename Acc<SV>::type;
+    if (st && gated_off(st, gate)) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
+        const int j = r.site(i);
+        A acc[6];
+        dslash_site<SV, SL, A, true>(a, j, acc);
+        if (pv.p) {
+            A p[6];
+            pv.load_cg(j, p);
+            const A m = (A)m4;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) acc[k] = acc[k] + m * p[k];
+        }
+        a.out.store(j, acc);
+    }
+}
+
+// Copies the first and the last three t-slices of a parity block into the
+// send buffers (the neighbours' forward and backward ghosts), element by
+// element in the storage format (E: double2 / float2 per component, int4
+// per 16-bit site; C components).
+template <typename E, int C>
+__global__ void __launch_bounds__(kBlock)
+k_halo_pack(const E *in, E *sback, E *sfwd, int vh, int st, int nt, const SolverState *state, int gate)
+{
+    if (state && gated_off(state, gate)) return;
+    const int n = 3 * st;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        sback[(size_t)c * n + i] = in[(size_t)c * vh + i];
+        sfwd[(size_t)c * n + i] = in[(size_t)c * vh + (size_t)(nt - 3) * st + i];
+    }
+}
+
+struct FinNothing {
+    __device__ void operator()(const double *) const {}
+};
+
+// p . ttt of this GPU into st->dd_red[0] (the reduction of the fused kernel
+// K2, which the halo path does not fuse), products formed as K2 forms them
+template <typename SV>
+__global__ void __launch_bounds__(kBlock)
+k_dd_dot(VecView<SV> p, VecView<SV> t, SolverState *st, double *partials, int gate)
+{
+    using A = typename Acc<SV>::type;
+    if (gated_off(st, gate)) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    double s[1] = {0.0};
+    if (j < p.vh) {
+        A a[6], b[6];
+        p.load_cg(j, a);
+        t.load_cg(j, b);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s[0] += (double)(a[k] * b[k]);
+    }
+    grid_reduce<1>(s, partials, &st->counter, FinNothing{}, st);
+}
+
+struct FinMdagm {
+    SolverState *st;
+    int mode;
+    __device__ void operator()(const double *t) const { mdagm_finalize(st, t[0], mode); }
+};
 
 // ---------------------------------------------------------------------------
 // TMA-pipelined Dslash.  A persistent CTA owns tiles of T consecutive output
@@ -644,11 +754,62 @@ static int tuned_variant(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV,
     return best;
 }
 
+static void cuda_check(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// element type and components per site of the pack kernel
+template <typename SV> struct PackElem { using type = cx_t<SV>; static constexpr int C = 3; };
+template <> struct PackElem<__half> { using type = int4; static constexpr int C = 1; };
+
+// The Dslash with the halo (halo.h): pack the input parity's first and last
+// three t-slices; with several GPUs send them over NCCL on the
+// communication stream while the interior runs; then the boundary bands.
+template <typename SV, typename SL>
+static void halo_dslash(const Launch &L, DslashArgs<SV, SL> a, VecBlock in, Prec pvp, const SolverState *st,
+                        int gate, VecView<SV> pv, double m4)
+{
+    const Halo &h = *L.halo;
+    const Geom &g = *L.g;
+    const int pi = (int)pvp;
+    a.gback = view<SV>(VecBlock{h.gback[pi]}, 3 * g.st);
+    a.gfwd = view<SV>(VecBlock{h.gfwd[pi]}, 3 * g.st);
+    using E = typename PackElem<SV>::type;
+    k_halo_pack<E, PackElem<SV>::C><<<grid_for(3 * g.st), kBlock, 0, L.stream>>>(
+        static_cast<const E *>(in.data), static_cast<E *>(h.sback[pi]), static_cast<E *>(h.sfwd[pi]), g.vh, g.st,
+        g.nt, st, gate);
+    const bool remote = h.nranks > 1;
+    if (remote) {
+        cuda_check(cudaEventRecord(h.ev_packed, L.stream), "halo: cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(h.comm_stream, h.ev_packed, 0), "halo: cudaStreamWaitEvent");
+        nccl_exchange(h.comm, h.sback[pi], h.sfwd[pi], h.gback[pi], h.gfwd[pi], h.face_bytes[pi], h.prev, h.next,
+                      h.comm_stream);
+        cuda_check(cudaEventRecord(h.ev_recv, h.comm_stream), "halo: cudaEventRecord");
+    }
+    auto run = [&](SiteRange r) {
+        if (r.n > 0) k_dslash_dd<SV, SL><<<grid_for(r.n), kBlock, 0, L.stream>>>(a, r, pv, m4, st, gate);
+    };
+    if (g.nt >= 6) {
+        const int inner = (g.nt - 6) * g.st;
+        run(SiteRange{inner, inner, 3 * g.st, 0});  // 3 <= t < Nt-3: no ghost needed
+        if (remote) cuda_check(cudaStreamWaitEvent(L.stream, h.ev_recv, 0), "halo: cudaStreamWaitEvent");
+        run(SiteRange{6 * g.st, 3 * g.st, 0, inner});  // t < 3 and t >= Nt-3
+    } else {
+        if (remote) cuda_check(cudaStreamWaitEvent(L.stream, h.ev_recv, 0), "halo: cudaStreamWaitEvent");
+        run(SiteRange{g.vh, g.vh, 0, 0});
+    }
+}
+
 template <typename SV, typename SL>
 static void launch_dslash(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb,
                           const SolverState *st, int gate, Prec pv)
 {
     auto a = make_args<SV, SL>(L, out, in, ls, cb);
+    if (L.halo) {
+        halo_dslash<SV, SL>(L, a, in, pv, st, gate, VecView<SV>{}, 0.0);
+        return;
+    }
     launch_variant<SV, SL>(tuned_variant<SV, SL>(pv, ls.prec, L, a, ls, cb), a, ls, cb, L, st, gate);
 }
 
@@ -775,6 +936,16 @@ static void launch_mdagm(const Launch &L, VecBlock ttt, VecBlock tmp, const Link
                          int gate, int mode, Prec p)
 {
     auto a = make_args<SV, SL>(L, ttt, tmp, ls, cb);
+    if (L.halo) {
+        // ttt = D tmp + m4 p through the halo, then p.ttt summed over the GPUs
+        // and the solver's scalar step
+        const int vh = L.g->vh;
+        halo_dslash<SV, SL>(L, a, tmp, p, st, gate, view<SV>(pv, vh), m4);
+        k_dd_dot<SV><<<grid_for(vh), kBlock, 0, L.stream>>>(view<SV>(pv, vh), view<SV>(ttt, vh), st, partials, gate);
+        if (L.halo->nranks > 1) nccl_allreduce_sum(L.halo->comm, st->dd_red, 1, L.stream);
+        k_dd_fin<1, FinMdagm><<<1, 32, 0, L.stream>>>(st, gate, FinMdagm{st, mode});
+        return;
+    }
     const int variant = tuned_variant_mdagm<SV, SL>(p, ls.prec, L, a, ls, cb);
     launch_mdagm_variant<SV, SL>(variant, a, ls, view<SV>(pv, L.g->vh), m4, cb, st, partials, gate, mode, L);
 }

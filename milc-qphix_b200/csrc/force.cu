@@ -98,6 +98,8 @@ static void force_impl(typename ForceApi<Real>::FL *H, int n, const Real *coef, 
     if (!H || !coef || !x || !grad_fat || !grad_lng) throw Error("asqtad_force: NULL argument");
     if (n < 1) throw Error("asqtad_force: n must be at least 1");
     if (parity != QPHIX_EVEN && parity != QPHIX_ODD) throw Error("asqtad_force: parity must be EVEN or ODD");
+    // the outer products need the t neighbours of the slab's boundary sites
+    if (c.halo.on && c.halo.nranks > 1) throw Error("asqtad_force: not available with several ranks");
     const int P = parity == QPHIX_EVEN ? 0 : 1;
     for (int k = 0; k < n; ++k)
         if (!x[k] || !(x[k]->parity & parity)) throw Error("asqtad_force: solution vector lacks the parity");

@@ -153,15 +153,20 @@ struct SolverState {
     // the device loop stopped for it
     double ms_delta2;
     int ms_ru;
+    // domain decomposition: this GPU's totals of the last split reduction,
+    // summed in place over the GPUs before k_dd_fin reads them
+    double dd_red[4];
 };
 
 // ----------------------------------------------------------------------------
 // Kernel launchers (implemented in the .cu files)
 // ----------------------------------------------------------------------------
+struct Halo;
 struct Launch {
     cudaStream_t stream;
     const Geom *g;
-    int *err;  // device word set by a kernel whose bounded wait gave up
+    int *err;                     // device word set by a kernel whose bounded wait gave up
+    const Halo *halo = nullptr;   // t faces through ghost buffers (domain decomposition)
 };
 
 // out[cb] = D in[1-cb];  links = block of output parity cb

@@ -98,6 +98,7 @@ extern "C" QPHIX_status_t QPHIX_B200_D3_asqtad_mdagm_noalloc(QPHIX_D3_FermionLin
             throw Error("mdagm_noalloc: lattice has " + std::to_string(c.g.vh) +
                         " sites per parity; the allocation-free path holds at most " +
                         std::to_string(kNoAllocMaxSites));
+        if (c.halo.on) throw Error("mdagm_noalloc: not available with the decomposed (halo) path");
         if (!L || !out || !in) throw Error("mdagm_noalloc: NULL argument");
         if (parity != QPHIX_EVEN && parity != QPHIX_ODD)
             throw Error("mdagm_noalloc: parity must be QPHIX_EVEN or QPHIX_ODD");

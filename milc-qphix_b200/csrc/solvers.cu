@@ -154,7 +154,8 @@ public:
         S.skip_axpy = 0;
         S.err = c.d_err;
         S.counter = S.counter2 = 0;
-        if (graphs_enabled() && !tl.on) {
+        // NCCL calls are not captured: a solve over several GPUs runs in chunks
+        if (graphs_enabled() && !tl.on && !(c.halo.on && c.halo.nranks > 1)) {
             if (!exec_) build(enqueue);
             S.use_cond = 1;
             S.cond = handle_;
@@ -264,6 +265,8 @@ int cg_reference(Prec P, const LinkSet &ls, SolveArgs &A)
     int otherparity = 1 - parity;
     int parity0 = inv->parity;
     const double V = 2.0 * c.g.vh;
+    // relative_residue divides by the volume of the whole lattice (ks_blas_utils_c.cpp:148)
+    const double Vglobal = c.halo.on ? (double)c.halo.global_sites : V;
     const bool relres = relrsqmin > 0;
     if (niter <= 0) throw Error("invert: inv_arg->max must be positive");
 
@@ -317,7 +320,7 @@ int cg_reference(Prec P, const LinkSet &ls, SolveArgs &A)
                 tl.collect(INT_MAX);
                 rsq = S.rsq;
                 require_finite("asqtad_invert", rsq, "the restart residual |b - M x|^2");
-                if (relres) relrsq = R(std::sqrt(2 * S.relrsq / V));
+                if (relres) relrsq = R(std::sqrt(2 * S.relrsq / Vglobal));
                 res->final_rsq = R(rsq) / source_norm;
                 res->final_rel = R(relrsq);
                 iteration++;
