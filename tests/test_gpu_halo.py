@@ -128,20 +128,33 @@ def test_loopback_fp64_cg(gpu, dims):
 
 def test_loopback_relresid(gpu):
     """relative_residue (ks_blas_utils_c.cpp:136-149) through the split
-    reductions: the same stopping point as the oracle."""
+    reductions, with restarts: the oracle's stopping point and relative
+    residue (the loopback path sums p.Ap in another order, so the last bits
+    may differ)."""
     dims = (8, 8, 8, 8)
     lib = gpu.use(dims)
     links = fields(dims, seed=1001)
     src = synthetic.gaussian_source(dims, seed=2002, parity="even")
-    ito, xo, reso = orc.invert(dims, links, src, 0.05, "even", "D", max_iter=2000, nrestart=5, resid=0.0,
-                               relresid=1e-16)
+    ito, xo, reso = orc.invert(dims, links, src, 0.05, "even", "D", 50, 8, 1e-16, relresid=1e-6)
     assert lib.set_loopback_halo(True) == 0
+    lib.set_inner_precision("double")
     try:
-        res, x, st = _cg(lib, links, src, 0.05, relresid=1e-16, resid=0.0)
+        L = lib.create_L("D", links)
+        b = lib.create_V("D", src, "even")
+        x = lib.create_V("D", np.zeros_like(src), "even")
+        it, info, res = lib.invert("D", L, x, b, 0.05, parity="even", max_iter=50, nrestart=8, resid=1e-16,
+                                   relresid=1e-6)
+        assert info.status == 0, lib.last_error()
+        xs = lib.extract_V("D", x, "even")
+        for h in (x, b):
+            lib.destroy_V("D", h)
+        lib.destroy_L("D", L)
     finally:
         lib.set_loopback_halo(False)
-    assert abs(res.final_iter - reso.final_iter) <= 1
-    assert abs(res.final_rel - reso.final_rel) <= 1e-3 * reso.final_rel
+    assert abs(res.final_iter - reso.final_iter) <= 1 and res.final_restart == reso.final_restart
+    if res.final_iter == reso.final_iter:
+        assert abs(res.final_rel - reso.final_rel) <= 1e-8 * abs(reso.final_rel)
+    assert rel_err(xs[: 3 * 4096], xo[: 3 * 4096]) < 1e-8
 
 
 def test_loopback_mixed_cg_and_multishift(gpu):
