@@ -8,9 +8,10 @@ than against the library itself.
     0.3 Naik links), m = 0.0012, 12 RHMC shifts sigma log-spaced 1e-5 .. 1
     (masses sqrt(m^2 + sigma/4)).  Mixed multi-shift (FP32 inner with 12-real
     Naik links, FP64 solutions): every shift's true residual, recomputed by
-    the oracle, below 1e-20 (squared, relative); solutions within 1e-8 of the
-    FP64 multi-shift's; the sloppy recurrence's iteration count within 2 %
-    of the FP64 recurrence's.
+    the oracle, below 1e-20 (squared, relative); solutions within 5e-8 of the
+    FP64 multi-shift's (both at |r|/|b| < 1e-10: they differ by up to the
+    condition number times that, 1.1e-8 for the lightest shifts); the sloppy
+    recurrence's iteration count within 2 % of the FP64 recurrence's.
   * Config 4: 16 Gaussian right-hand sides on 24^3x48 plus two lattices each
     of 8^4, 12^4, 16^3x32 and 20^3x40, m = 0.02, in one batched solve: every
     system's oracle true residual below 1e-20 and its solution within 1e-8 of
@@ -106,7 +107,9 @@ def test_config3_mixed_multishift_32x32x32x64(gpu):
     e = slice(0, 3 * V)
     for k, m in enumerate(masses):
         assert orc.true_residual(dims, links, xm[k], src, m, "even") < 1.5 * RESID, k
-        assert rel_err(xm[k][e], x64[k][e]) < 1e-8, k
+        # two solutions with |r|/|b| < 1e-10 differ by up to the condition
+        # number times that; the light shifts here differ by ~1e-8
+        assert rel_err(xm[k][e], x64[k][e]) < 5e-8, k
     # both calls return the iterations of the shifted recurrence (the mixed
     # one before its per-shift refinements)
     assert abs(itm - it64) <= 0.02 * it64, (itm, it64)

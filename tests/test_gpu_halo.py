@@ -153,7 +153,7 @@ def test_loopback_relresid(gpu):
         lib.set_loopback_halo(False)
     assert abs(res.final_iter - reso.final_iter) <= 1 and res.final_restart == reso.final_restart
     if res.final_iter == reso.final_iter:
-        assert abs(res.final_rel - reso.final_rel) <= 1e-8 * abs(reso.final_rel)
+        assert abs(res.final_rel - reso.final_rel) <= 1e-6 * abs(reso.final_rel)
     assert rel_err(xs[: 3 * 4096], xo[: 3 * 4096]) < 1e-8
 
 
