@@ -1068,6 +1068,53 @@ def run_force(args):
     }))
 
 
+GF_WORKLOAD = ("Symanzik one-loop gauge force (6 plaquette, 18 rectangle, 24 parallelogram staples per link), "
+               "momentum update of one checkerboard, random SU(3) links")
+
+
+def run_gforce(args):
+    """--mode gforce: QPHIX_{D3,F3}_symanzik_1loop_gauge_force on --lattice
+    (default 32^3x64), one checkerboard per call, device time per call
+    (CUDA events around the kernel, mean of --reps calls after one warm-up)
+    and GFLOP/s by the call's own flop count (info.final_flop)."""
+    import torch  # noqa: F401  (CUDA context through the library)
+
+    dims = tuple(int(v) for v in args.lattice.split("x")) if args.lattice else MS_DIMS
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    lat = synthetic.Lattice(dims)
+    rng = np.random.default_rng(LINK_SEED)
+    # random SU(3) per link from QR of complex Gaussians (det fixed to 1)
+    V = lat.V
+    a = rng.standard_normal((V * 4, 3, 3)) + 1j * rng.standard_normal((V * 4, 3, 3))
+    q, r = np.linalg.qr(a)
+    q = q * (np.diagonal(r, axis1=1, axis2=2) / np.abs(np.diagonal(r, axis1=1, axis2=2)))[:, None, :]
+    q = q / np.linalg.det(q)[:, None, None] ** (1.0 / 3.0)
+    raw = np.empty((V * 4, 3, 3, 2))
+    raw[..., 0], raw[..., 1] = q.real, q.imag
+    Uraw = raw.reshape(-1)
+    mom = np.zeros(V * 72)
+    coeffs = {"plaquette": 1.0, "rectangle": -0.0545, "parallelogram": -0.0123}
+    lib = capi.QphixLib(LIB_PATH)
+    assert lib.init(dims) == 0, lib.last_error()
+    out = {"mode": "gforce", "workload": GF_WORKLOAD, "lattice": "x".join(map(str, dims)), "coeffs": coeffs}
+    for prec in ("D", "F"):
+        g = lib.create_G(prec, Uraw, "even")
+        f = lib.create_F(prec, mom, "even")
+        info = lib.gauge_force(prec, g, f, coeffs, 0.01)  # warm-up (table upload, module load)
+        assert info.status == 0, lib.last_error()
+        ms = []
+        for _ in range(max(1, args.reps)):
+            info = lib.gauge_force(prec, g, f, coeffs, 0.01)
+            ms.append(lib.last_stats().solve_ms)
+        t = float(np.mean(ms))
+        out[prec] = {"ms_per_call": t, "gflops": info.final_flop / (t * 1e-3) / 1e9,
+                     "flop_per_call": info.final_flop, "links_per_call": 4 * V // 2}
+        lib.destroy_G(prec, g)
+        lib.destroy_F(prec, f)
+    lib.finalize()
+    print(json.dumps(out))
+
+
 DD_WORKLOAD = ("domain-decomposed asqtad CG: the lattice cut into t slabs, one per GPU, faces over NCCL "
                "send/recv into each GPU's ghost buffer, FP64 sums by ncclAllReduce")
 
@@ -1152,7 +1199,7 @@ def run_dd(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--mode", default="bench",
-                    choices=["bench", "dslash", "mixed", "multishift", "batch", "force", "dd"],
+                    choices=["bench", "dslash", "mixed", "multishift", "batch", "force", "dd", "gforce"],
                     help="bench: the benchmark line; dslash/mixed: small profiling targets; "
                          "multishift: the 32^3x64 CG and 12-shift multi-shift workload; "
                          "batch: 24 systems on 9 lattices in one batched solve; "
@@ -1198,6 +1245,9 @@ def main():
         return
     if args.mode == "dd":
         run_dd(args)
+        return
+    if args.mode == "gforce":
+        run_gforce(args)
         return
     if args.impl == "reference":
         run_reference(args)

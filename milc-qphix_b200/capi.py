@@ -77,6 +77,11 @@ def make_layout(dims, machsize=(1, 1, 1, 1), this_node=0):
     return lay
 
 
+class GaugeCoeffs(C.Structure):
+    _fields_ = [("plaquette", C.c_double), ("rectangle", C.c_double),
+                ("parallelogram", C.c_double), ("adjoint_plaquette", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("solve_ms", C.c_double), ("iterations", C.c_int),
                 ("reliable_updates", C.c_int), ("dslash_launches", C.c_int),
@@ -128,6 +133,16 @@ class QphixLib:
             f.argtypes = [C.POINTER(Info), C.c_void_p, C.POINTER(InvertArg),
                           C.POINTER(C.POINTER(ResidArg)), rp, C.c_int,
                           C.POINTER(C.c_void_p), C.c_void_p]
+            for obj in ("G", "F"):
+                f = getattr(L, f"QPHIX_{P}3_create_{obj}_from_raw")
+                f.restype, f.argtypes = C.c_void_p, [rp, C.c_int]
+                f = getattr(L, f"QPHIX_{P}3_extract_{obj}_to_raw")
+                f.restype, f.argtypes = None, [rp, C.c_void_p, C.c_int]
+                f = getattr(L, f"QPHIX_{P}3_destroy_{obj}")
+                f.restype, f.argtypes = None, [C.c_void_p]
+            f = getattr(L, f"QPHIX_{P}3_symanzik_1loop_gauge_force")
+            f.restype = None
+            f.argtypes = [C.POINTER(Info), C.c_void_p, C.c_void_p, C.POINTER(GaugeCoeffs), real]
 
         # QPHIX_B200_* additions (absent from the reference library)
         self.has_b200 = hasattr(L, "QPHIX_B200_version")
@@ -403,6 +418,43 @@ class QphixLib:
 
     def destroy_L(self, prec, handle):
         self._fn(prec, "asqtad_destroy_L")(handle)
+
+    def create_G(self, prec, raw, evenodd="evenodd"):
+        ct, nt = self._real(prec)
+        a = np.ascontiguousarray(raw, dtype=nt)
+        return self._fn(prec, "create_G_from_raw")(a.ctypes.data_as(C.POINTER(ct)), PARITY[evenodd])
+
+    def create_F(self, prec, raw, evenodd="evenodd"):
+        ct, nt = self._real(prec)
+        a = np.ascontiguousarray(raw, dtype=nt)
+        return self._fn(prec, "create_F_from_raw")(a.ctypes.data_as(C.POINTER(ct)), PARITY[evenodd])
+
+    def _extract72(self, prec, name, handle, evenodd):
+        ct, nt = self._real(prec)
+        out = np.zeros(int(np.prod(self.dims)) * 72, dtype=nt)
+        self._fn(prec, name)(out.ctypes.data_as(C.POINTER(ct)), handle, PARITY[evenodd])
+        return out
+
+    def extract_G(self, prec, handle, evenodd="evenodd"):
+        return self._extract72(prec, "extract_G_to_raw", handle, evenodd)
+
+    def extract_F(self, prec, handle, evenodd="evenodd"):
+        return self._extract72(prec, "extract_F_to_raw", handle, evenodd)
+
+    def destroy_G(self, prec, handle):
+        self._fn(prec, "destroy_G")(handle)
+
+    def destroy_F(self, prec, handle):
+        self._fn(prec, "destroy_F")(handle)
+
+    def gauge_force(self, prec, G, F, coeffs, eps):
+        """QPHIX_*_symanzik_1loop_gauge_force; coeffs: dict of plaquette,
+        rectangle, parallelogram.  Returns the info struct."""
+        info = Info()
+        co = GaugeCoeffs(coeffs.get("plaquette", 0.0), coeffs.get("rectangle", 0.0),
+                         coeffs.get("parallelogram", 0.0), coeffs.get("adjoint_plaquette", 0.0))
+        self._fn(prec, "symanzik_1loop_gauge_force")(C.byref(info), G, F, C.byref(co), eps)
+        return info
 
     def dslash(self, prec, L, out, inp, parity):
         self._fn(prec, "asqtad_dslash")(L, out, inp, PARITY[parity])

@@ -654,12 +654,6 @@ int variant_report(int kernel, int p, double us[3])
     return v;
 }
 
-void not_on_path(QPHIX_info_t *info, const char *what)
-{
-    ctx().last_error = std::string(what) + ": the gauge force is not part of this library's solver path";
-    if (info) info->status = QPHIX_FAIL;
-}
-
 }  // namespace
 
 #pragma GCC visibility push(default)
@@ -707,17 +701,6 @@ int QPHIX_F3_asqtad_invert_multi(QPHIX_info_t *info, QPHIX_F3_FermionLinksAsqtad
 {
     return asqtad_invert_multi<float>(info, L, inv, res, mass, n, out, in);
 }
-QPHIX_F3_Force *QPHIX_F3_create_F_from_raw(QPHIX_F_Real *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_F3_create_F_from_raw"); return nullptr; }
-void QPHIX_F3_extract_F_to_raw(QPHIX_F_Real *, QPHIX_F3_Force *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_F3_extract_F_to_raw"); }
-void QPHIX_F3_destroy_F(QPHIX_F3_Force *) {}
-QPHIX_F3_GaugeField *QPHIX_F3_create_G_from_raw(QPHIX_F_Real *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_F3_create_G_from_raw"); return nullptr; }
-void QPHIX_F3_extract_G_to_raw(QPHIX_F_Real *, QPHIX_F3_GaugeField *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_F3_extract_G_to_raw"); }
-void QPHIX_F3_destroy_G(QPHIX_F3_GaugeField *) {}
-void QPHIX_F3_symanzik_1loop_gauge_force(QPHIX_info_t *info, QPHIX_F3_GaugeField *, QPHIX_F3_Force *,
-                                         QPHIX_gauge_coeffs_t *, QPHIX_F_Real)
-{
-    not_on_path(info, "QPHIX_F3_symanzik_1loop_gauge_force");
-}
 
 // ------------------------------------------------------------------- D3 --
 QPHIX_D3_ColorVector *QPHIX_D3_create_V_from_raw(QPHIX_D_Real *src, QPHIX_evenodd_t evenodd) { return create_V<double>(src, evenodd); }
@@ -749,17 +732,6 @@ int QPHIX_D3_asqtad_invert_multi(QPHIX_info_t *info, QPHIX_D3_FermionLinksAsqtad
                                  QPHIX_D3_ColorVector *in)
 {
     return asqtad_invert_multi<double>(info, L, inv, res, mass, n, out, in);
-}
-QPHIX_D3_Force *QPHIX_D3_create_F_from_raw(QPHIX_D_Real *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_D3_create_F_from_raw"); return nullptr; }
-void QPHIX_D3_extract_F_to_raw(QPHIX_D_Real *, QPHIX_D3_Force *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_D3_extract_F_to_raw"); }
-void QPHIX_D3_destroy_F(QPHIX_D3_Force *) {}
-QPHIX_D3_GaugeField *QPHIX_D3_create_G_from_raw(QPHIX_D_Real *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_D3_create_G_from_raw"); return nullptr; }
-void QPHIX_D3_extract_G_to_raw(QPHIX_D_Real *, QPHIX_D3_GaugeField *, QPHIX_evenodd_t) { not_on_path(nullptr, "QPHIX_D3_extract_G_to_raw"); }
-void QPHIX_D3_destroy_G(QPHIX_D3_GaugeField *) {}
-void QPHIX_D3_symanzik_1loop_gauge_force(QPHIX_info_t *info, QPHIX_D3_GaugeField *, QPHIX_D3_Force *,
-                                         QPHIX_gauge_coeffs_t *, QPHIX_D_Real)
-{
-    not_on_path(info, "QPHIX_D3_symanzik_1loop_gauge_force");
 }
 
 // --------------------------------------------------------------- B200 API --

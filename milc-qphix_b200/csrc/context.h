@@ -181,25 +181,33 @@ struct QPHIX_D3_FermionLinksAsqtad_struct {
     qb::LinkSet sloppy_recon;   // derived FP32 copy with 12-real or 13-real Naik links
     int recon_checked = 0;      // 1: compression was tried (sloppy_recon valid if it applied)
 };
+// Gauge fields and momenta of the gauge force (gforce.cu): both parity
+// blocks on the device, per block [dir][9 complex][Vh] (site-minor), FP32
+// for F3 and FP64 for D3.  `parity` is the checkerboard whose links the
+// force updates (the reference's rule: EVENODD works on EVEN).
 struct QPHIX_F3_GaugeField_struct {
     void *geo;
     int parity;
     int compress12;
+    void *blk[2];
 };
 struct QPHIX_D3_GaugeField_struct {
     void *geo;
     int parity;
     int compress12;
+    void *blk[2];
 };
 struct QPHIX_F3_Force_struct {
     void *heo;
     void *htmp;
     int parity;
+    void *blk[2];
 };
 struct QPHIX_D3_Force_struct {
     void *heo;
     void *htmp;
     int parity;
+    void *blk[2];
 };
 
 namespace qb {

@@ -114,6 +114,8 @@ def test_neighbour_index_rejects_out_of_range(product_lib_path):
 
 
 def test_gauge_force_entry_points_fail_cleanly(product_lib_path):
+    """Without QPHIX_init (and with NULL arguments) the gauge-force entry
+    points return QPHIX_FAIL / NULL instead of exiting."""
     lib = capi.QphixLib(product_lib_path)
     info = capi.Info()
     lib.lib.QPHIX_D3_symanzik_1loop_gauge_force.argtypes = [C.POINTER(capi.Info), C.c_void_p, C.c_void_p,
