@@ -115,10 +115,19 @@ QPHIX_status_t QPHIX_B200_D3_dslash_timed(void *links, void *out, void *in,
 #define QPHIX_B200_TUNE_F32_R13 5
 int QPHIX_B200_dslash_variant(int p, double us[3]);
 int QPHIX_B200_mdagm_variant(int p, double us[3]);
+/* The same for kernel 0 (Dslash) or 1 (fused M^dag M), with the timings of
+ * all variants: us[0..n-1] for variants 0..n-1, where variant 3 is the
+ * TMA neighbour-tile kernel (the nine (z, t) input planes of each output
+ * plane staged in shared memory by cp.async.bulk; FP32 and FP64 vectors,
+ * planes of up to 227 KB in all; 0 where a variant does not apply).
+ * Returns the chosen variant or -1. */
+int QPHIX_B200_tuning(int kernel, int p, double *us, int n);
 
-/* Forces the Dslash variant of every precision (0, 1 or 2 as above) or,
- * with -1 (the default), lets the autotuner choose.  Same effect as
- * QPHIX_B200_DSLASH=plain|full|tma, which sets the value at load. */
+/* Forces the Dslash variant of every precision (0, 1, 2 as above, 3 the
+ * neighbour-tile kernel of QPHIX_B200_tuning; a variant that does not apply
+ * to a precision or lattice runs as 1) or, with -1 (the default), lets the
+ * autotuner choose.  Same effect as QPHIX_B200_DSLASH=plain|full|tma|tile,
+ * which sets the value at load. */
 QPHIX_status_t QPHIX_B200_set_dslash_variant(int variant);
 
 /* Poll limit of the bounded mbarrier waits of the TMA-pipeline Dslash

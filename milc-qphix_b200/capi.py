@@ -165,6 +165,8 @@ class QphixLib:
             L.QPHIX_B200_mdagm_variant.restype = C.c_int
             L.QPHIX_B200_mdagm_variant.argtypes = [C.c_int, C.POINTER(C.c_double)]
             L.QPHIX_B200_set_dslash_variant.argtypes = [C.c_int]
+            L.QPHIX_B200_tuning.restype = C.c_int
+            L.QPHIX_B200_tuning.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double), C.c_int]
             L.QPHIX_B200_comm_unique_id.argtypes = [C.c_void_p]
             L.QPHIX_B200_comm_init.argtypes = [C.c_void_p, C.c_int, C.c_int]
             L.QPHIX_B200_set_loopback_halo.argtypes = [C.c_int]
@@ -327,6 +329,12 @@ class QphixLib:
     def set_loopback_halo(self, on):
         """Run one GPU through the decomposed (halo) path."""
         return self.lib.QPHIX_B200_set_loopback_halo(1 if on else 0)
+
+    def tuning(self, prec_name, kernel="dslash"):
+        """(variant, [us of variants 0..3]) of the autotuner."""
+        us = (C.c_double * 4)()
+        v = self.lib.QPHIX_B200_tuning(0 if kernel == "dslash" else 1, TUNE_CODE[prec_name], us, 4)
+        return v, list(us)
 
     def set_dslash_variant(self, variant):
         """Force Dslash variant 0, 1 or 2 everywhere; -1 returns to the autotuner."""

@@ -634,7 +634,7 @@ QPHIX_status_t dslash_timed(void *links, void *out, void *in, QPHIX_evenodd_t pa
 
 // autotuner report of kernel 0 (Dslash) / 1 (fused M^dag M) for the
 // precision codes of QPHIX_B200_dslash_variant
-int variant_report(int kernel, int p, double us[3])
+int variant_report(int kernel, int p, double *us, int n)
 {
     Prec pv;
     int slot;
@@ -647,10 +647,10 @@ int variant_report(int kernel, int p, double us[3])
     case QPHIX_B200_TUNE_F32_R13: pv = Prec::Single; slot = 4; break;
     default: return -1;
     }
-    float t[3] = {0, 0, 0};
+    float t[kDslashVariants] = {0, 0, 0, 0};
     const int v = dslash_variant(kernel, pv, slot, t);
     if (us)
-        for (int i = 0; i < 3; ++i) us[i] = t[i];
+        for (int i = 0; i < n && i < kDslashVariants; ++i) us[i] = t[i];
     return v;
 }
 
@@ -847,8 +847,12 @@ QPHIX_status_t QPHIX_B200_set_loopback_halo(int on)
         }
     });
 }
-int QPHIX_B200_dslash_variant(int p, double us[3]) { return variant_report(0, p, us); }
-int QPHIX_B200_mdagm_variant(int p, double us[3]) { return variant_report(1, p, us); }
+int QPHIX_B200_dslash_variant(int p, double us[3]) { return variant_report(0, p, us, 3); }
+int QPHIX_B200_mdagm_variant(int p, double us[3]) { return variant_report(1, p, us, 3); }
+int QPHIX_B200_tuning(int kernel, int p, double *us, int n)
+{
+    return (kernel == 0 || kernel == 1) ? variant_report(kernel, p, us, n) : -1;
+}
 QPHIX_status_t QPHIX_B200_set_dslash_variant(int variant) { return guarded([&] { set_forced_variant(variant); }); }
 QPHIX_status_t QPHIX_B200_set_wait_limit(long polls) { return guarded([&] { set_wait_limit(polls); }); }
 

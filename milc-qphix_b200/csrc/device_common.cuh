@@ -457,6 +457,15 @@ __device__ __forceinline__ uint64_t policy_evict_first()
     return p;
 }
 
+// L2 eviction policy for data read again soon (the neighbour planes of the
+// tile variant: every input plane is staged for nine output planes)
+__device__ __forceinline__ uint64_t policy_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 {
     uint32_t ok;

@@ -41,15 +41,28 @@ struct DslashArgs {
     VecView<SV> gback, gfwd;
 };
 
-// Gathers neighbour k of output site s.  Without the halo (DD = false) every
-// neighbour is inside the lattice with periodic wrap.  With it the t
-// direction does not wrap: t - 1, t - 3 below 0 and t + 1, t + 3 at or
-// beyond Nt come from the ghost slices.  A t hop keeps xh (the parity flip
-// and the odd hop cancel in x = 2 xh + ((y+z+t+cb) & 1)).
-template <bool DD, typename SV, typename SL, typename A>
-__device__ __forceinline__ void load_nb(const DslashArgs<SV, SL> &a, const SiteCoords &s, int k, A v[6])
-{
-    if constexpr (DD) {
+// Where the Dslash gathers neighbour k of output site s from:
+//  * NbGlobal: the input block, every neighbour inside the lattice with
+//    periodic wrap;
+//  * NbHalo: the same, except that the t direction does not wrap: t - 1,
+//    t - 3 below 0 and t + 1, t + 3 at or beyond Nt come from the ghost
+//    slices of the neighbouring slabs (domain decomposition);
+//  * NbTile: nine (z, t) planes of the input staged in shared memory (the
+//    TMA tile variant, k_dslash_tile).
+// A z or t hop keeps xh (the parity flip and the odd hop cancel in
+// x = 2 xh + ((y+z+t+cb) & 1)).
+struct NbGlobal {
+    template <typename SV, typename SL, typename A>
+    __device__ __forceinline__ void load(const DslashArgs<SV, SL> &a, const SiteCoords &s, int k, A v[6]) const
+    {
+        a.in.load(neighbor(a.g, s, k), v);
+    }
+};
+
+struct NbHalo {
+    template <typename SV, typename SL, typename A>
+    __device__ __forceinline__ void load(const DslashArgs<SV, SL> &a, const SiteCoords &s, int k, A v[6]) const
+    {
         if (((k & 7) >> 1) == 3) {
             const int hop = k < 8 ? 1 : 3;
             const int t = s.t + ((k & 1) ? hop : -hop);
@@ -59,14 +72,40 @@ __device__ __forceinline__ void load_nb(const DslashArgs<SV, SL> &a, const SiteC
             else a.in.load(t * a.g.st + face, v);
             return;
         }
+        a.in.load(neighbor(a.g, s, k), v);
     }
-    a.in.load(neighbor(a.g, s, k), v);
-}
+};
+
+// Nine planes of np = Nxh*Ny sites in shared memory, each [3][np] complex:
+// slot 0 the output plane's own (z, t), 1/2 z -/+ 1, 3/4 z -/+ 3, 5/6 t -/+ 1,
+// 7/8 t -/+ 3.  x and y neighbours stay in slot 0 (their block index minus
+// the plane's first index p0); z and t neighbours keep (xh, y).
+template <typename SV>
+struct NbTile {
+    const cx_t<SV> *base;
+    int np, p0;
+    template <typename SL, typename A>
+    __device__ __forceinline__ void load(const DslashArgs<SV, SL> &a, const SiteCoords &s, int k, A v[6]) const
+    {
+        const int d = (k & 7) >> 1;
+        int slot, idx;
+        if (d < 2) {
+            slot = 0;
+            idx = neighbor(a.g, s, k) - p0;
+        } else {
+            slot = 1 + (d - 2) * 4 + (k >= 8 ? 2 : 0) + (k & 1);
+            idx = s.y * a.g.sy + s.xh;
+        }
+        const cx_t<SV> *q = base + (size_t)slot * 3 * np + idx;
+        const cx_t<SV> x0 = q[0], x1 = q[np], x2 = q[2 * np];
+        v[0] = x0.x; v[1] = x0.y; v[2] = x1.x; v[3] = x1.y; v[4] = x2.x; v[5] = x2.y;
+    }
+};
 
 // Neighbour k of output site s: one hop 2*d (backward) / 2*d+1 (forward),
 // three hops 8+2*d / 9+2*d (the reference's NeighTable order).
-template <typename SV, typename SL, typename A, bool DD = false>
-__device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, A acc[6])
+template <typename SV, typename SL, typename A, typename NB = NbGlobal>
+__device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, A acc[6], const NB &nb = NB{})
 {
     const SiteCoords s = decode(a.g, a.cb, j);
 #pragma unroll
@@ -79,7 +118,7 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
             for (int sl = 0; sl < 4; ++sl) {
                 const int k = (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1);
                 A u[18], v[6];
-                load_nb<DD>(a, s, k, v);
+                nb.load(a, s, k, v);
                 a.links.load_mat(d, sl, j, u);
                 if (sl & 1) mv_adj_sub(acc, u, v);
                 else mv_add(acc, u, v);
@@ -102,8 +141,8 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
         A v[2][2][6];
         auto issue = [&](int st, int b) {
             const int d = st >> 1, h = st & 1;
-            load_nb<DD>(a, s, 8 * h + 2 * d + 1, v[b][0]);
-            load_nb<DD>(a, s, 8 * h + 2 * d, v[b][1]);
+            nb.load(a, s, 8 * h + 2 * d + 1, v[b][0]);
+            nb.load(a, s, 8 * h + 2 * d, v[b][1]);
             if constexpr (RN) {
                 if (h) {
                     a.links.fetch_naik(d, j, c[b]);
@@ -147,7 +186,7 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
         auto issue = [&](int d, int b) {
 #pragma unroll
             for (int sl = 0; sl < 4; ++sl)
-                load_nb<DD>(a, s, (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1), v[b][sl]);
+                nb.load(a, s, (sl < 2 ? 0 : 8) + 2 * d + (sl & 1 ? 0 : 1), v[b][sl]);
             a.links.load_quad(d, j, raw[b]);
         };
         issue(0, 0);
@@ -296,7 +335,7 @@ k_dslash_dd(DslashArgs<SV, SL> a, SiteRange r, VecView<SV> pv, double m4, const 
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
         const int j = r.site(i);
         A acc[6];
-        dslash_site<SV, SL, A, true>(a, j, acc);
+        dslash_site<SV, SL, A>(a, j, acc, NbHalo{});
         if (pv.p) {
             A p[6];
             pv.load_cg(j, p);
@@ -541,6 +580,114 @@ k_dslash_tma(DslashArgs<SV, SL> a, const char *links, VecView<SV> pv, double m4,
         grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) { mdagm_finalize(st, tot[0], mode); });
 }
 
+// ---------------------------------------------------------------------------
+// TMA neighbour-tile Dslash (variant 3).  A persistent CTA walks the (z, t)
+// planes of the output parity (np = Nxh*Ny sites each); for each plane one
+// thread issues cp.async.bulk copies of the nine input planes its sites
+// gather from -- its own (z, t), z -/+ 1, z -/+ 3, t -/+ 1, t -/+ 3, three
+// colour components each, 27 contiguous runs of np complex numbers -- into
+// shared memory, completing on an mbarrier; the threads then compute their
+// sites with every neighbour read from shared memory and the links streamed
+// from global memory as in the register kernel.  The input vectors, the
+// data with reuse, thus cross L2 -> SM once per plane (9 x 24 B per site in
+// FP32) instead of through per-thread gathers (16 x 24 B).  The wait is
+// bounded like the link pipeline's; no copy uses .multicast::cluster.
+// ---------------------------------------------------------------------------
+constexpr int kTileMaxThreads = 512;
+
+template <typename SV>
+__host__ __device__ constexpr size_t tile_smem_bytes(int np)
+{
+    return (size_t)27 * np * sizeof(cx_t<SV>) + 16;
+}
+
+// MODE 0: out = D in.  MODE 1: out = D in + m4 pv, pv.out reduced, then the
+// solver's scalar step.
+template <typename SV, typename SL, int MODE>
+__global__ void __launch_bounds__(kTileMaxThreads)
+k_dslash_tile(DslashArgs<SV, SL> a, VecView<SV> pv, double m4, SolverState *st, double *partials, int gate, int mode,
+              int *err, unsigned wait_limit)
+{
+    using A = typename Acc<SV>::type;
+    using E = cx_t<SV>;
+    if (st && gated_off(st, gate)) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const Geom &g = a.g;
+    const int np = g.sz;  // Nxh * Ny
+    E *tile = reinterpret_cast<E *>(smem);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + (size_t)27 * np * sizeof(E));
+    const int tid = threadIdx.x;
+    const int nplanes = g.nz * g.nt;
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const E *in = a.in.p;
+    const uint32_t run = (uint32_t)(np * sizeof(E));
+    double dot[1] = {0.0};
+    uint32_t phase = 0;
+    bool failed = false;
+    for (int plane = blockIdx.x; plane < nplanes; plane += gridDim.x) {
+        const int z = plane % g.nz, t = plane / g.nz;
+        if (tid == 0) {
+            // the barrier at the end of the previous plane ordered every read
+            // of the tile before this point
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(bar, 27u * run);
+#pragma unroll 1
+            for (int sl = 0; sl < 9; ++sl) {
+                // slot sl: 1/2 z -/+ 1, 3/4 z -/+ 3, 5/6 t -/+ 1, 7/8 t -/+ 3
+                const int hop = (sl - 1) % 4 < 2 ? 1 : 3;
+                const int step = sl == 0 ? 0 : ((sl & 1) ? -hop : hop);
+                const int zs = wrap(z + (sl >= 1 && sl <= 4 ? step : 0), g.nz);
+                const int ts = wrap(t + (sl >= 5 ? step : 0), g.nt);
+                const size_t p0 = (size_t)(ts * g.nz + zs) * np;
+#pragma unroll 1
+                for (int c = 0; c < 3; ++c)
+                    bulk_g2s(tile + ((size_t)sl * 3 + c) * np, in + (size_t)c * g.vh + p0, run, bar,
+                             policy_evict_last());
+            }
+        }
+        const bool ok = mbar_wait_bounded(bar, phase, wait_limit);
+        phase ^= 1u;
+        if (ok) {
+            const NbTile<SV> nb{tile, np, plane * np};
+            for (int i = tid; i < np; i += blockDim.x) {
+                const int j = plane * np + i;
+                A acc[6];
+                dslash_site<SV, SL, A>(a, j, acc, nb);
+                if constexpr (MODE == 0) {
+                    a.out.store(j, acc);
+                } else {
+                    A p[6];
+                    pv.load_cg(j, p);
+                    const A m = (A)m4;
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) acc[k] = acc[k] + m * p[k];
+                    a.out.store(j, acc);
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) dot[0] += (double)(p[k] * acc[k]);
+                }
+            }
+        }
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+    }
+    if (failed) {
+        if (tid == 0) {
+            atomicExch(err, 1);
+            // the plane's copies may still be in flight (the phase just waited on)
+            (void)mbar_wait_bounded(bar, phase ^ 1u, kDrainPolls);
+        }
+        return;
+    }
+    if constexpr (MODE == 1)
+        grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) { mdagm_finalize(st, tot[0], mode); });
+}
+
 template <typename SV, typename SL>
 static DslashArgs<SV, SL> make_args(const Launch &L, VecBlock out, VecBlock in, const LinkSet &ls, int cb)
 {
@@ -612,9 +759,9 @@ static int tma_grid(int vh)
 // vectors with the caller's links and keeps the fastest; QPHIX_B200_DSLASH=
 // plain|full|tma forces one.  The fused M^dag M kernel follows the choice.
 // ---------------------------------------------------------------------------
-constexpr int kVariants = 3;
+constexpr int kVariants = 4;
 
-// -1: tuned; 0..2 forced (QPHIX_B200_DSLASH at load, QPHIX_B200_set_dslash_variant)
+// -1: tuned; 0..3 forced (QPHIX_B200_DSLASH at load, QPHIX_B200_set_dslash_variant)
 static int g_forced = -2;
 
 static int forced_variant()
@@ -625,13 +772,14 @@ static int forced_variant()
         if (e && !std::strcmp(e, "plain")) g_forced = 0;
         if (e && !std::strcmp(e, "full")) g_forced = 1;
         if (e && !std::strcmp(e, "tma")) g_forced = 2;
+        if (e && !std::strcmp(e, "tile")) g_forced = 3;
     }
     return g_forced;
 }
 
 void set_forced_variant(int v)
 {
-    if (v < -1 || v >= 3) throw std::runtime_error("set_dslash_variant: variant must be -1, 0, 1 or 2");
+    if (v < -1 || v >= kVariants) throw std::runtime_error("set_dslash_variant: variant must be -1, 0, 1, 2 or 3");
     g_forced = v;
 }
 
@@ -643,7 +791,7 @@ void set_wait_limit(long polls)
 struct TuneEntry {
     int vh = -1;
     int variant = 0;
-    float us[kVariants] = {0, 0, 0};
+    float us[kVariants] = {0, 0, 0, 0};
 };
 // per (vector precision, link storage: Prec, or 3 / 4 = 12-real / 13-real Naik)
 static TuneEntry g_tune[3][5];
@@ -662,12 +810,12 @@ static std::string tune_key(const char *kernel, int vh, Prec pv, int slot)
 }
 
 // a cached choice for this (kernel, volume, precisions), if the cache has one
-static bool tune_from_cache(TuneEntry &t, const std::string &key, int vh, int nvariants)
+static bool tune_from_cache(TuneEntry &t, const std::string &key, int vh)
 {
     std::vector<double> v;
     if (!tune_cache_get(key, v) || v.size() != 1 + kVariants) return false;
     const int variant = (int)v[0];
-    if (variant < 0 || variant >= nvariants) return false;
+    if (variant < 0 || variant >= kVariants) return false;
     t.vh = vh;
     t.variant = variant;
     for (int i = 0; i < kVariants; ++i) t.us[i] = (float)v[1 + i];
@@ -676,7 +824,7 @@ static bool tune_from_cache(TuneEntry &t, const std::string &key, int vh, int nv
 
 static void tune_to_cache(const TuneEntry &t, const std::string &key)
 {
-    tune_cache_put(key, {(double)t.variant, t.us[0], t.us[1], t.us[2]});
+    tune_cache_put(key, {(double)t.variant, t.us[0], t.us[1], t.us[2], t.us[3]});
 }
 
 // the tuner times the pipeline with the default wait limit
@@ -691,10 +839,70 @@ struct DefaultWaitLimit {
 template <typename SL>
 constexpr bool has_tma() { return !std::is_same<SL, Recon12>::value && !std::is_same<SL, Recon13>::value; }
 
+// the tile variant stages FP32 or FP64 vectors; nine planes must fit the
+// 227 KB of shared memory a CTA may have
+constexpr size_t kMaxDynSmem = 232448;
+template <typename SV>
+static bool tile_ok(const Geom &g)
+{
+    if constexpr (std::is_same<SV, float>::value || std::is_same<SV, double>::value)
+        return tile_smem_bytes<SV>(g.sz) <= kMaxDynSmem;
+    else
+        return false;
+}
+
+template <typename SV, typename SL>
+static bool variant_ok(int v, const Geom &g)
+{
+    if (v == 2) return has_tma<SL>();
+    if (v == 3) return tile_ok<SV>(g);
+    return v == 0 || v == 1;
+}
+
+// launch shape of the tile variant: one CTA per plane at a time, all CTAs
+// resident
+struct TileShape {
+    int block, grid;
+    size_t smem;
+};
+template <typename SV, typename SL, int MODE>
+static TileShape tile_shape(const Geom &g)
+{
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_dslash_tile<SV, SL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kMaxDynSmem);
+        attr = true;
+    }
+    TileShape t;
+    t.block = std::min(kTileMaxThreads, (g.sz + 31) / 32 * 32);
+    t.smem = tile_smem_bytes<SV>(g.sz);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dslash_tile<SV, SL, MODE>, t.block, t.smem) !=
+            cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    t.grid = std::min(g.nz * g.nt, per_sm * sms);
+    return t;
+}
+
 template <typename SV, typename SL>
 static void launch_variant(int variant, const DslashArgs<SV, SL> &a, const LinkSet &ls, int cb, const Launch &L,
                            const SolverState *st, int gate)
 {
+    if (variant == 3) {
+        if constexpr (std::is_same<SV, float>::value || std::is_same<SV, double>::value) {
+            if (tile_ok<SV>(*L.g)) {
+                const TileShape ts = tile_shape<SV, SL, 0>(*L.g);
+                k_dslash_tile<SV, SL, 0><<<ts.grid, ts.block, ts.smem, L.stream>>>(
+                    a, a.out, 0.0, const_cast<SolverState *>(st), nullptr, gate, 0, L.err, g_wait_limit);
+                return;
+            }
+        }
+        variant = 1;
+    }
     if constexpr (!has_tma<SL>()) {
         if (variant == 2) variant = 1;
     } else if (variant == 2) {
@@ -718,7 +926,7 @@ static int tuned_variant(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV,
     TuneEntry &t = g_tune[(int)pv][link_slot<SL>(pl)];
     if (t.vh == L.g->vh) return t.variant;
     const std::string key = tune_key("dslash", L.g->vh, pv, link_slot<SL>(pl));
-    if (tune_from_cache(t, key, L.g->vh, has_tma<SL>() ? kVariants : 2)) return t.variant;
+    if (tune_from_cache(t, key, L.g->vh) && variant_ok<SV, SL>(t.variant, *L.g)) return t.variant;
     DefaultWaitLimit wl;
     // time the variants on scratch vectors so no caller data is touched twice
     const size_t vb = vec_bytes(pv, L.g->vh);
@@ -733,7 +941,9 @@ static int tuned_variant(Prec pv, Prec pl, const Launch &L, const DslashArgs<SV,
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int best = 0;
-    for (int v = 0; v < (has_tma<SL>() ? kVariants : 2); ++v) {
+    for (int v = 0; v < kVariants; ++v) {
+        t.us[v] = 0.f;
+        if (!variant_ok<SV, SL>(v, *L.g)) continue;
         launch_variant<SV, SL>(v, s, ls, cb, L, nullptr, -1);  // warm
         cudaEventRecord(e0, L.stream);
         for (int r = 0; r < 3; ++r) launch_variant<SV, SL>(v, s, ls, cb, L, nullptr, -1);
@@ -847,6 +1057,17 @@ static void launch_mdagm_variant(int variant, const DslashArgs<SV, SL> &a, const
                                  double m4, int cb, SolverState *st, double *partials, int gate, int mode,
                                  const Launch &L)
 {
+    if (variant == 3) {
+        if constexpr (std::is_same<SV, float>::value || std::is_same<SV, double>::value) {
+            if (tile_ok<SV>(*L.g)) {
+                const TileShape ts = tile_shape<SV, SL, 1>(*L.g);
+                k_dslash_tile<SV, SL, 1><<<ts.grid, ts.block, ts.smem, L.stream>>>(a, pv, m4, st, partials, gate,
+                                                                                   mode, L.err, g_wait_limit);
+                return;
+            }
+        }
+        variant = 1;
+    }
     if constexpr (!has_tma<SL>()) {
         if (variant == 2) variant = 1;
     } else if (variant == 2) {
@@ -875,7 +1096,7 @@ static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashAr
     TuneEntry &t = g_tune_mdagm[(int)pv][link_slot<SL>(pl)];
     if (t.vh == L.g->vh) return t.variant;
     const std::string key = tune_key("mdagm", L.g->vh, pv, link_slot<SL>(pl));
-    if (tune_from_cache(t, key, L.g->vh, has_tma<SL>() ? kVariants : 2)) return t.variant;
+    if (tune_from_cache(t, key, L.g->vh) && variant_ok<SV, SL>(t.variant, *L.g)) return t.variant;
     DefaultWaitLimit wl;
     // scratch vectors, solver state and partials: no caller data is touched
     const size_t vb = vec_bytes(pv, L.g->vh);
@@ -898,7 +1119,9 @@ static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashAr
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int best = 0;
-    for (int v = 0; v < (has_tma<SL>() ? kVariants : 2); ++v) {
+    for (int v = 0; v < kVariants; ++v) {
+        t.us[v] = 0.f;
+        if (!variant_ok<SV, SL>(v, *L.g)) continue;
         launch_mdagm_variant<SV, SL>(v, s, ls, p, 0.0, cb, st, part, -1, 0, L);  // warm
         cudaEventRecord(e0, L.stream);
         for (int r = 0; r < 3; ++r) launch_mdagm_variant<SV, SL>(v, s, ls, p, 0.0, cb, st, part, -1, 0, L);
@@ -920,8 +1143,9 @@ static int tuned_variant_mdagm(Prec pv, Prec pl, const Launch &L, const DslashAr
 }
 
 // kernel 0: the Dslash (K1), 1: the fused M^dag M kernel (K2); slot: link
-// storage (Prec, or 3 / 4 for 12-real / 13-real Naik links)
-int dslash_variant(int kernel, Prec pv, int slot, float us[3])
+// storage (Prec, or 3 / 4 for 12-real / 13-real Naik links); us receives
+// kVariants timings
+int dslash_variant(int kernel, Prec pv, int slot, float us[4])
 {
     if (slot < 0 || slot > 4) return -1;
     const TuneEntry &t = (kernel == 0 ? g_tune : g_tune_mdagm)[(int)pv][slot];
@@ -962,6 +1186,12 @@ static void prepare_impl(Prec pv, const LinkSet &ls, const Launch &L)
     if constexpr (has_tma<SL>()) {
         (void)tma_grid<SV, SL, 0>(L.g->vh);
         (void)tma_grid<SV, SL, 1>(L.g->vh);
+    }
+    if constexpr (std::is_same<SV, float>::value || std::is_same<SV, double>::value) {
+        if (tile_ok<SV>(*L.g)) {
+            (void)tile_shape<SV, SL, 0>(*L.g);
+            (void)tile_shape<SV, SL, 1>(*L.g);
+        }
     }
 }
 

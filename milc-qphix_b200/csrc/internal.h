@@ -195,7 +195,8 @@ void dslash_prepare(Prec pv, const LinkSet &ls, const Launch &L);
 // variant chosen by the autotuner for kernel 0 (Dslash) or 1 (fused M^dag M)
 // with vectors in pv and link storage `slot` (Prec, or 3 / 4 = 12-real /
 // 13-real Naik links); us = its timings; -1 before the first tuning
-int dslash_variant(int kernel, Prec pv, int slot, float us[3]);
+int dslash_variant(int kernel, Prec pv, int slot, float us[4]);
+constexpr int kDslashVariants = 4;
 // -1: autotuned variants; 0..2: that variant everywhere
 void set_forced_variant(int v);
 // poll limit of the TMA pipeline's waits (< 0: the default)
