@@ -55,7 +55,7 @@ K1_TRAFFIC_PER_SITE_F32 = 264.33e6 / 221184
 K1_TRAFFIC_PER_SITE_R12 = 332.361728e6 / 331776
 DSLASH_FLOPS = 1146
 METRIC = "time to |r|/|b|<1e-10, mixed vs FP64 CG on 1 B200; Dslash HBM GB/s"
-VARIANTS = ["resident-grid", "full-grid", "tma-pipeline"]
+VARIANTS = ["resident-grid", "full-grid", "tma-link-pipeline", "tma-neighbour-tiles"]
 WORKLOAD = ("asqtad mixed-precision CG 24^3x48 m=0.01 tol 1e-10 (FP32 inner with 12-real Naik links, "
             "FP64 reliable updates)")
 
@@ -347,9 +347,8 @@ def run_gpu(args):
     lib.destroy_V("D", vout)
     lib.destroy_V("D", b)
     lib.destroy_L("D", L)
-    tuning = {name: lib.dslash_variant(name) for name in ("single", "single-r12", "double", "half", "half-links")}
-    tuning_k2 = {name: lib.dslash_variant(name, "mdagm")
-                 for name in ("single", "single-r12", "double", "half", "half-links")}
+    tuning = {name: lib.tuning(name) for name in ("single", "single-r12", "double", "half", "half-links")}
+    tuning_k2 = {name: lib.tuning(name, "mdagm") for name in ("single", "single-r12", "double", "half", "half-links")}
     lib.finalize()
     # the north-star size in the same run: 32^3x64, HISQ-shaped links,
     # m = 0.0012 -- FP64 and mixed CG, FP64 and mixed 12-shift multi-shift
@@ -659,8 +658,11 @@ def run_profile_mixed(args):
         lib.destroy_V("D", x)
     lib.destroy_V("D", b)
     lib.destroy_L("D", L)
+    name = {"single": "single-r12" if args.compress else "single"}.get(args.inner, args.inner)
+    lib_tuning = (lib.tuning(name), lib.tuning(name, "mdagm"))
     lib.finalize()
-    print(json.dumps({"mode": "mixed", "inner": args.inner, "solves": res_all}))
+    print(json.dumps({"mode": "mixed", "inner": args.inner, "solves": res_all,
+                      "tuning_k1": lib_tuning[0], "tuning_k2": lib_tuning[1]}))
 
 
 MS_DIMS = (32, 32, 32, 64)

@@ -318,7 +318,7 @@ template <int NV, typename F>
 __device__ __forceinline__ void grid_reduce(double (&v)[NV], double *partials,
                                             unsigned int *counter, F fin, SolverState *split = nullptr)
 {
-    __shared__ double sm[NV][kBlock / 32];
+    __shared__ double sm[NV][32];  // one slot per warp, any block size up to 1024
     __shared__ bool am_last;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nw = blockDim.x >> 5;

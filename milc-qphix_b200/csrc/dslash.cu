@@ -840,8 +840,9 @@ template <typename SL>
 constexpr bool has_tma() { return !std::is_same<SL, Recon12>::value && !std::is_same<SL, Recon13>::value; }
 
 // the tile variant stages FP32 or FP64 vectors; nine planes must fit the
-// 227 KB of shared memory a CTA may have
-constexpr size_t kMaxDynSmem = 232448;
+// 227 KB of shared memory a CTA may have, beside the kernel's static shared
+// memory (the grid reduction's, at most 1 KB)
+constexpr size_t kMaxDynSmem = 232448 - 1024;
 template <typename SV>
 static bool tile_ok(const Geom &g)
 {
@@ -868,15 +869,21 @@ struct TileShape {
 template <typename SV, typename SL, int MODE>
 static TileShape tile_shape(const Geom &g)
 {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_dslash_tile<SV, SL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kMaxDynSmem);
-        attr = true;
-    }
     TileShape t;
     t.block = std::min(kTileMaxThreads, (g.sz + 31) / 32 * 32);
     t.smem = tile_smem_bytes<SV>(g.sz);
+    // the opt-in above 48 KB, for this lattice's planes (static + dynamic
+    // shared memory must stay within the per-CTA limit)
+    static size_t attr = 0;
+    if (t.smem > attr) {
+        const cudaError_t e = cudaFuncSetAttribute(k_dslash_tile<SV, SL, MODE>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();  // not sticky; the launch would fail, so report it here
+            throw std::runtime_error(std::string("tile Dslash: cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        }
+        attr = t.smem;
+    }
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
