@@ -350,6 +350,11 @@ struct FinMsResidual {
             st->ms_ru = 1;
             stop_run(st, gate);
         }
+        // deferred shift updates: this iteration takes the segment's last slot
+        if (st->ms_seg_cap > 0 && st->iteration - st->ms_seg_start >= st->ms_seg_cap) {
+            st->ms_seg_full = 1;
+            stop_run(st, gate);
+        }
         if (st->iteration >= st->max_cg || run_guard(st)) stop_run(st, gate);
     }
 };
@@ -424,6 +429,123 @@ k_ms_update(VecBlock *xs, VecBlock *ps, VecView<S> r, int n, SolverState *st, in
                 p[i] = tt + ak * p[i];
             }
             pk.store(j, p);
+        }
+    }
+}
+
+// ------------------------------------ multi-shift, deferred shift updates --
+// The shifted directions and solutions are linear combinations of the base
+// residuals: p_k(t+1) = z_k r(t+1) + a_k p_k(t), x_k += b_k p_k(t).  Instead
+// of updating 2n vectors every iteration, an iteration stores its residual
+// (the vector the updates would read) and the scalars they would use; the
+// host expands the recurrences into coefficients and k_ms_flush applies them
+// once per segment in FP64, so a segment rounds p_k once instead of every
+// iteration.  The base direction is the Dslash input and is updated here,
+// with the arithmetic of k_ms_update (its iterations are unchanged).
+__global__ void __launch_bounds__(kBlock)
+k_ms_defer(VecView<float> p_low, VecView<float> r, float2 *hist, MsHistEntry *hs, int n, SolverState *st, int gate)
+{
+    if (gated_off(st, gate)) return;
+    const int it = st->iteration;
+    const bool conv = st->converged;
+    const int slot = it - st->ms_seg_start - 1;
+    // the stop test of the residual kernel keeps slot < ms_seg_cap; a slot
+    // outside the buffer is reported and not written
+    if (slot < 0 || slot >= st->ms_seg_cap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            st->error = 3;
+            stop_run(st, gate);
+        }
+        return;
+    }
+    const int jl = st->j_low;
+    const int nn = st->num_now;
+    if (blockIdx.x == 0) {
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            MsHistEntry e;
+            e.b = st->beta_i[k];
+            e.a = st->alpha[k];
+            e.z = st->zeta_ip1[k];
+            const int sd = st->shift_done_at[k];
+            e.upd = k >= nn || sd < it ? 0 : (1 | (!conv && sd != it ? 2 : 0));
+            hs[(size_t)slot * n + k] = e;
+        }
+    }
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= r.vh) return;
+    float rv[6];
+    r.load_cg(j, rv);
+    VecView<float> h{hist + (size_t)slot * 3 * r.vh, r.vh};
+    h.store(j, rv);
+    if (!conv) {
+        float p[6];
+        p_low.load_cg(j, p);
+        const float ak = (float)st->alpha[jl];
+        const double zk = st->zeta_ip1[jl];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const float tt = (float)((double)rv[i] * zk);
+            p[i] = tt + ak * p[i];
+        }
+        p_low.store(j, p);
+    }
+}
+
+// One thread per complex number of the parity block; NS jobs per pass over
+// the stored residuals, FP64 accumulation; the pass's coefficients are read
+// from shared memory.  p0s: the directions at the start of the segment (the
+// base direction's copy, the other shifts' own vectors, which ps overwrites).
+template <int NS>
+__global__ void __launch_bounds__(kBlock)
+k_ms_flush(const float2 *hist, int m, const double *coef, const int *jobs, int njobs, VecBlock *xs,
+           const VecBlock *p0s, VecBlock *ps, int n3)
+{
+    extern __shared__ double sc[];  // [NS][2 (m + 1)]
+    const int stride = 2 * (m + 1);
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int k0 = 0; k0 < njobs; k0 += NS) {
+        const int nj = min(NS, njobs - k0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nj * stride; i += blockDim.x) sc[i] = coef[(size_t)k0 * stride + i];
+        __syncthreads();
+        if (e >= n3) continue;
+        double ax[NS][2], ap[NS][2];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            if (q >= nj) break;
+            const int s = jobs[k0 + q] & 0xffff;
+            const float2 p0 = static_cast<const float2 *>(p0s[s].data)[e];
+            const double *c = sc + q * stride;
+            ax[q][0] = c[0] * p0.x;
+            ax[q][1] = c[0] * p0.y;
+            ap[q][0] = c[m + 1] * p0.x;
+            ap[q][1] = c[m + 1] * p0.y;
+        }
+        for (int t = 0; t < m; ++t) {
+            const float2 hv = __ldcs(hist + (size_t)t * n3 + e);
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+                if (q >= nj) break;
+                const double *c = sc + q * stride;
+                const double cx = c[1 + t], cp = c[m + 2 + t];
+                ax[q][0] = fma(cx, (double)hv.x, ax[q][0]);
+                ax[q][1] = fma(cx, (double)hv.y, ax[q][1]);
+                ap[q][0] = fma(cp, (double)hv.x, ap[q][0]);
+                ap[q][1] = fma(cp, (double)hv.y, ap[q][1]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            if (q >= nj) break;
+            const int jb = jobs[k0 + q];
+            const int s = jb & 0xffff;
+            if (jb >> 16 & 1) {
+                double2 *x = static_cast<double2 *>(xs[s].data) + e;
+                const double2 xv = *x;
+                *x = make_double2(xv.x + ax[q][0], xv.y + ax[q][1]);
+            }
+            if (jb >> 17 & 1)
+                static_cast<float2 *>(ps[s].data)[e] = make_float2((float)ap[q][0], (float)ap[q][1]);
         }
     }
 }
@@ -620,6 +742,25 @@ void ms_update(Prec p, const Launch &L, Prec xprec, VecBlock *x, VecBlock *pv, V
         k_ms_update<float, float><<<grid, kBlock, 0, L.stream>>>(x, pv, view<float>(r, vh), n, st, gate);
     else if (xprec == Prec::Single && p == Prec::Half)
         k_ms_update<__half, float><<<grid, kBlock, 0, L.stream>>>(x, pv, view<__half>(r, vh), n, st, gate);
+}
+
+void ms_defer(const Launch &L, VecBlock p_low, VecBlock r, VecBlock hist, MsHistEntry *hist_s, int n,
+              SolverState *st, int gate)
+{
+    const int vh = L.g->vh;
+    k_ms_defer<<<grid_for(vh), kBlock, 0, L.stream>>>(view<float>(p_low, vh), view<float>(r, vh),
+                                                       static_cast<float2 *>(hist.data), hist_s, n, st, gate);
+}
+
+void ms_flush(const Launch &L, VecBlock hist, int m, const double *coef, const int *jobs, int njobs,
+              VecBlock *x, const VecBlock *p0, VecBlock *p)
+{
+    constexpr int NS = 8;
+    static_assert(sizeof(double) * NS * 2 * (kMsSegMax + 1) <= 48 * 1024, "flush coefficients exceed 48 KB");
+    const int n3 = 3 * L.g->vh;
+    const size_t smem = sizeof(double) * NS * 2 * (m + 1);
+    k_ms_flush<NS><<<grid_for(n3), kBlock, smem, L.stream>>>(static_cast<const float2 *>(hist.data), m, coef, jobs,
+                                                            njobs, x, p0, p, n3);
 }
 
 template <typename S>

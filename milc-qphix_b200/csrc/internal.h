@@ -153,6 +153,13 @@ struct SolverState {
     // the device loop stopped for it
     double ms_delta2;
     int ms_ru;
+    // mixed multi-shift, deferred shift updates (ms_seg_cap > 0): iteration
+    // it of the segment that began after iteration ms_seg_start stores its
+    // residual and scalars in slot it - ms_seg_start - 1; the device loop
+    // stops (ms_seg_full) when the last of the ms_seg_cap slots is taken
+    int ms_seg_start;
+    int ms_seg_cap;
+    int ms_seg_full;
     // domain decomposition: this GPU's totals of the last split reduction,
     // summed in place over the GPUs before k_dd_fin reads them
     double dd_red[4];
@@ -220,6 +227,27 @@ void ms_residual(Prec p, const Launch &L, VecBlock r, VecBlock ttt, SolverState 
 // multi-shift: update_pm / update_dest for all active shifts in one pass
 void ms_update(Prec p, const Launch &L, Prec xprec, VecBlock *x, VecBlock *pv, VecBlock r,
                int n, SolverState *st, int gate);
+// One iteration's scalars of one shift, as the vector updates would use them:
+// x += b p (upd bit 0), then p = z r + a p (upd bit 1).
+struct MsHistEntry {
+    double b, a, z;
+    int upd;
+};
+constexpr int kMsSegMax = 256;  // iterations of one deferred segment at most
+// multi-shift with deferred shift updates (FP32 Krylov vectors): only the
+// base direction is updated, p_low = z r + a p_low; r is stored in the
+// iteration's slot of `hist` (FP32 parity blocks, slot s at s * 3 Vh
+// complex numbers) and every shift's scalars in hist_s[slot * n + k]
+void ms_defer(const Launch &L, VecBlock p_low, VecBlock r, VecBlock hist, MsHistEntry *hist_s, int n,
+              SolverState *st, int gate);
+// End of a deferred segment of m iterations.  For every job k (jobs[k] =
+// shift | do_x << 16 | do_p << 17), with c = coef + k * 2 (m + 1) and p0_s
+// the shift's direction at the start of the segment:
+//   x_s += c[0] p0_s + sum_t c[1 + t] hist_t       (x FP64)
+//   p_s  = c[m+1] p0_s + sum_t c[m+2+t] hist_t     (p FP32)
+// (x, p0, p: device arrays indexed by shift)
+void ms_flush(const Launch &L, VecBlock hist, int m, const double *coef, const int *jobs, int njobs,
+              VecBlock *x, const VecBlock *p0, VecBlock *p);
 
 // elementwise helpers
 void vec_copy(Prec dst_p, VecBlock dst, Prec src_p, VecBlock src, const Launch &L);

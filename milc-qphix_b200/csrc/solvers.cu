@@ -9,7 +9,9 @@
 // chunk that overshoots costs a few empty launches, never extra arithmetic,
 // and the sequence of arithmetic is exactly the reference's.
 #include <cmath>
+#include <cstdlib>
 #include <functional>
+#include <memory>
 
 #include "context.h"
 #include "device_common.cuh"
@@ -101,6 +103,9 @@ struct TimedLaunches {
 // and ends the run; the call returns QPHIX_FAIL with this message.
 [[noreturn]] void breakdown(const char *who, int code, int iteration)
 {
+    if (code == 3)
+        throw Error(std::string(who) + ": internal error at iteration " + std::to_string(iteration) +
+                    " (deferred multi-shift update outside its segment)");
     throw Error(std::string(who) + ": CG breakdown at iteration " + std::to_string(iteration) +
                 (code == 2 ? " (p.Ap is zero or not finite)" : " (the residual is not finite)"));
 }
@@ -615,6 +620,148 @@ struct MsPass {
     double rsq = 0, source_norm = 0;
 };
 
+// Deferred shift updates of the mixed multi-shift (FP32 Krylov vectors).
+// A segment runs m iterations that store their residuals r(t) (slot t: the
+// residual after iteration t, which that iteration's direction updates read)
+// and every shift's scalars; no shifted vector is touched.  At the end of
+// the segment (a reliable update of the base, a full buffer, convergence)
+// the recurrences
+//   x += b_t p(t)          (upd bit 0)
+//   p(t+1) = z_t r(t) + a_t p(t)   (upd bit 1)
+// are expanded on the host: p(t) = P_t p(0) + sum_{u<t} D_t[u] r(u), so
+//   x += GX p(0) + sum_u CX[u] r(u),   p(m) = P_m p(0) + sum_u D_m[u] r(u),
+// with GX = sum_t b_t P_t and CX[u] = sum_{t>u} b_t D_t[u], and k_ms_flush
+// applies them in FP64.  The base direction (the Dslash input) is updated
+// every iteration as before; its solution is deferred like the others, from
+// a copy of the direction taken at the start of the segment.
+class MsDeferred {
+public:
+    // nullptr when fewer than kMinSlots residuals fit in the memory budget
+    static std::unique_ptr<MsDeferred> make(int n, int j_low, const std::vector<VecBlock> &pm)
+    {
+        Context &c = ctx();
+        const size_t slot = vec_bytes(Prec::Single, c.g.vh);
+        size_t free_b = 0, total_b = 0;
+        QB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t budget = std::min(kBudgetBytes, free_b / 4);
+        size_t fit = std::min<size_t>(budget / slot, kMsSegMax);
+        // QPHIX_B200_MS_SEGMENT: fewer iterations per segment (at least
+        // kMinSlots), to exercise the segment hand-over on small lattices
+        if (const char *e = std::getenv("QPHIX_B200_MS_SEGMENT"))
+            fit = std::min<size_t>(fit, (size_t)std::max(std::atoi(e), kMinSlots));
+        if (fit < (size_t)kMinSlots) return nullptr;
+        return std::unique_ptr<MsDeferred>(new MsDeferred(n, j_low, pm, (int)fit));
+    }
+    ~MsDeferred()
+    {
+        dev_free(hist_.data);
+        dev_free(d_hist_);
+        dev_free(d_coef_);
+        dev_free(d_jobs_);
+        dev_free(d_p0_);
+        free_vec(p_low0_);
+    }
+    VecBlock hist() const { return hist_; }
+    MsHistEntry *hist_scalars() const { return d_hist_; }
+
+    // a segment begins after the current iteration, from the current base direction
+    void begin(SolverState &S, const Launch &L)
+    {
+        S.ms_seg_cap = cap_;
+        S.ms_seg_start = S.iteration;
+        S.ms_seg_full = 0;
+        vec_copy(Prec::Single, p_low0_, Prec::Single, pm_[j_low_], L);
+    }
+
+    // apply the segment's updates to the solutions d_x (FP64) and the shifted
+    // directions d_p (FP32), then begin the next segment
+    void flush(SolverState &S, VecBlock *d_x, VecBlock *d_p, const Launch &L)
+    {
+        const int m = S.iteration - S.ms_seg_start;
+        if (m < 0 || m > cap_) throw Error("invert_multi: deferred segment out of range");
+        if (m > 0) {
+            h_hist_.resize((size_t)m * n_);
+            QB_CUDA(cudaMemcpyAsync(h_hist_.data(), d_hist_, sizeof(MsHistEntry) * h_hist_.size(),
+                                    cudaMemcpyDeviceToHost, L.stream));
+            QB_CUDA(cudaStreamSynchronize(L.stream));
+            const int stride = 2 * (m + 1);
+            h_coef_.clear();
+            h_jobs_.clear();
+            std::vector<double> D(m), CX(m);
+            for (int s = 0; s < n_; ++s) {
+                double P = 1.0, GX = 0.0;
+                std::fill(D.begin(), D.end(), 0.0);
+                std::fill(CX.begin(), CX.end(), 0.0);
+                bool any_x = false, any_p = false;
+                for (int t = 0; t < m; ++t) {
+                    const MsHistEntry &e = h_hist_[(size_t)t * n_ + s];
+                    if (e.upd & 1) {
+                        any_x = true;
+                        GX += e.b * P;
+                        for (int u = 0; u < t; ++u) CX[u] += e.b * D[u];
+                    }
+                    if (e.upd & 2) {
+                        any_p = true;
+                        P *= e.a;
+                        for (int u = 0; u < t; ++u) D[u] *= e.a;
+                        D[t] = e.z;
+                    }
+                }
+                const bool do_x = any_x, do_p = any_p && s != j_low_;
+                if (!do_x && !do_p) continue;
+                h_jobs_.push_back(s | (do_x ? 1 << 16 : 0) | (do_p ? 1 << 17 : 0));
+                h_coef_.push_back(GX);
+                h_coef_.insert(h_coef_.end(), CX.begin(), CX.end());
+                h_coef_.push_back(P);
+                h_coef_.insert(h_coef_.end(), D.begin(), D.end());
+            }
+            if (!h_jobs_.empty()) {
+                if ((int)h_coef_.size() != stride * (int)h_jobs_.size())
+                    throw Error("invert_multi: deferred coefficient table size");
+                QB_CUDA(cudaMemcpyAsync(d_coef_, h_coef_.data(), sizeof(double) * h_coef_.size(),
+                                        cudaMemcpyHostToDevice, L.stream));
+                QB_CUDA(cudaMemcpyAsync(d_jobs_, h_jobs_.data(), sizeof(int) * h_jobs_.size(),
+                                        cudaMemcpyHostToDevice, L.stream));
+                ms_flush(L, hist_, m, d_coef_, d_jobs_, (int)h_jobs_.size(), d_x, d_p0_, d_p);
+                // the host vectors are reused by the next flush
+                QB_CUDA(cudaStreamSynchronize(L.stream));
+            }
+        }
+        begin(S, L);
+    }
+
+private:
+    static constexpr size_t kBudgetBytes = size_t(2) << 30;
+    static constexpr int kMinSlots = 16;
+
+    MsDeferred(int n, int j_low, const std::vector<VecBlock> &pm, int cap)
+        : cap_(cap), n_(n), j_low_(j_low), pm_(pm)
+    {
+        Context &c = ctx();
+        hist_.data = dev_alloc(vec_bytes(Prec::Single, c.g.vh) * cap_);
+        d_hist_ = static_cast<MsHistEntry *>(dev_alloc(sizeof(MsHistEntry) * cap_ * n_));
+        d_coef_ = static_cast<double *>(dev_alloc(sizeof(double) * 2 * (cap_ + 1) * n_));
+        d_jobs_ = static_cast<int *>(dev_alloc(sizeof(int) * n_));
+        d_p0_ = static_cast<VecBlock *>(dev_alloc(sizeof(VecBlock) * n_));
+        p_low0_ = alloc_vec(Prec::Single);
+        std::vector<VecBlock> p0(pm);
+        p0[j_low_] = p_low0_;
+        QB_CUDA(cudaMemcpyAsync(d_p0_, p0.data(), sizeof(VecBlock) * n_, cudaMemcpyHostToDevice, c.stream));
+        QB_CUDA(cudaStreamSynchronize(c.stream));
+    }
+
+    int cap_, n_, j_low_;
+    std::vector<VecBlock> pm_;
+    VecBlock hist_, p_low0_;
+    MsHistEntry *d_hist_ = nullptr;
+    double *d_coef_ = nullptr;
+    int *d_jobs_ = nullptr;
+    VecBlock *d_p0_ = nullptr;
+    std::vector<MsHistEntry> h_hist_;
+    std::vector<double> h_coef_;
+    std::vector<int> h_jobs_;
+};
+
 // one parity pass of the multi-shift recurrence; x[] in precision xp, the
 // Krylov vectors in precision p
 MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<VecBlock> &x,
@@ -623,7 +770,7 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
                double offset_low, double rsqmin, int max_cg, bool single, TimedLaunches &tl,
                double shift_rsqmin, double ru_delta2 = 0.0,
                const std::function<double()> &reliable_update = std::function<double()>(),
-               double ru_rsqmin = 0.0)
+               double ru_rsqmin = 0.0, MsDeferred *df = nullptr)
 {
     Context &c = ctx();
     const Launch L = c.launch();
@@ -662,6 +809,8 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
     for (int j = 0; j < n; ++j) S.shift_done_at[j] = INT_MAX;
     S.ms_delta2 = reliable_update ? ru_delta2 : 0.0;
     S.rsq_ru = out.source_norm;
+    S.ms_seg_cap = 0;
+    if (df) df->begin(S, L);
     const double m4 = round_prec(-1.0 * offset_low, single);
     double size_prev = out.rsq;
     dslash_prepare(p, ls, L);
@@ -676,7 +825,8 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
                     dslash_mdagm_dot(p, L, ttt, tmp, ls, pm[j_low], m4, parity, c.d_state, c.d_partials, k, 1);
                 });
                 ms_residual(p, L, resid, ttt, c.d_state, c.d_partials, k);
-                ms_update(p, L, xp, d_x, d_p, resid, n, c.d_state, k);
+                if (df) ms_defer(L, pm[j_low], resid, df->hist(), df->hist_scalars(), n, c.d_state, k);
+                else ms_update(p, L, xp, d_x, d_p, resid, n, c.d_state, k);
             },
             [&](int chunk, int it0) {
                 const int m = next_chunk(chunk, size_prev, S.rsq, S.iteration - it0, S.rsqstop, max_cg - S.iteration);
@@ -685,7 +835,11 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
             },
             tl, max_cg + 1);
         if (S.error) breakdown("asqtad_invert_multi", S.error, S.iteration);
-        if (S.converged || !S.ms_ru || S.iteration >= max_cg) break;
+        const bool seg_full = S.ms_seg_full != 0;
+        if (df) df->flush(S, d_x, d_p, L);  // (and begins the next segment)
+        if (S.converged || S.iteration >= max_cg) break;
+        if (seg_full && !S.ms_ru) continue;  // a full segment, flushed: carry on
+        if (!S.ms_ru) break;
         // reliable update of the base shift: r = b - (A + sigma_low) x_low in FP64
         const double prev = S.rsq_ru;
         const double rsq = reliable_update();
@@ -856,11 +1010,18 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
     for (int j = 0; j < n; ++j)
         if (j != j_low) shifts[j] -= shifts[j_low];
     for (int j = 0; j < n; ++j) c.h_state->finished[j] = 0;
-    // With base reliable updates the shifted solutions accumulate between
-    // updates in FP32 partial sums y_j (24 instead of 48 bytes read and
-    // written per site and shift each iteration); every reliable update and
-    // the end of the recurrence add them into the FP64 x_j.
-    const bool partial = base_ru_on;
+    // FP32 Krylov vectors: the shifted solutions and directions are updated
+    // once per segment from the stored base residuals (MsDeferred), so an
+    // iteration moves the bytes of one CG iteration whatever the number of
+    // shifts, and each shifted direction is rounded to FP32 once per segment
+    // instead of once per iteration.
+    std::unique_ptr<MsDeferred> df;
+    if (ps == Prec::Single) df = MsDeferred::make(n, j_low, pm);
+    // Otherwise, with base reliable updates, the shifted solutions accumulate
+    // between updates in FP32 partial sums y_j (24 instead of 48 bytes read
+    // and written per site and shift each iteration); every reliable update
+    // and the end of the recurrence add them into the FP64 x_j.
+    const bool partial = base_ru_on && !df;
     std::vector<VecBlock> y(partial ? n : 0);
     for (auto &v : y) v = ws.get(Prec::Single);
     VecBlock *d_x = static_cast<VecBlock *>(dev_alloc(sizeof(VecBlock) * n));
@@ -902,7 +1063,8 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
         MsPass r = ms_pass(ps, partial ? Prec::Single : Prec::Double, lss, src_s, partial ? y : x, pm, ttt, tmp,
                            resid, d_x, d_p, parity, shifts, j_low, offset_low, rsq_sloppy, max_cg, false, tl,
                            floor * kShiftStopFactor, c.reliable_delta * c.reliable_delta,
-                           base_ru_on ? std::function<double()>(base_ru) : std::function<double()>(), target);
+                           base_ru_on ? std::function<double()>(base_ru) : std::function<double()>(), target,
+                           df.get());
         if (partial) flush(c.launch());
         rus += r.reliable_updates;
         total += r.iteration;

@@ -95,6 +95,34 @@ def test_multishift_mixed_every_shift_converges(gpu, inner):
         assert orc.true_residual(dims, links, x, src, m, "even") < 1e-20
 
 
+def test_multishift_mixed_short_segments(gpu, monkeypatch):
+    """FP32 Krylov vectors: the shifted solutions and directions are rebuilt
+    from the stored base residuals once per segment.  Segments of 16
+    iterations (QPHIX_B200_MS_SEGMENT) hand over many times inside one
+    recurrence; the solutions still meet every shift's tolerance against the
+    oracle, and the sloppy recurrence takes the iterations of the run with
+    the default segments (the base direction is updated identically; only
+    the summation order of the deferred solutions differs)."""
+    dims = (8, 8, 8, 8)
+    lib = gpu.use(dims)
+    links = fields(dims)
+    src = synthetic.gaussian_source(dims, seed=2002, parity="even")
+    masses = _masses(0.01, 6)
+    lib.set_inner_precision("single")
+    try:
+        it0, xs0, res0, _ = _multi(lib, "D", links, src, masses, "even", max_iter=4000, nrestart=5, resid=1e-20)
+        monkeypatch.setenv("QPHIX_B200_MS_SEGMENT", "16")
+        it1, xs1, res1, info = _multi(lib, "D", links, src, masses, "even", max_iter=4000, nrestart=5, resid=1e-20)
+    finally:
+        lib.set_inner_precision("double")
+    assert info.status == 0
+    assert it0 > 3 * 16, "the recurrence must span several segments"
+    assert abs(it1 - it0) <= 2, (it0, it1)
+    for m, x, r in zip(masses, xs1, res1):
+        assert r.final_rsq < 1e-20
+        assert orc.true_residual(dims, links, x, src, m, "even") < 1e-20
+
+
 def _crossed(v, V):
     """The reference's multi-shift with EVENODD solves the even half with the
     odd-checkerboard operator and then the odd half with the even one
