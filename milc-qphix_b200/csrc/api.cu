@@ -384,6 +384,12 @@ const LinkSet &single_inner_links(QPHIX_D3_FermionLinksAsqtad *H)
     return H->sloppy_recon.valid ? H->sloppy_recon : single_links(H);
 }
 
+bool refine_batched_env()
+{
+    const char *e = std::getenv("QPHIX_B200_MS_REFINE");
+    return e && std::strcmp(e, "batched") == 0;
+}
+
 SloppyCfg sloppy_cfg(QPHIX_D3_FermionLinksAsqtad *H, int mode)
 {
     switch (mode) {
@@ -586,7 +592,23 @@ int asqtad_invert_multi(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_inv
                 iters = multishift_reference(Prec::Double, H->links, a);
             } else {
                 const SloppyCfg s = sloppy_cfg(H, c.inner_mode);
-                iters = multishift_mixed(s.vec, H->links, *s.links, s.up, a);
+                // FP32 inner vectors on one GPU: the shifts are refined
+                // together by the batched solver, on the 18-real FP32 links
+                const LinkSet *l32 =
+                    s.vec == Prec::Single && !c.halo.on && refine_batched_env() ? &single_links(H) : nullptr;
+                // The per-shift refinements run on the sloppy recurrence's
+                // operator.  QPHIX_B200_MS_REFINE_STORAGE=half-links or half
+                // runs them on 16-bit links (a fifth less time at 32^3x64
+                // with the same iterations, but five times the iterations
+                // of the lightest refined shift at 24^3x48, m = 0.0012:
+                // the link rounding times its condition number is near 1).
+                const char *e = std::getenv("QPHIX_B200_MS_REFINE_STORAGE");
+                const std::string rs = e ? e : "single";
+                RefineOp rop{s.vec, s.links, s.up};
+                if (rs == "half-links") rop = {Prec::Single, &half_links(H), &single_inner_links(H)};
+                else if (rs == "half") rop = {Prec::Half, &half_links(H), &single_inner_links(H)};
+                else if (rs != "single") throw Error("QPHIX_B200_MS_REFINE_STORAGE: single, half-links or half");
+                iters = multishift_mixed(s.vec, H->links, *s.links, s.up, a, l32, &rop);
                 c.stats.links_compressed = s.links->recon;
             }
         } else {

@@ -787,6 +787,20 @@ __global__ void k_b_to_raw(double *raw, const double2 *f, long long voff, int vh
     }
 }
 
+// FP64 parity block of the library's vector layout (complex e = c*Vh + j)
+// <-> slot r of a segment
+__global__ void k_b_from_blk(double2 *f, long long voff, int n3, int nrhs, int r, const double2 *v)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n3) f[voff + (size_t)e * nrhs + r] = v[e];
+}
+
+__global__ void k_b_to_blk(double2 *v, const double2 *f, long long voff, int n3, int nrhs, int r)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n3) v[e] = f[voff + (size_t)e * nrhs + r];
+}
+
 }  // namespace qb
 
 // FP64 <-> FP32 copy of a whole batched field (n complex numbers)
@@ -1262,6 +1276,56 @@ void free_batch_links(QPHIX_B200_Batch &B)
 }
 
 }  // namespace
+
+// Refinement of several systems (4 m_k^2 - D D) x_k = b on the library's own
+// lattice, one batched solve: x_k (FP64 parity blocks) are the initial
+// guesses and receive the solutions; each system stops at its own squared
+// relative tolerance tol_k on the FP64 true residual.  l32 is the 18-real
+// FP32 copy of l64 (the batched kernels' link format).
+void batch_refine(const LinkSet &l64, const LinkSet &l32, VecBlock b, const std::vector<VecBlock> &x,
+                  const std::vector<double> &mass, const std::vector<double> &tol, int parity, int iter_cap,
+                  std::vector<RefineResult> &out)
+{
+    Context &c = ctx();
+    const int nsys = (int)x.size();
+    if (nsys < 1 || nsys > kBMaxSys) throw Error("batch_refine: 1.." + std::to_string(kBMaxSys) + " systems");
+    std::vector<int> lat(nsys, 0), slot_of;
+    const std::vector<SegPlan> plan = plan_segments(1, nsys, lat.data(), slot_of);
+    const std::vector<LatRef> lats{LatRef{&c.g, &l64, &l32}};
+    std::vector<double> m4(nsys), rs(nsys);
+    for (int k = 0; k < nsys; ++k) {
+        m4[slot_of[k]] = 4.0 * mass[k] * mass[k];
+        rs[slot_of[k]] = tol[k];
+    }
+    out.assign(nsys, RefineResult{});
+    const int n3 = 3 * c.g.vh;
+    const Stats keep = c.stats;  // run_batch reports into the context's stats
+    run_batch(
+        lats, plan, nsys, m4.data(), rs.data(), parity, iter_cap,
+        [&](const BFields &f, const BTable &vt, BatchMem &) {
+            for (size_t s = 0; s < plan.size(); ++s)
+                for (int r = 0; r < plan[s].nrhs; ++r) {
+                    const int k = plan[s].user[r];
+                    k_b_from_blk<<<grid_for(n3), kBlock, 0, c.stream>>>(f.b, vt.seg[s].voff, n3, plan[s].nrhs, r,
+                                                                       static_cast<const double2 *>(b.data));
+                    k_b_from_blk<<<grid_for(n3), kBlock, 0, c.stream>>>(f.x, vt.seg[s].voff, n3, plan[s].nrhs, r,
+                                                                       static_cast<const double2 *>(x[k].data));
+                }
+        },
+        [&](const BFields &f, const BTable &vt, const BState *h, BatchMem &) {
+            for (size_t s = 0; s < plan.size(); ++s)
+                for (int r = 0; r < plan[s].nrhs; ++r) {
+                    const int k = plan[s].user[r];
+                    const BSys &y = h->sys[plan[s].sys0 + r];
+                    k_b_to_blk<<<grid_for(n3), kBlock, 0, c.stream>>>(static_cast<double2 *>(x[k].data), f.x,
+                                                                     vt.seg[s].voff, n3, plan[s].nrhs, r);
+                    out[k].true_rsq_rel = y.bnorm > 0 ? y.true_rsq / y.bnorm : 0.0;
+                    out[k].iterations = y.iterations;
+                    out[k].reliable_updates = y.reliable_updates;
+                }
+        });
+    c.stats = keep;
+}
 
 static QPHIX_B200_Batch *batch_create(int nlat, const int *latsize, double *const *fat, double *const *lng,
                                       double *const *fatback, double *const *lngback)

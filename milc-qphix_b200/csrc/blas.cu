@@ -491,62 +491,73 @@ k_ms_defer(VecView<float> p_low, VecView<float> r, float2 *hist, MsHistEntry *hs
     }
 }
 
-// One thread per complex number of the parity block; NS jobs per pass over
-// the stored residuals, FP64 accumulation; the pass's coefficients are read
-// from shared memory.  p0s: the directions at the start of the segment (the
-// base direction's copy, the other shifts' own vectors, which ps overwrites).
-template <int NS>
-__global__ void __launch_bounds__(kBlock)
+// One thread per complex number of the parity block and kFlushJobs jobs;
+// the job groups of a range of numbers are adjacent blocks, so the stored
+// residuals come from DRAM once per flush and from L2 for the other
+// groups.  FP64 accumulation, kFlushDepth slots loaded ahead of their
+// arithmetic (about 48 KB in flight per SM at three blocks per SM).
+// Coefficients per job: {GX, P, (CX[t], D[t])...}, one uniform 16-byte load
+// per slot and job.
+constexpr int kFlushJobs = 4;
+constexpr int kFlushDepth = 8;
+__global__ void __launch_bounds__(kBlock, 3)
 k_ms_flush(const float2 *hist, int m, const double *coef, const int *jobs, int njobs, VecBlock *xs,
            const VecBlock *p0s, VecBlock *ps, int n3)
 {
-    extern __shared__ double sc[];  // [NS][2 (m + 1)]
+    const int groups = (njobs + kFlushJobs - 1) / kFlushJobs;
+    const int k0 = (int)(blockIdx.x % groups) * kFlushJobs;
+    const int e = (int)(blockIdx.x / groups) * kBlock + threadIdx.x;
+    if (e >= n3) return;
+    const int nj = min(kFlushJobs, njobs - k0);
     const int stride = 2 * (m + 1);
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int k0 = 0; k0 < njobs; k0 += NS) {
-        const int nj = min(NS, njobs - k0);
-        __syncthreads();
-        for (int i = threadIdx.x; i < nj * stride; i += blockDim.x) sc[i] = coef[(size_t)k0 * stride + i];
-        __syncthreads();
-        if (e >= n3) continue;
-        double ax[NS][2], ap[NS][2];
+    const double2 *cf = reinterpret_cast<const double2 *>(coef + (size_t)k0 * stride);
+    const int cstride = m + 1;  // in double2
+    double ax[kFlushJobs][2], ap[kFlushJobs][2];
 #pragma unroll
-        for (int q = 0; q < NS; ++q) {
-            if (q >= nj) break;
+    for (int q = 0; q < kFlushJobs; ++q) {
+        ax[q][0] = ax[q][1] = ap[q][0] = ap[q][1] = 0.0;
+        if (q < nj) {
             const int s = jobs[k0 + q] & 0xffff;
             const float2 p0 = static_cast<const float2 *>(p0s[s].data)[e];
-            const double *c = sc + q * stride;
-            ax[q][0] = c[0] * p0.x;
-            ax[q][1] = c[0] * p0.y;
-            ap[q][0] = c[m + 1] * p0.x;
-            ap[q][1] = c[m + 1] * p0.y;
+            const double2 g = __ldg(cf + q * cstride);
+            ax[q][0] = g.x * p0.x;
+            ax[q][1] = g.x * p0.y;
+            ap[q][0] = g.y * p0.x;
+            ap[q][1] = g.y * p0.y;
         }
-        for (int t = 0; t < m; ++t) {
-            const float2 hv = __ldcs(hist + (size_t)t * n3 + e);
+    }
+    auto step = [&](int t, float2 hv) {
 #pragma unroll
-            for (int q = 0; q < NS; ++q) {
-                if (q >= nj) break;
-                const double *c = sc + q * stride;
-                const double cx = c[1 + t], cp = c[m + 2 + t];
-                ax[q][0] = fma(cx, (double)hv.x, ax[q][0]);
-                ax[q][1] = fma(cx, (double)hv.y, ax[q][1]);
-                ap[q][0] = fma(cp, (double)hv.x, ap[q][0]);
-                ap[q][1] = fma(cp, (double)hv.y, ap[q][1]);
+        for (int q = 0; q < kFlushJobs; ++q) {
+            if (q < nj) {
+                const double2 cc = __ldg(cf + q * cstride + 1 + t);
+                ax[q][0] = fma(cc.x, (double)hv.x, ax[q][0]);
+                ax[q][1] = fma(cc.x, (double)hv.y, ax[q][1]);
+                ap[q][0] = fma(cc.y, (double)hv.x, ap[q][0]);
+                ap[q][1] = fma(cc.y, (double)hv.y, ap[q][1]);
             }
         }
+    };
+    int t = 0;
+    for (; t + kFlushDepth <= m; t += kFlushDepth) {
+        float2 hv[kFlushDepth];
 #pragma unroll
-        for (int q = 0; q < NS; ++q) {
-            if (q >= nj) break;
-            const int jb = jobs[k0 + q];
-            const int s = jb & 0xffff;
-            if (jb >> 16 & 1) {
-                double2 *x = static_cast<double2 *>(xs[s].data) + e;
-                const double2 xv = *x;
-                *x = make_double2(xv.x + ax[q][0], xv.y + ax[q][1]);
-            }
-            if (jb >> 17 & 1)
-                static_cast<float2 *>(ps[s].data)[e] = make_float2((float)ap[q][0], (float)ap[q][1]);
+        for (int u = 0; u < kFlushDepth; ++u) hv[u] = __ldg(hist + (size_t)(t + u) * n3 + e);
+#pragma unroll
+        for (int u = 0; u < kFlushDepth; ++u) step(t + u, hv[u]);
+    }
+    for (; t < m; ++t) step(t, __ldg(hist + (size_t)t * n3 + e));
+#pragma unroll
+    for (int q = 0; q < kFlushJobs; ++q) {
+        if (q >= nj) break;
+        const int jb = jobs[k0 + q];
+        const int s = jb & 0xffff;
+        if (jb >> 16 & 1) {
+            double2 *x = static_cast<double2 *>(xs[s].data) + e;
+            const double2 xv = *x;
+            *x = make_double2(xv.x + ax[q][0], xv.y + ax[q][1]);
         }
+        if (jb >> 17 & 1) static_cast<float2 *>(ps[s].data)[e] = make_float2((float)ap[q][0], (float)ap[q][1]);
     }
 }
 
@@ -755,12 +766,11 @@ void ms_defer(const Launch &L, VecBlock p_low, VecBlock r, VecBlock hist, MsHist
 void ms_flush(const Launch &L, VecBlock hist, int m, const double *coef, const int *jobs, int njobs,
               VecBlock *x, const VecBlock *p0, VecBlock *p)
 {
-    constexpr int NS = 8;
-    static_assert(sizeof(double) * NS * 2 * (kMsSegMax + 1) <= 48 * 1024, "flush coefficients exceed 48 KB");
     const int n3 = 3 * L.g->vh;
-    const size_t smem = sizeof(double) * NS * 2 * (m + 1);
-    k_ms_flush<NS><<<grid_for(n3), kBlock, smem, L.stream>>>(static_cast<const float2 *>(hist.data), m, coef, jobs,
-                                                            njobs, x, p0, p, n3);
+    const unsigned groups = (njobs + kFlushJobs - 1) / kFlushJobs;
+    const unsigned grid = groups * (unsigned)grid_for(n3);
+    k_ms_flush<<<grid, kBlock, 0, L.stream>>>(static_cast<const float2 *>(hist.data), m, coef, jobs, njobs, x, p0,
+                                              p, n3);
 }
 
 template <typename S>

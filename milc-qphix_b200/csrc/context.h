@@ -238,6 +238,15 @@ struct MultiArgs {
     VecBlock in[2];
 };
 int multishift_reference(Prec p, const LinkSet &ls, MultiArgs &a);
-int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &ls_s, const LinkSet *ls_up, MultiArgs &a);
+// ls32: the 18-real FP32 links for refining all shifts in one batched solve
+// (nullptr: the shifts are refined one after the other); rop: the inner
+// operator of the per-shift refinements (nullptr: the sloppy recurrence's)
+struct RefineOp {
+    Prec vec;
+    const LinkSet *links;
+    const LinkSet *up;
+};
+int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &ls_s, const LinkSet *ls_up, MultiArgs &a,
+                     const LinkSet *ls32 = nullptr, const RefineOp *rop = nullptr);
 
 }  // namespace qb

@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <string>
 #include <type_traits>
+#include <vector>
 
 #include "geometry.cuh"
 
@@ -234,6 +235,18 @@ struct MsHistEntry {
     int upd;
 };
 constexpr int kMsSegMax = 256;  // iterations of one deferred segment at most
+
+// Batched refinement (batch.cu): the systems (4 m_k^2 - D D) x_k = b of the
+// library's lattice in one batched solve from the initial guesses x_k, each
+// to its squared relative tolerance tol_k on the FP64 true residual; l32 is
+// the 18-real FP32 copy of l64.  At most 64 systems.
+struct RefineResult {
+    double true_rsq_rel = 0;
+    int iterations = 0, reliable_updates = 0;
+};
+void batch_refine(const LinkSet &l64, const LinkSet &l32, VecBlock b, const std::vector<VecBlock> &x,
+                  const std::vector<double> &mass, const std::vector<double> &tol, int parity, int iter_cap,
+                  std::vector<RefineResult> &out);
 // multi-shift with deferred shift updates (FP32 Krylov vectors): only the
 // base direction is updated, p_low = z r + a p_low; r is stored in the
 // iteration's slot of `hist` (FP32 parity blocks, slot s at s * 3 Vh
@@ -243,8 +256,8 @@ void ms_defer(const Launch &L, VecBlock p_low, VecBlock r, VecBlock hist, MsHist
 // End of a deferred segment of m iterations.  For every job k (jobs[k] =
 // shift | do_x << 16 | do_p << 17), with c = coef + k * 2 (m + 1) and p0_s
 // the shift's direction at the start of the segment:
-//   x_s += c[0] p0_s + sum_t c[1 + t] hist_t       (x FP64)
-//   p_s  = c[m+1] p0_s + sum_t c[m+2+t] hist_t     (p FP32)
+//   x_s += c[0] p0_s + sum_t c[2 + 2t] hist_t      (x FP64)
+//   p_s  = c[1] p0_s + sum_t c[3 + 2t] hist_t      (p FP32)
 // (x, p0, p: device arrays indexed by shift)
 void ms_flush(const Launch &L, VecBlock hist, int m, const double *coef, const int *jobs, int njobs,
               VecBlock *x, const VecBlock *p0, VecBlock *p);

@@ -10,6 +10,7 @@
 // and the sequence of arithmetic is exactly the reference's.
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <functional>
 #include <memory>
 
@@ -415,6 +416,18 @@ constexpr int kInnerStallWindow = 256;
 constexpr double kShiftStopFactor = 1e-6;
 // reliable-update threshold of the per-shift refinements, relative to the CG's
 constexpr double kRefineDeltaFactor = 0.25;
+// least |r|^2 reduction of one reliable-update cycle of a refinement on
+// 16-bit links before it continues on FP32 links
+constexpr double kRefineEscalate = 20.0;
+// systems of one batched refinement (the batched solver's limit)
+constexpr int kBatchRefineMax = 64;
+// QPHIX_B200_MS_REFINE=batched refines the shifts of a mixed multi-shift in
+// one batched solve instead of one after the other (mixed CG each)
+bool refine_batched()
+{
+    const char *e = std::getenv("QPHIX_B200_MS_REFINE");
+    return e && std::strcmp(e, "batched") == 0;
+}
 
 struct MixedResult {
     double true_rsq_rel = 0;
@@ -425,8 +438,12 @@ struct MixedResult {
 
 // `ls_up`: FP32 links to continue with when a 16-bit inner solve stops
 // converging (see below); may be null.
+// escalate_ratio / escalate_after: a 16-bit inner solve continues in FP32
+// after `escalate_after` reliable updates in a row whose true |r|^2 fell by
+// less than 1 / escalate_ratio (or that an inner stagnation forced)
 MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const LinkSet *ls_up, VecBlock x,
-                       VecBlock b, int parity, double mass, double tol, int max_cg, TimedLaunches &tl)
+                       VecBlock b, int parity, double mass, double tol, int max_cg, TimedLaunches &tl,
+                       double escalate_ratio = 0.25, int escalate_after = 2)
 {
     Context &c = ctx();
     const LinkSet *ls_cur = &lss;
@@ -525,8 +542,8 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
         // that fail to halve the true residual, or that an inner stagnation
         // forced, switch the inner solve to FP32.
         const bool inner_stall = S.ru_stalled != 0;
-        stalled = (rsq > 0.25 * prev_true || inner_stall) ? stalled + 1 : 0;
-        if (stalled >= 2 && (ps == Prec::Half || ls_cur->prec == Prec::Half) && ls_up && ls_up->valid) {
+        stalled = (rsq > escalate_ratio * prev_true || inner_stall) ? stalled + 1 : 0;
+        if (stalled >= escalate_after && (ps == Prec::Half || ls_cur->prec == Prec::Half) && ls_up && ls_up->valid) {
             VecBlock p32 = ws.get(Prec::Single);
             vec_copy(Prec::Single, p32, ps, pv, L);
             pv = p32;
@@ -711,9 +728,11 @@ public:
                 if (!do_x && !do_p) continue;
                 h_jobs_.push_back(s | (do_x ? 1 << 16 : 0) | (do_p ? 1 << 17 : 0));
                 h_coef_.push_back(GX);
-                h_coef_.insert(h_coef_.end(), CX.begin(), CX.end());
                 h_coef_.push_back(P);
-                h_coef_.insert(h_coef_.end(), D.begin(), D.end());
+                for (int u = 0; u < m; ++u) {
+                    h_coef_.push_back(CX[u]);
+                    h_coef_.push_back(D[u]);
+                }
             }
             if (!h_jobs_.empty()) {
                 if ((int)h_coef_.size() != stride * (int)h_jobs_.size())
@@ -816,8 +835,10 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
     dslash_prepare(p, ls, L);
     IterLoop loop;
     int ru_stalls = 0;
+    double t_run = 0, t_flush = 0, t_ru = 0;  // verbose: host-side phase times
     for (;;) {
         S.ms_ru = 0;
+        const double t0 = c.verbose ? wall_seconds() : 0.0;
         loop.run(
             [&](int k) {
                 tl.run(0, k, [&] { dslash_gated(p, L, tmp, pm[j_low], ls, other, c.d_state, k); });
@@ -836,13 +857,22 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
             tl, max_cg + 1);
         if (S.error) breakdown("asqtad_invert_multi", S.error, S.iteration);
         const bool seg_full = S.ms_seg_full != 0;
+        const double t1 = c.verbose ? wall_seconds() : 0.0;
         if (df) df->flush(S, d_x, d_p, L);  // (and begins the next segment)
+        if (c.verbose) {
+            sync_check();
+            const double t2 = wall_seconds();
+            t_run += t1 - t0;
+            t_flush += t2 - t1;
+        }
         if (S.converged || S.iteration >= max_cg) break;
         if (seg_full && !S.ms_ru) continue;  // a full segment, flushed: carry on
         if (!S.ms_ru) break;
         // reliable update of the base shift: r = b - (A + sigma_low) x_low in FP64
         const double prev = S.rsq_ru;
+        const double t3 = c.verbose ? wall_seconds() : 0.0;
         const double rsq = reliable_update();
+        if (c.verbose) t_ru += wall_seconds() - t3;
         require_finite("asqtad_invert_multi", rsq, "the base shift's true residual");
         S.rsq = rsq;
         S.rsq_ru = rsq;
@@ -859,6 +889,9 @@ MsPass ms_pass(Prec p, Prec xp, const LinkSet &ls, VecBlock src, std::vector<Vec
     out.iteration = S.iteration;
     out.converged = S.converged != 0;
     out.rsq = S.rsq;
+    if (c.verbose)
+        std::fprintf(stderr, "qphix_b200 multi-shift pass: device loops %.1f ms, segment flushes %.1f ms, "
+                             "reliable updates %.1f ms\n", 1e3 * t_run, 1e3 * t_flush, 1e3 * t_ru);
     if (c.verbose) {
         std::fprintf(stderr, "qphix_b200 multi-shift: iter %d converged %d rsq/src %.3e active %d pkp %.3e\n",
                      S.iteration, out.converged, S.rsq / out.source_norm, S.num_now, S.pkp);
@@ -971,7 +1004,8 @@ int multishift_reference(Prec P, const LinkSet &ls, MultiArgs &A)
 // started from its multi-shift solution, to its own tolerance on the FP64
 // true residual.
 // ===========================================================================
-int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const LinkSet *ls_up, MultiArgs &A)
+int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const LinkSet *ls_up, MultiArgs &A,
+                     const LinkSet *ls32, const RefineOp *rop)
 {
     Context &c = ctx();
     const int n = A.n;
@@ -1066,6 +1100,13 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
                            base_ru_on ? std::function<double()>(base_ru) : std::function<double()>(), target,
                            df.get());
         if (partial) flush(c.launch());
+        double t_refine = 0;
+        if (c.verbose) {
+            sync_check();
+            t_refine = wall_seconds();
+            std::fprintf(stderr, "qphix_b200 mixed multi-shift: sloppy phase %d iterations, %d reliable updates, "
+                                 "%.1f ms\n", r.iteration, r.reliable_updates, 1e3 * (t_refine - info->final_sec));
+        }
         rus += r.reliable_updates;
         total += r.iteration;
         last = r.iteration;
@@ -1081,9 +1122,37 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
             DeltaScope(double &v, double f) : d(v), keep(v) { d = f * v; }
             ~DeltaScope() { d = keep; }
         } refine_delta(c.reliable_delta, base_ru_on ? kRefineDeltaFactor : 1.0);
-        for (int j = 0; j < n; ++j) {
+        // All shifts at once (batch_refine): one batched solve reads the
+        // links once per segment of up to 32 shifts and iteration instead of
+        // once per shift and iteration.  FP32 inner vectors, one GPU.
+        const bool batched = ls32 && n >= 2 && n <= kBatchRefineMax && !c.halo.on && refine_batched();
+        if (batched) {
+            std::vector<double> mj(A.mass, A.mass + n), tj(n);
+            for (int j = 0; j < n; ++j) tj[j] = A.res[j]->resid > 0 ? A.res[j]->resid : A.res[0]->resid;
+            std::vector<RefineResult> rr;
+            batch_refine(ls64, *ls32, src, x, mj, tj, parity, max_cg, rr);
+            int longest = 0;
+            for (int j = 0; j < n; ++j) {
+                longest = std::max(longest, rr[j].iterations);
+                rus += rr[j].reliable_updates;
+                worst = std::max(worst, rr[j].true_rsq_rel);
+                A.res[j]->final_rsq = rr[j].true_rsq_rel;
+                A.res[j]->size_r = rr[j].true_rsq_rel;
+                A.res[j]->size_relr = A.res[j]->final_rel;
+                A.res[j]->final_iter = r.iteration + rr[j].iterations;
+                A.res[j]->final_restart = rr[j].reliable_updates;
+            }
+            total += longest;
+        }
+        for (int j = 0; j < n && !batched; ++j) {
             const double tol = A.res[j]->resid > 0 ? A.res[j]->resid : A.res[0]->resid;
-            MixedResult m = mixed_pass(ps, ls64, lss, ls_up, x[j], src, parity, A.mass[j], tol, max_cg, tl);
+            // A refinement on 16-bit links that gains less than a factor
+            // kRefineEscalate in |r|^2 over one reliable-update cycle is too
+            // ill-conditioned for them (the link rounding times the
+            // condition number is near 1) and continues on FP32 links.
+            MixedResult m = rop ? mixed_pass(rop->vec, ls64, *rop->links, rop->up, x[j], src, parity, A.mass[j], tol,
+                                             max_cg, tl, 1.0 / kRefineEscalate, 1)
+                                : mixed_pass(ps, ls64, lss, ls_up, x[j], src, parity, A.mass[j], tol, max_cg, tl);
             c.stats.escalated |= m.escalated;
             total += m.iterations;
             rus += m.reliable_updates;
@@ -1093,6 +1162,11 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
             A.res[j]->size_relr = A.res[j]->final_rel;
             A.res[j]->final_iter = r.iteration + m.iterations;
             A.res[j]->final_restart = m.reliable_updates;
+        }
+        if (c.verbose) {
+            sync_check();
+            std::fprintf(stderr, "qphix_b200 mixed multi-shift: %s refinement %.1f ms\n",
+                         batched ? "batched" : "sequential", 1e3 * (wall_seconds() - t_refine));
         }
         if (parity0 == QPHIX_EVENODD) {
             parity = 0;

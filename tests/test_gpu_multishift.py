@@ -123,6 +123,34 @@ def test_multishift_mixed_short_segments(gpu, monkeypatch):
         assert orc.true_residual(dims, links, x, src, m, "even") < 1e-20
 
 
+@pytest.mark.parametrize("refine", ["batched", "sequential"])
+def test_multishift_mixed_refinement_paths(gpu, monkeypatch, refine):
+    """After the sloppy recurrence every shift is refined to its own
+    tolerance: by default all shifts in one batched solve (the batched
+    solver's kernels, FP64 reliable updates per shift), with
+    QPHIX_B200_MS_REFINE=sequential one mixed CG per shift.  Both meet every
+    shift's tolerance on the oracle's true residual and agree with the FP64
+    multi-shift."""
+    dims = (8, 8, 8, 8)
+    lib = gpu.use(dims)
+    links = fields(dims)
+    src = synthetic.gaussian_source(dims, seed=2002, parity="even")
+    masses = _masses(0.01, 6)
+    V = int(np.prod(dims))
+    lib.set_inner_precision("double")
+    _, x64, _, _ = _multi(lib, "D", links, src, masses, "even", max_iter=4000, nrestart=5, resid=1e-20)
+    monkeypatch.setenv("QPHIX_B200_MS_REFINE", refine)
+    lib.set_inner_precision("single")
+    try:
+        it, xs, res, info = _multi(lib, "D", links, src, masses, "even", max_iter=4000, nrestart=5, resid=1e-20)
+    finally:
+        lib.set_inner_precision("double")
+    for m, x, xd, r in zip(masses, xs, x64, res):
+        assert r.final_rsq < 1e-20
+        assert orc.true_residual(dims, links, x, src, m, "even") < 1e-20
+        assert rel_err(x[: 3 * V], xd[: 3 * V]) < 1e-8
+
+
 def _crossed(v, V):
     """The reference's multi-shift with EVENODD solves the even half with the
     odd-checkerboard operator and then the odd half with the even one
