@@ -596,14 +596,15 @@ int asqtad_invert_multi(QPHIX_info_t *info, typename Api<Real>::FL *H, QPHIX_inv
                 // together by the batched solver, on the 18-real FP32 links
                 const LinkSet *l32 =
                     s.vec == Prec::Single && !c.halo.on && refine_batched_env() ? &single_links(H) : nullptr;
-                // The per-shift refinements run on the sloppy recurrence's
-                // operator.  QPHIX_B200_MS_REFINE_STORAGE=half-links or half
-                // runs them on 16-bit links (a fifth less time at 32^3x64
-                // with the same iterations, but five times the iterations
-                // of the lightest refined shift at 24^3x48, m = 0.0012:
-                // the link rounding times its condition number is near 1).
+                // The per-shift refinements need a few digits per reliable
+                // update: with FP32 vectors they run on the 16-bit links,
+                // and a refinement that stagnates there continues on the
+                // FP32 links (multishift_mixed).  At 32^3x64 the
+                // refinements take 247 ms against 295 ms on FP32 links.
+                // QPHIX_B200_MS_REFINE_STORAGE=single|half-links|half
+                // overrides the choice.
                 const char *e = std::getenv("QPHIX_B200_MS_REFINE_STORAGE");
-                const std::string rs = e ? e : "single";
+                const std::string rs = e ? e : (s.vec == Prec::Single ? "half-links" : "single");
                 RefineOp rop{s.vec, s.links, s.up};
                 if (rs == "half-links") rop = {Prec::Single, &half_links(H), &single_inner_links(H)};
                 else if (rs == "half") rop = {Prec::Half, &half_links(H), &single_inner_links(H)};

@@ -414,8 +414,13 @@ constexpr int kInnerStallWindow = 256;
 // 1942 iterations at 32^3x64), and the update traffic of the heavy shifts,
 // which get there in a fraction of the iterations, is saved.
 constexpr double kShiftStopFactor = 1e-6;
-// reliable-update threshold of the per-shift refinements, relative to the CG's
-constexpr double kRefineDeltaFactor = 0.25;
+// reliable-update threshold of the per-shift refinements, relative to the
+// CG's: at 32^3x64 0.25, 0.1 and 0.05 give the same iterations with 49, 40
+// and 38 reliable updates (303, 296, 293 ms of refinement)
+constexpr double kRefineDeltaFactor = 0.1;
+// inner stagnation window of a refinement on 16-bit links (24 restarts
+// healthy refinements too often; 256 lets an ill-conditioned one crawl)
+constexpr int kRefineStallWindow = 48;
 // least |r|^2 reduction of one reliable-update cycle of a refinement on
 // 16-bit links before it continues on FP32 links
 constexpr double kRefineEscalate = 20.0;
@@ -441,9 +446,11 @@ struct MixedResult {
 // escalate_ratio / escalate_after: a 16-bit inner solve continues in FP32
 // after `escalate_after` reliable updates in a row whose true |r|^2 fell by
 // less than 1 / escalate_ratio (or that an inner stagnation forced)
+// stall_window: inner iterations without a new smallest |r|^2 that force a
+// reliable update (and count as a stall)
 MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const LinkSet *ls_up, VecBlock x,
                        VecBlock b, int parity, double mass, double tol, int max_cg, TimedLaunches &tl,
-                       double escalate_ratio = 0.25, int escalate_after = 2)
+                       double escalate_ratio = 0.25, int escalate_after = 2, int stall_window = kInnerStallWindow)
 {
     Context &c = ctx();
     const LinkSet *ls_cur = &lss;
@@ -496,7 +503,7 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
     S.prec_single = 0;
     S.ru_best = rsq;
     S.ru_best_iter = 0;
-    S.ru_stall_window = kInnerStallWindow;
+    S.ru_stall_window = stall_window;
     S.ru_stalled = 0;
     int stalled = 0;
     dslash_prepare(ps, *ls_cur, L);
@@ -1146,12 +1153,18 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
         }
         for (int j = 0; j < n && !batched; ++j) {
             const double tol = A.res[j]->resid > 0 ? A.res[j]->resid : A.res[0]->resid;
-            // A refinement on 16-bit links that gains less than a factor
-            // kRefineEscalate in |r|^2 over one reliable-update cycle is too
-            // ill-conditioned for them (the link rounding times the
-            // condition number is near 1) and continues on FP32 links.
+            // A refinement on 16-bit links that stagnates for
+            // kRefineStallWindow inner iterations, or gains less than a
+            // factor kRefineEscalate in |r|^2 over one reliable-update
+            // cycle, is too ill-conditioned for them (the link rounding
+            // times the condition number is near 1) and continues on FP32
+            // links: at 24^3x48, m = 0.0012 the lightest refined shift
+            // takes 1084 iterations on 16-bit links without this and 207
+            // with it (201 on FP32 links).
+            const bool r16 = rop && (rop->vec == Prec::Half || rop->links->prec == Prec::Half);
             MixedResult m = rop ? mixed_pass(rop->vec, ls64, *rop->links, rop->up, x[j], src, parity, A.mass[j], tol,
-                                             max_cg, tl, 1.0 / kRefineEscalate, 1)
+                                             max_cg, tl, 1.0 / kRefineEscalate, 1,
+                                             r16 ? kRefineStallWindow : kInnerStallWindow)
                                 : mixed_pass(ps, ls64, lss, ls_up, x[j], src, parity, A.mass[j], tol, max_cg, tl);
             c.stats.escalated |= m.escalated;
             total += m.iterations;

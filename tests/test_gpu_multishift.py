@@ -123,14 +123,17 @@ def test_multishift_mixed_short_segments(gpu, monkeypatch):
         assert orc.true_residual(dims, links, x, src, m, "even") < 1e-20
 
 
-@pytest.mark.parametrize("refine", ["batched", "sequential"])
-def test_multishift_mixed_refinement_paths(gpu, monkeypatch, refine):
+@pytest.mark.parametrize("refine,storage", [("sequential", None), ("sequential", "single"),
+                                            ("sequential", "half"), ("batched", None)])
+def test_multishift_mixed_refinement_paths(gpu, monkeypatch, refine, storage):
     """After the sloppy recurrence every shift is refined to its own
-    tolerance: by default all shifts in one batched solve (the batched
-    solver's kernels, FP64 reliable updates per shift), with
-    QPHIX_B200_MS_REFINE=sequential one mixed CG per shift.  Both meet every
-    shift's tolerance on the oracle's true residual and agree with the FP64
-    multi-shift."""
+    tolerance: by default one mixed CG per shift on the 16-bit links
+    (continuing on FP32 links if it stagnates), with
+    QPHIX_B200_MS_REFINE_STORAGE=single on the FP32 links, =half with 16-bit
+    vectors too, and with QPHIX_B200_MS_REFINE=batched all shifts in one
+    batched solve (the batched solver's kernels, FP64 reliable updates per
+    shift).  Every path meets every shift's tolerance on the oracle's true
+    residual and agrees with the FP64 multi-shift."""
     dims = (8, 8, 8, 8)
     lib = gpu.use(dims)
     links = fields(dims)
@@ -140,6 +143,8 @@ def test_multishift_mixed_refinement_paths(gpu, monkeypatch, refine):
     lib.set_inner_precision("double")
     _, x64, _, _ = _multi(lib, "D", links, src, masses, "even", max_iter=4000, nrestart=5, resid=1e-20)
     monkeypatch.setenv("QPHIX_B200_MS_REFINE", refine)
+    if storage:
+        monkeypatch.setenv("QPHIX_B200_MS_REFINE_STORAGE", storage)
     lib.set_inner_precision("single")
     try:
         it, xs, res, info = _multi(lib, "D", links, src, masses, "even", max_iter=4000, nrestart=5, resid=1e-20)
