@@ -491,6 +491,47 @@ k_ms_defer(VecView<float> p_low, VecView<float> r, float2 *hist, MsHistEntry *hs
     }
 }
 
+// The coefficients of a segment's expansion, on the device (one block per
+// shift, no host round trip).  With p(t) = P_t p(0) + sum_{u<t} D_t[u] r(u),
+//   t-th update:  x += b_t p(t) (upd bit 0);  p(t+1) = z_t r(t) + a_t p(t) (bit 1)
+// the column u of D and CX = sum_t b_t D_t[u] depends only on the entries
+// t >= u, so thread u computes it alone; thread 0 adds the scalars
+// GX = sum_t b_t P_t, P = P_m and the shift's job word (shift | x << 16 |
+// p << 17; the base direction is kept by the iterations, not rebuilt).
+__global__ void __launch_bounds__(kBlock)
+k_ms_coef(const MsHistEntry *hs, int m, int n, int j_low, double *coef, int *jobs)
+{
+    const int s = blockIdx.x;
+    double *c = coef + (size_t)s * 2 * (m + 1);
+    for (int u = threadIdx.x; u < m; u += blockDim.x) {
+        double D = 0.0, CX = 0.0;
+        for (int t = u; t < m; ++t) {
+            const MsHistEntry e = hs[(size_t)t * n + s];
+            if (t == u) {
+                if (e.upd & 2) D = e.z;
+            } else {
+                if (e.upd & 1) CX = fma(e.b, D, CX);
+                if (e.upd & 2) D *= e.a;
+            }
+        }
+        c[2 + 2 * u] = CX;
+        c[3 + 2 * u] = D;
+    }
+    if (threadIdx.x == 0) {
+        double P = 1.0, GX = 0.0;
+        int any = 0;
+        for (int t = 0; t < m; ++t) {
+            const MsHistEntry e = hs[(size_t)t * n + s];
+            if (e.upd & 1) GX = fma(e.b, P, GX);
+            if (e.upd & 2) P *= e.a;
+            any |= e.upd;
+        }
+        c[0] = GX;
+        c[1] = P;
+        jobs[s] = s | ((any & 1) << 16) | ((any & 2) && s != j_low ? 1 << 17 : 0);
+    }
+}
+
 // One thread per complex number of the parity block and kFlushJobs jobs;
 // the job groups of a range of numbers are adjacent blocks, so the stored
 // residuals come from DRAM once per flush and from L2 for the other
@@ -512,11 +553,20 @@ k_ms_flush(const float2 *hist, int m, const double *coef, const int *jobs, int n
     const int stride = 2 * (m + 1);
     const double2 *cf = reinterpret_cast<const double2 *>(coef + (size_t)k0 * stride);
     const int cstride = m + 1;  // in double2
+    // jobs without an update in the segment (finished shifts) are skipped
+    bool live[kFlushJobs];
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < kFlushJobs; ++q) {
+        live[q] = q < nj && (jobs[k0 + q] >> 16 & 3) != 0;
+        any |= live[q];
+    }
+    if (!any) return;
     double ax[kFlushJobs][2], ap[kFlushJobs][2];
 #pragma unroll
     for (int q = 0; q < kFlushJobs; ++q) {
         ax[q][0] = ax[q][1] = ap[q][0] = ap[q][1] = 0.0;
-        if (q < nj) {
+        if (live[q]) {
             const int s = jobs[k0 + q] & 0xffff;
             const float2 p0 = static_cast<const float2 *>(p0s[s].data)[e];
             const double2 g = __ldg(cf + q * cstride);
@@ -529,7 +579,7 @@ k_ms_flush(const float2 *hist, int m, const double *coef, const int *jobs, int n
     auto step = [&](int t, float2 hv) {
 #pragma unroll
         for (int q = 0; q < kFlushJobs; ++q) {
-            if (q < nj) {
+            if (live[q]) {
                 const double2 cc = __ldg(cf + q * cstride + 1 + t);
                 ax[q][0] = fma(cc.x, (double)hv.x, ax[q][0]);
                 ax[q][1] = fma(cc.x, (double)hv.y, ax[q][1]);
@@ -549,7 +599,7 @@ k_ms_flush(const float2 *hist, int m, const double *coef, const int *jobs, int n
     for (; t < m; ++t) step(t, __ldg(hist + (size_t)t * n3 + e));
 #pragma unroll
     for (int q = 0; q < kFlushJobs; ++q) {
-        if (q >= nj) break;
+        if (!live[q]) continue;
         const int jb = jobs[k0 + q];
         const int s = jb & 0xffff;
         if (jb >> 16 & 1) {
@@ -761,6 +811,11 @@ void ms_defer(const Launch &L, VecBlock p_low, VecBlock r, VecBlock hist, MsHist
     const int vh = L.g->vh;
     k_ms_defer<<<grid_for(vh), kBlock, 0, L.stream>>>(view<float>(p_low, vh), view<float>(r, vh),
                                                        static_cast<float2 *>(hist.data), hist_s, n, st, gate);
+}
+
+void ms_coef(const Launch &L, const MsHistEntry *hist_s, int m, int n, int j_low, double *coef, int *jobs)
+{
+    k_ms_coef<<<n, kBlock, 0, L.stream>>>(hist_s, m, n, j_low, coef, jobs);
 }
 
 void ms_flush(const Launch &L, VecBlock hist, int m, const double *coef, const int *jobs, int njobs,

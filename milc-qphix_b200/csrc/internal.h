@@ -253,6 +253,10 @@ void batch_refine(const LinkSet &l64, const LinkSet &l32, VecBlock b, const std:
 // complex numbers) and every shift's scalars in hist_s[slot * n + k]
 void ms_defer(const Launch &L, VecBlock p_low, VecBlock r, VecBlock hist, MsHistEntry *hist_s, int n,
               SolverState *st, int gate);
+// The expansion coefficients of a deferred segment of m iterations from its
+// scalar history, for the n shifts (job k = shift k; coef and jobs as
+// ms_flush reads them)
+void ms_coef(const Launch &L, const MsHistEntry *hist_s, int m, int n, int j_low, double *coef, int *jobs);
 // End of a deferred segment of m iterations.  For every job k (jobs[k] =
 // shift | do_x << 16 | do_p << 17), with c = coef + k * 2 (m + 1) and p0_s
 // the shift's direction at the start of the segment:

@@ -554,7 +554,9 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
             VecBlock p32 = ws.get(Prec::Single);
             vec_copy(Prec::Single, p32, ps, pv, L);
             pv = p32;
+            // the partial solution restarts at zero (x holds the sum so far)
             xs = ws.get(Prec::Single);
+            vec_zero(Prec::Single, xs, L);
             rs = ws.get(Prec::Single);
             tmps = ws.get(Prec::Single);
             ttts = ws.get(Prec::Single);
@@ -652,7 +654,8 @@ struct MsPass {
 // the recurrences
 //   x += b_t p(t)          (upd bit 0)
 //   p(t+1) = z_t r(t) + a_t p(t)   (upd bit 1)
-// are expanded on the host: p(t) = P_t p(0) + sum_{u<t} D_t[u] r(u), so
+// are expanded on the device (k_ms_coef): p(t) = P_t p(0) + sum_{u<t}
+// D_t[u] r(u), so
 //   x += GX p(0) + sum_u CX[u] r(u),   p(m) = P_m p(0) + sum_u D_m[u] r(u),
 // with GX = sum_t b_t P_t and CX[u] = sum_{t>u} b_t D_t[u], and k_ms_flush
 // applies them in FP64.  The base direction (the Dslash input) is updated
@@ -698,66 +701,20 @@ public:
     }
 
     // apply the segment's updates to the solutions d_x (FP64) and the shifted
-    // directions d_p (FP32), then begin the next segment
+    // directions d_p (FP32), then begin the next segment; no host round trip
     void flush(SolverState &S, VecBlock *d_x, VecBlock *d_p, const Launch &L)
     {
         const int m = S.iteration - S.ms_seg_start;
         if (m < 0 || m > cap_) throw Error("invert_multi: deferred segment out of range");
         if (m > 0) {
-            h_hist_.resize((size_t)m * n_);
-            QB_CUDA(cudaMemcpyAsync(h_hist_.data(), d_hist_, sizeof(MsHistEntry) * h_hist_.size(),
-                                    cudaMemcpyDeviceToHost, L.stream));
-            QB_CUDA(cudaStreamSynchronize(L.stream));
-            const int stride = 2 * (m + 1);
-            h_coef_.clear();
-            h_jobs_.clear();
-            std::vector<double> D(m), CX(m);
-            for (int s = 0; s < n_; ++s) {
-                double P = 1.0, GX = 0.0;
-                std::fill(D.begin(), D.end(), 0.0);
-                std::fill(CX.begin(), CX.end(), 0.0);
-                bool any_x = false, any_p = false;
-                for (int t = 0; t < m; ++t) {
-                    const MsHistEntry &e = h_hist_[(size_t)t * n_ + s];
-                    if (e.upd & 1) {
-                        any_x = true;
-                        GX += e.b * P;
-                        for (int u = 0; u < t; ++u) CX[u] += e.b * D[u];
-                    }
-                    if (e.upd & 2) {
-                        any_p = true;
-                        P *= e.a;
-                        for (int u = 0; u < t; ++u) D[u] *= e.a;
-                        D[t] = e.z;
-                    }
-                }
-                const bool do_x = any_x, do_p = any_p && s != j_low_;
-                if (!do_x && !do_p) continue;
-                h_jobs_.push_back(s | (do_x ? 1 << 16 : 0) | (do_p ? 1 << 17 : 0));
-                h_coef_.push_back(GX);
-                h_coef_.push_back(P);
-                for (int u = 0; u < m; ++u) {
-                    h_coef_.push_back(CX[u]);
-                    h_coef_.push_back(D[u]);
-                }
-            }
-            if (!h_jobs_.empty()) {
-                if ((int)h_coef_.size() != stride * (int)h_jobs_.size())
-                    throw Error("invert_multi: deferred coefficient table size");
-                QB_CUDA(cudaMemcpyAsync(d_coef_, h_coef_.data(), sizeof(double) * h_coef_.size(),
-                                        cudaMemcpyHostToDevice, L.stream));
-                QB_CUDA(cudaMemcpyAsync(d_jobs_, h_jobs_.data(), sizeof(int) * h_jobs_.size(),
-                                        cudaMemcpyHostToDevice, L.stream));
-                ms_flush(L, hist_, m, d_coef_, d_jobs_, (int)h_jobs_.size(), d_x, d_p0_, d_p);
-                // the host vectors are reused by the next flush
-                QB_CUDA(cudaStreamSynchronize(L.stream));
-            }
+            ms_coef(L, d_hist_, m, n_, j_low_, d_coef_, d_jobs_);
+            ms_flush(L, hist_, m, d_coef_, d_jobs_, n_, d_x, d_p0_, d_p);
         }
         begin(S, L);
     }
 
 private:
-    static constexpr size_t kBudgetBytes = size_t(2) << 30;
+    static constexpr size_t kBudgetBytes = size_t(4) << 30;
     static constexpr int kMinSlots = 16;
 
     MsDeferred(int n, int j_low, const std::vector<VecBlock> &pm, int cap)
@@ -783,9 +740,6 @@ private:
     double *d_coef_ = nullptr;
     int *d_jobs_ = nullptr;
     VecBlock *d_p0_ = nullptr;
-    std::vector<MsHistEntry> h_hist_;
-    std::vector<double> h_coef_;
-    std::vector<int> h_jobs_;
 };
 
 // one parity pass of the multi-shift recurrence; x[] in precision xp, the
