@@ -310,52 +310,64 @@ k_mx_update_flat(typename Wide<R>::type *x, const typename Wide<R>::type *p, typ
 struct FinMsResidual {
     SolverState *st;
     int gate;
-    __device__ void operator()(const double *t) const
+    // one warp: lane k updates shifts k, k + 32, ... (per-shift arithmetic
+    // as in the sequential form)
+    static constexpr bool kWarp = true;
+    __device__ void operator()(const double *t, int lane) const
     {
         const int single = st->prec_single;
-        const double oldrsq = st->rsq;
         const double rsq = t[0];
-        st->oldrsq = oldrsq;
-        st->rsq = rsq;
-        if (!isfinite(rsq) && !st->error) st->error = 1;  // non-finite residual: breakdown
-        if (st->error) {  // (or a zero p.Ap in the Dslash kernel before)
-            stop_run(st, gate);
-            return;
-        }
-        if (rsq <= st->rsqstop) {
-            st->converged = 1;
-            stop_run(st, gate);
-            return;
-        }
-        const int jl = st->j_low;
-        st->alpha[jl] = round_to(rsq / oldrsq, single);
-        for (int k = 0; k < st->num_now; ++k) {
-            if (k == jl) continue;
-            const double zb = round_to(st->zeta_i[k] * st->beta_i[jl], single);
-            if (zb != 0.0)
-                st->alpha[k] = round_to(round_to(round_to(st->alpha[jl] * st->zeta_ip1[k], single) *
-                                                 st->beta_i[k], single) / zb, single);
-            else { st->alpha[k] = 0.0; st->finished[k] = 1; }
-        }
-        if (st->shift_stop > 0.0) {
-            for (int k = 0; k < st->num_now; ++k) {
-                if (k == jl || st->shift_done_at[k] != INT_MAX) continue;
-                const double z = st->zeta_ip1[k];
-                if (z * z * rsq <= st->shift_stop) st->shift_done_at[k] = st->iteration;
+        int done = 0;
+        if (lane == 0) {
+            const double oldrsq = st->rsq;
+            st->oldrsq = oldrsq;
+            st->rsq = rsq;
+            if (!isfinite(rsq) && !st->error) st->error = 1;  // non-finite residual: breakdown
+            if (st->error) {  // (or a zero p.Ap in the Dslash kernel before)
+                stop_run(st, gate);
+                done = 1;
+            } else if (rsq <= st->rsqstop) {
+                st->converged = 1;
+                stop_run(st, gate);
+                done = 1;
+            } else {
+                st->alpha[st->j_low] = round_to(rsq / oldrsq, single);
             }
         }
-        // the iteration completes (its vector updates are not gated off);
-        // the host then replaces r by the FP64 residual of the base shift
-        if (st->ms_delta2 > 0.0 && rsq < st->ms_delta2 * st->rsq_ru) {
-            st->ms_ru = 1;
-            stop_run(st, gate);
+        if (__shfl_sync(0xffffffffu, done, 0)) return;
+        __syncwarp();
+        const int jl = st->j_low;
+        const int nn = st->num_now;
+        const double a_jl = st->alpha[jl], b_jl = st->beta_i[jl];
+        const int it = st->iteration;
+        const double stop = st->shift_stop;
+        for (int k = lane; k < nn; k += 32) {
+            if (k == jl) continue;
+            const double zb = round_to(st->zeta_i[k] * b_jl, single);
+            if (zb != 0.0)
+                st->alpha[k] = round_to(round_to(round_to(a_jl * st->zeta_ip1[k], single) * st->beta_i[k], single) / zb,
+                                        single);
+            else { st->alpha[k] = 0.0; st->finished[k] = 1; }
+            if (stop > 0.0 && st->shift_done_at[k] == INT_MAX) {
+                const double z = st->zeta_ip1[k];
+                if (z * z * rsq <= stop) st->shift_done_at[k] = it;
+            }
         }
-        // deferred shift updates: this iteration takes the segment's last slot
-        if (st->ms_seg_cap > 0 && st->iteration - st->ms_seg_start >= st->ms_seg_cap) {
-            st->ms_seg_full = 1;
-            stop_run(st, gate);
+        __syncwarp();
+        if (lane == 0) {
+            // the iteration completes (its vector updates are not gated off);
+            // the host then replaces r by the FP64 residual of the base shift
+            if (st->ms_delta2 > 0.0 && rsq < st->ms_delta2 * st->rsq_ru) {
+                st->ms_ru = 1;
+                stop_run(st, gate);
+            }
+            // deferred shift updates: this iteration takes the segment's last slot
+            if (st->ms_seg_cap > 0 && st->iteration - st->ms_seg_start >= st->ms_seg_cap) {
+                st->ms_seg_full = 1;
+                stop_run(st, gate);
+            }
+            if (st->iteration >= st->max_cg || run_guard(st)) stop_run(st, gate);
         }
-        if (st->iteration >= st->max_cg || run_guard(st)) stop_run(st, gate);
     }
 };
 

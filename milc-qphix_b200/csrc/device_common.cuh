@@ -6,6 +6,8 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "internal.h"
 
 namespace qb {
@@ -300,6 +302,13 @@ __device__ __forceinline__ void mv_adj_sub(A acc[6], const A u[18], const A v[6]
 }
 
 // ------------------------------------------------------------- reductions --
+// A finishing functor with `static constexpr bool kWarp = true` is called as
+// fin(totals, lane) by all 32 lanes of one warp (per-shift work in parallel,
+// with __syncwarp between dependent steps); others as fin(totals) by one
+// thread.
+template <typename F, typename = void> struct IsWarpFin : std::false_type {};
+template <typename F> struct IsWarpFin<F, std::void_t<decltype(F::kWarp)>> : std::bool_constant<F::kWarp> {};
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll
@@ -352,21 +361,27 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NV], double *partials,
         if (lane == 0) sm[i][w] = s;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (w == 0) {
 #pragma unroll
         for (int i = 0; i < NV; ++i) {
             double s = 0;
             for (int k = 0; k < nw; ++k) s += sm[i][k];
-            t[i] = s;
+            t[i] = s;  // every lane of warp 0 sums the same slots in the same order
         }
         if (split) {
+            if (lane == 0)
 #pragma unroll
-            for (int i = 0; i < NV; ++i) split->dd_red[i] = t[i];
-        } else {
+                for (int i = 0; i < NV; ++i) split->dd_red[i] = t[i];
+        } else if constexpr (IsWarpFin<F>::value) {
+            fin(t, lane);
+        } else if (lane == 0) {
             fin(t);
         }
-        *counter = 0;
-        __threadfence();
+        __syncwarp();
+        if (lane == 0) {
+            *counter = 0;
+            __threadfence();
+        }
     }
 }
 
@@ -386,11 +401,13 @@ inline int grid_for(int n) { return (n + kBlock - 1) / kBlock; }
 template <int NV, typename Fin>
 __global__ void k_dd_fin(SolverState *st, int gate, Fin fin)
 {
-    if (threadIdx.x || (gate >= 0 && gate > *(volatile const int *)&st->stop_at)) return;
+    // launched with one warp
+    if (threadIdx.x >= 32 || (gate >= 0 && gate > *(volatile const int *)&st->stop_at)) return;
     double t[NV];
 #pragma unroll
     for (int i = 0; i < NV; ++i) t[i] = st->dd_red[i];
-    fin(t);
+    if constexpr (IsWarpFin<Fin>::value) fin(t, (int)threadIdx.x);
+    else if (threadIdx.x == 0) fin(t);
 }
 
 // Ends the device run of a solver phase: records the stopping iteration for

@@ -221,59 +221,78 @@ template <> struct MinBlocks<float, Recon13> { static constexpr int value = 3; }
 template <> struct MinBlocks<float, __half> { static constexpr int value = 3; };
 template <> struct MinBlocks<__half, __half> { static constexpr int value = 3; };
 
-// Scalar step after p.(M^dag M p) is known: CG (mode 0) a = -rsq/pkp;
-// multi-shift (mode 1) the shift recurrences.  Runs in one thread.
+// Scalar step after p.(M^dag M p) is known, run by one warp of the last
+// block of the reduction: CG (mode 0) a = -rsq/pkp in lane 0; multi-shift
+// (mode 1) the shift recurrences, lane k handling shifts k, k + 32, ...
+// (each shift's arithmetic is the sequential one, so the results do not
+// depend on the lane split; one thread walking the shifts through device
+// memory took ~10 us per iteration at 12 shifts).
 // A zero or non-finite p.(M p) is a breakdown (M is positive definite for
 // m > 0; the reference divides by it unchecked, ks_d_congrad_fn.cpp:511):
 // the step is set to zero, st->error = 2 and the update kernel that follows
 // ends the device run, so the host returns QPHIX_FAIL.
-__device__ __forceinline__ void mdagm_finalize(SolverState *st, double pkp, int mode)
-{
-    st->pkp = pkp;
-    st->iteration += 1;
-    if (!(pkp != 0.0) || !isfinite(pkp)) {
-        st->error = 2;
-        st->a = 0.0;
-        return;
-    }
-    if (mode == 0) {
-        st->a = round_to(-st->rsq / pkp, st->prec_single);
-    } else {
+struct FinMdagm {
+    SolverState *st;
+    int mode;
+    static constexpr bool kWarp = true;
+    __device__ void operator()(const double *t, int lane) const
+    {
+        const double pkp = t[0];
+        int done = 0;
+        if (lane == 0) {
+            st->pkp = pkp;
+            st->iteration += 1;
+            if (!(pkp != 0.0) || !isfinite(pkp)) {
+                st->error = 2;
+                st->a = 0.0;
+                done = 1;
+            } else if (mode == 0) {
+                st->a = round_to(-st->rsq / pkp, st->prec_single);
+                done = 1;
+            }
+        }
+        if (__shfl_sync(0xffffffffu, done, 0)) return;
         // multi-shift scalar recurrences (ks_multicg_offset.cpp:475-496);
         // the values of the previous iteration are scrolled first
         // (:617-622), which the reference does at the end of that iteration
         const int single = st->prec_single;
         const int jl = st->j_low;
+        const int nn = st->num_now;
         if (!st->first_iter) {
-            for (int k = 0; k < st->num_now; ++k) {
+            for (int k = lane; k < nn; k += 32) {
                 st->beta_im1[k] = st->beta_i[k];
                 st->zeta_im1[k] = st->zeta_i[k];
                 st->zeta_i[k] = st->zeta_ip1[k];
             }
         }
-        st->first_iter = 0;
-        st->beta_i[jl] = round_to(-st->rsq / pkp, single);
-        st->zeta_ip1[jl] = 1.0;
-        int nn = st->num_now;
-        for (int k = 0; k < nn; ++k) {
+        __syncwarp();
+        if (lane == 0) {
+            st->first_iter = 0;
+            st->beta_i[jl] = round_to(-st->rsq / pkp, single);
+            st->zeta_ip1[jl] = 1.0;
+        }
+        __syncwarp();
+        const double b_jl = st->beta_i[jl], a_jl = st->alpha[jl], bm1_jl = st->beta_im1[jl];
+        for (int k = lane; k < nn; k += 32) {
             if (k == jl) continue;
-            double z = round_to(round_to(st->zeta_i[k] * st->zeta_im1[k], single) * st->beta_im1[jl], single);
-            const double c1 = round_to(round_to(st->beta_i[jl] * st->alpha[jl], single) *
-                                           round_to(st->zeta_im1[k] - st->zeta_i[k], single), single);
-            const double c2 = round_to(round_to(st->zeta_im1[k] * st->beta_im1[jl], single) *
-                                           (1.0 + round_to(st->shifts[k] * st->beta_i[jl], single)), single);
+            const double zi = st->zeta_i[k], zim1 = st->zeta_im1[k];
+            double z = round_to(round_to(zi * zim1, single) * bm1_jl, single);
+            const double c1 = round_to(round_to(b_jl * a_jl, single) * round_to(zim1 - zi, single), single);
+            const double c2 =
+                round_to(round_to(zim1 * bm1_jl, single) * (1.0 + round_to(st->shifts[k] * b_jl, single)), single);
             const double den = round_to(c1 + c2, single);
             if (den != 0.0) z = round_to(z / den, single);
             else { z = 0.0; st->finished[k] = 1; }
             st->zeta_ip1[k] = z;
-            if (st->zeta_i[k] != 0.0)
-                st->beta_i[k] = round_to(round_to(st->beta_i[jl] * z, single) / st->zeta_i[k], single);
+            if (zi != 0.0)
+                st->beta_i[k] = round_to(round_to(b_jl * z, single) / zi, single);
             else { st->zeta_ip1[k] = 0.0; st->beta_i[k] = 0.0; st->finished[k] = 1; }
-            if (st->finished[k] == 1 && k == nn - 1 && k > jl) nn--;
         }
-        st->num_now = nn;
+        __syncwarp();
+        // the last active shift leaves the recurrence once it has finished
+        if (lane == 0 && nn - 1 > jl && st->finished[nn - 1] == 1) st->num_now = nn - 1;
     }
-}
+};
 
 template <typename SV, typename SL>
 __global__ void __launch_bounds__(kBlock, MinBlocks<SV, SL>::value) k_dslash(DslashArgs<SV, SL> a, const SolverState *st, int gate)
@@ -310,7 +329,7 @@ k_dslash_mdagm(DslashArgs<SV, SL> a, VecView<SV> pv, double m4, SolverState *st,
 #pragma unroll
         for (int i = 0; i < 6; ++i) dot[0] += (double)(p[i] * acc[i]);
     }
-    grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) { mdagm_finalize(st, tot[0], mode); });
+    grid_reduce<1>(dot, partials, &st->counter, FinMdagm{st, mode});
 }
 
 // ---------------------------------------------------------------------------
@@ -389,12 +408,6 @@ k_dd_dot(VecView<SV> p, VecView<SV> t, SolverState *st, double *partials, int ga
     }
     grid_reduce<1>(s, partials, &st->counter, FinNothing{}, st);
 }
-
-struct FinMdagm {
-    SolverState *st;
-    int mode;
-    __device__ void operator()(const double *t) const { mdagm_finalize(st, t[0], mode); }
-};
 
 // ---------------------------------------------------------------------------
 // TMA-pipelined Dslash.  A persistent CTA owns tiles of T consecutive output
@@ -479,7 +492,7 @@ __device__ __forceinline__ void tma_direction(const DslashArgs<SV, SL> &a, const
 }
 
 // MODE 0: out = D in.  MODE 1: out = D in + m4 p, p.out reduced, then the
-// solver's scalar step (mdagm_finalize).
+// solver's scalar step (FinMdagm).
 // Every mbarrier wait gives up after `wait_limit` polls.  The CTA then
 // stops as a whole (the failure is OR-ed over the CTA at the end of the
 // stage), thread 0 waits -- with a generous limit -- for every copy still
@@ -577,7 +590,7 @@ k_dslash_tma(DslashArgs<SV, SL> a, const char *links, VecView<SV> pv, double m4,
         return;
     }
     if constexpr (MODE == 1)
-        grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) { mdagm_finalize(st, tot[0], mode); });
+        grid_reduce<1>(dot, partials, &st->counter, FinMdagm{st, mode});
 }
 
 // ---------------------------------------------------------------------------
@@ -685,7 +698,7 @@ k_dslash_tile(DslashArgs<SV, SL> a, VecView<SV> pv, double m4, SolverState *st, 
         return;
     }
     if constexpr (MODE == 1)
-        grid_reduce<1>(dot, partials, &st->counter, [&](const double *tot) { mdagm_finalize(st, tot[0], mode); });
+        grid_reduce<1>(dot, partials, &st->counter, FinMdagm{st, mode});
 }
 
 template <typename SV, typename SL>
