@@ -27,6 +27,7 @@
 // 48 staple paths of a constant table; the links it gathers come from
 // L1/L2 (every link is read by ~200 threads).  FP64 for D3, FP32 for F3.
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "context.h"
@@ -146,12 +147,13 @@ __device__ __forceinline__ void mm_inplace(R a[18], const R b[18], bool adj_b)
 }
 
 // One thread per link (direction-major: a warp's threads share the path
-// table entry and gather consecutive sites).  The path product is formed in
-// place, one row at a time; in FP64 a register cap of four blocks per SM
-// measured 15.6 ms against 16.2 ms per 32^3x64 checkerboard (a cap in FP32
-// was slower: 9.7 against 9.3 ms).  Moving the staple sum to shared memory
-// and interleaving the four directions of a site over adjacent threads was
-// slower in both (17.4 / 11.8 ms).
+// table entry and gather consecutive sites).  In FP64 the path product is
+// formed in place, one row at a time, under a register cap of four blocks per
+// SM: 15.6 ms against 16.2 ms per 32^3x64 checkerboard.  In FP32 both were
+// slower (9.7 ms with the cap, 10.6 ms in place without it, against 9.3 ms),
+// so FP32 keeps the product in a third matrix.  Moving the staple sum to
+// shared memory and interleaving the four directions of a site over adjacent
+// threads was slower in both (17.4 / 11.8 ms).
 constexpr int kGfThreads = 128;
 template <typename R> struct GfMinBlocks { static constexpr int value = 1; };
 template <> struct GfMinBlocks<double> { static constexpr int value = 4; };
@@ -199,8 +201,13 @@ k_gauge_force(GaugeView<R> U, cx_t<R> *mom, int cb, R eps, R c0, R c1, R c2)
 #pragma unroll
                     for (int i = 0; i < 18; ++i) M[i] = Lk[i];
                 }
-            } else {
+            } else if constexpr (std::is_same<R, double>::value) {
                 mm_inplace(M, Lk, back);
+            } else {
+                R T[18];
+                mm(M, Lk, T, back);
+#pragma unroll
+                for (int i = 0; i < 18; ++i) M[i] = T[i];
             }
         }
 #pragma unroll
