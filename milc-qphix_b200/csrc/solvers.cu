@@ -1105,6 +1105,7 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
             }
             total += longest;
         }
+        double t_shift = c.verbose ? wall_seconds() : 0.0;
         for (int j = 0; j < n && !batched; ++j) {
             const double tol = A.res[j]->resid > 0 ? A.res[j]->resid : A.res[0]->resid;
             // A refinement on 16-bit links that stagnates for
@@ -1124,6 +1125,13 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
             total += m.iterations;
             rus += m.reliable_updates;
             worst = std::max(worst, m.true_rsq_rel);
+            if (c.verbose) {
+                sync_check();
+                const double now = wall_seconds();
+                std::fprintf(stderr, "qphix_b200 mixed multi-shift: shift %d refinement %d iterations, %d updates, "
+                                     "%.2f ms\n", j, m.iterations, m.reliable_updates, 1e3 * (now - t_shift));
+                t_shift = now;
+            }
             A.res[j]->final_rsq = m.true_rsq_rel;
             A.res[j]->size_r = m.true_rsq_rel;
             A.res[j]->size_relr = A.res[j]->final_rel;
