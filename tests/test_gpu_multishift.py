@@ -156,6 +156,32 @@ def test_multishift_mixed_refinement_paths(gpu, monkeypatch, refine, storage):
         assert rel_err(x[: 3 * V], xd[: 3 * V]) < 1e-8
 
 
+@pytest.mark.parametrize("inner", ["single", "half"])
+def test_multishift_mixed_edge_cases(gpu, inner):
+    """A single shift (the base is the only shift the deferred updates and
+    the refinement see) meets the tolerance against the oracle; a zero
+    source returns zero solutions with success, as the reference does
+    (ks_multicg_offset.cpp:377-419)."""
+    dims = (8, 8, 8, 8)
+    lib = gpu.use(dims)
+    links = fields(dims)
+    src = synthetic.gaussian_source(dims, seed=2002, parity="even")
+    lib.set_inner_precision(inner)
+    try:
+        it, xs, res, info = _multi(lib, "D", links, src, [0.03], "even", max_iter=4000, nrestart=5, resid=1e-20)
+        assert info.status == 0
+        assert res[0].final_rsq < 1e-20
+        assert orc.true_residual(dims, links, xs[0], src, 0.03, "even") < 1e-20
+        zero = np.zeros_like(src)
+        it0, xs0, res0, info0 = _multi(lib, "D", links, zero, _masses(0.02, 4), "even", max_iter=4000, nrestart=5,
+                                       resid=1e-20)
+        assert info0.status == 0
+        for x, r in zip(xs0, res0):
+            assert not np.any(x) and r.final_rsq == 0.0
+    finally:
+        lib.set_inner_precision("double")
+
+
 def _crossed(v, V):
     """The reference's multi-shift with EVENODD solves the even half with the
     odd-checkerboard operator and then the odd half with the even one
