@@ -679,15 +679,7 @@ public:
         if (fit < (size_t)kMinSlots) return nullptr;
         return std::unique_ptr<MsDeferred>(new MsDeferred(n, j_low, pm, (int)fit));
     }
-    ~MsDeferred()
-    {
-        dev_free(hist_.data);
-        dev_free(d_hist_);
-        dev_free(d_coef_);
-        dev_free(d_jobs_);
-        dev_free(d_p0_);
-        free_vec(p_low0_);
-    }
+    ~MsDeferred() { release(); }
     VecBlock hist() const { return hist_; }
     MsHistEntry *hist_scalars() const { return d_hist_; }
 
@@ -721,16 +713,36 @@ private:
         : cap_(cap), n_(n), j_low_(j_low), pm_(pm)
     {
         Context &c = ctx();
-        hist_.data = dev_alloc(vec_bytes(Prec::Single, c.g.vh) * cap_);
-        d_hist_ = static_cast<MsHistEntry *>(dev_alloc(sizeof(MsHistEntry) * cap_ * n_));
-        d_coef_ = static_cast<double *>(dev_alloc(sizeof(double) * 2 * (cap_ + 1) * n_));
-        d_jobs_ = static_cast<int *>(dev_alloc(sizeof(int) * n_));
-        d_p0_ = static_cast<VecBlock *>(dev_alloc(sizeof(VecBlock) * n_));
-        p_low0_ = alloc_vec(Prec::Single);
-        std::vector<VecBlock> p0(pm);
-        p0[j_low_] = p_low0_;
-        QB_CUDA(cudaMemcpyAsync(d_p0_, p0.data(), sizeof(VecBlock) * n_, cudaMemcpyHostToDevice, c.stream));
-        QB_CUDA(cudaStreamSynchronize(c.stream));
+        try {  // (a failed allocation releases the ones before it)
+            hist_.data = dev_alloc(vec_bytes(Prec::Single, c.g.vh) * cap_);
+            d_hist_ = static_cast<MsHistEntry *>(dev_alloc(sizeof(MsHistEntry) * cap_ * n_));
+            d_coef_ = static_cast<double *>(dev_alloc(sizeof(double) * 2 * (cap_ + 1) * n_));
+            d_jobs_ = static_cast<int *>(dev_alloc(sizeof(int) * n_));
+            d_p0_ = static_cast<VecBlock *>(dev_alloc(sizeof(VecBlock) * n_));
+            p_low0_ = alloc_vec(Prec::Single);
+            std::vector<VecBlock> p0(pm);
+            p0[j_low_] = p_low0_;
+            QB_CUDA(cudaMemcpyAsync(d_p0_, p0.data(), sizeof(VecBlock) * n_, cudaMemcpyHostToDevice, c.stream));
+            QB_CUDA(cudaStreamSynchronize(c.stream));
+        } catch (...) {
+            release();
+            throw;
+        }
+    }
+
+    void release()
+    {
+        dev_free(hist_.data);
+        dev_free(d_hist_);
+        dev_free(d_coef_);
+        dev_free(d_jobs_);
+        dev_free(d_p0_);
+        if (p_low0_.data) free_vec(p_low0_);
+        hist_.data = p_low0_.data = nullptr;
+        d_hist_ = nullptr;
+        d_coef_ = nullptr;
+        d_jobs_ = nullptr;
+        d_p0_ = nullptr;
     }
 
     int cap_, n_, j_low_;
