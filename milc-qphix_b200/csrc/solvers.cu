@@ -1022,8 +1022,10 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
     // iteration moves the bytes of one CG iteration whatever the number of
     // shifts, and each shifted direction is rounded to FP32 once per segment
     // instead of once per iteration.
+    // (QPHIX_B200_MS_DEFER=0 keeps the per-iteration updates, for comparison)
     std::unique_ptr<MsDeferred> df;
-    if (ps == Prec::Single) df = MsDeferred::make(n, j_low, pm);
+    const char *defer_env = std::getenv("QPHIX_B200_MS_DEFER");
+    if (ps == Prec::Single && !(defer_env && defer_env[0] == '0')) df = MsDeferred::make(n, j_low, pm);
     // Otherwise, with base reliable updates, the shifted solutions accumulate
     // between updates in FP32 partial sums y_j (24 instead of 48 bytes read
     // and written per site and shift each iteration); every reliable update

@@ -95,6 +95,39 @@ def test_multishift_mixed_every_shift_converges(gpu, inner):
         assert orc.true_residual(dims, links, x, src, m, "even") < 1e-20
 
 
+def test_multishift_mixed_deferred_matches_explicit_updates(gpu, monkeypatch):
+    """The deferred shift updates (stored residuals, coefficients expanded on
+    the device, one FP64 flush per segment) against the per-iteration
+    updates they replace (QPHIX_B200_MS_DEFER=0: x_j and p_j updated every
+    iteration, x_j in FP32 partial sums): the base recurrence takes the same
+    iterations to within the rounding of the base solution its reliable
+    updates read (FP64 expansion against FP32 partial sums), both meet every
+    shift's tolerance against the oracle, and the two sets of solutions agree
+    to the tolerance's level."""
+    dims = (8, 8, 8, 8)
+    lib = gpu.use(dims)
+    links = fields(dims)
+    src = synthetic.gaussian_source(dims, seed=2002, parity="even")
+    masses = _masses(0.01, 6)
+    V = int(np.prod(dims))
+    out = {}
+    lib.set_inner_precision("single")
+    try:
+        for defer in ("1", "0"):
+            monkeypatch.setenv("QPHIX_B200_MS_DEFER", defer)
+            out[defer] = _multi(lib, "D", links, src, masses, "even", max_iter=4000, nrestart=5, resid=1e-20)
+    finally:
+        lib.set_inner_precision("double")
+    assert abs(out["1"][0] - out["0"][0]) <= 2, (out["1"][0], out["0"][0])
+    for defer in ("1", "0"):
+        it, xs, res, info = out[defer]
+        for m, x, r in zip(masses, xs, res):
+            assert r.final_rsq < 1e-20
+            assert orc.true_residual(dims, links, x, src, m, "even") < 1e-20, defer
+    for a, b in zip(out["1"][1], out["0"][1]):
+        assert rel_err(a[: 3 * V], b[: 3 * V]) < 1e-8
+
+
 def test_multishift_mixed_short_segments(gpu, monkeypatch):
     """FP32 Krylov vectors: the shifted solutions and directions are rebuilt
     from the stored base residuals once per segment.  Segments of 16
