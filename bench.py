@@ -352,14 +352,20 @@ def run_gpu(args):
     lib.finalize()
     # the north-star size in the same run: 32^3x64, HISQ-shaped links,
     # m = 0.0012 -- FP64 and mixed CG, FP64 and mixed 12-shift multi-shift
+    # (one GPU only: the scaling runs time the headline workload alone)
     target = None
-    if not args.no_target:
+    batch = None
+    if not args.no_target and world == 1:
         t = multishift_workload(MS_DIMS, 2, {"fp64_cg", "mixed_cg_single", "fp64_multishift",
                                              "mixed_multishift_single"}, True, False, notes=False)
         target = {k: t[k] for k in ("workload", "lattice", "mass", "sigmas", "resid_sq", "reliable_delta",
                                     "fp64_cg", "mixed_cg_single", "fp64_multishift", "mixed_multishift_single")}
         target["timing"] = ("device time of each solve (CUDA events on the library stream), inputs resident, "
                             "the second of two solves; true residuals recomputed through the FP64 Dslash")
+    if not args.no_batch and world == 1:
+        bw = batch_workload(None, steps=1, warmup=1, sequential=True, notes=False)
+        batch = {k: bw[k] for k in ("workload", "systems", "lattices", "batch_s", "sequential_s",
+                                    "speedup_vs_sequential", "rhs_per_thread", "true_rsq_rel_max", "timing")}
 
     peak, peak_kind = peaks()
     k1_ms = dslash_ms / max(dslash_n, 1)
@@ -446,6 +452,7 @@ def run_gpu(args):
         "clocks": clk,
         "cpu_baseline": cpu,
         "target_32x32x32x64": target,
+        "config4_batch": batch,
     }
     # our kernel launches per step: 4 per iteration + restart/reliable-update kernels
     line["gpu_launches"] = int(np.median(iters)) * 4 + 8 * int(np.median(rus)) + 8
@@ -878,25 +885,27 @@ BATCH_WORKLOAD = ("batched mixed CG: 16 Gaussian RHS on 24^3x48 + 8 lattices (8^
                   "two of each, one RHS each), m=0.02, tol 1e-10, one device run")
 
 
-def run_batch(args):
-    """--mode batch: 24 systems on 9 lattices in one QPHIX_B200_D3_batch_invert
-    call (host buffers in and out), against the same systems solved one at a
-    time through QPHIX_D3_asqtad_invert with the FP32 inner solve.  Every
-    solution's FP64 true residual is checked through the FP64 Dslash."""
+def batch_workload(lattice=None, steps=1, warmup=1, sequential=True, notes=True):
+    """24 systems on 9 lattices in one QPHIX_B200_D3_batch_invert call (host
+    buffers in and out), against the same systems solved one at a time
+    through QPHIX_D3_asqtad_invert with the FP32 inner solve.  Every
+    solution's FP64 true residual is checked through the FP64 Dslash.
+    lattice: the 16 right-hand sides on that lattice alone (profiling
+    target).  Returns a dict."""
     import torch
 
     dev = "cuda" if torch.cuda.is_available() else None
     t0 = time.perf_counter()
-    # --lattice: the 16 right-hand sides on that lattice alone (profiling target)
-    big = tuple(int(v) for v in args.lattice.split("x")) if args.lattice else BATCH_BIG
-    lats = [big] + ([] if args.lattice else [d for d in BATCH_SMALL for _ in range(2)])
+    big = tuple(int(v) for v in lattice.split("x")) if lattice else BATCH_BIG
+    lats = [big] + ([] if lattice else [d for d in BATCH_SMALL for _ in range(2)])
     links = [synthetic.asqtad_links(d, seed=LINK_SEED + i, device=dev) for i, d in enumerate(lats)]
     systems = [(0, BATCH_MASS, synthetic.gaussian_source(big, seed=SRC_SEED + r, parity="even"))
                for r in range(BATCH_NRHS)]
     systems += [(l, BATCH_MASS, synthetic.gaussian_source(lats[l], seed=SRC_SEED + 100 + l, parity="even"))
                 for l in range(1, len(lats))]
     gen_s = time.perf_counter() - t0
-    print(json.dumps({"field_generation_s": gen_s}), file=sys.stderr, flush=True)
+    if notes:
+        print(json.dumps({"field_generation_s": gen_s}), file=sys.stderr, flush=True)
     if dev:
         torch.cuda.empty_cache()
     lib = capi.QphixLib(LIB_PATH)
@@ -922,20 +931,21 @@ def run_batch(args):
         assert info.status == 0, lib.last_error()
         return max(ms / 1e3, wall), res, [x.copy() for x in xs]
 
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         batch_solve()
     times = []
-    for _ in range(max(1, args.steps)):
+    for _ in range(max(1, steps)):
         s, res, xs = batch_solve()
         times.append(s)
     s_batch = float(np.median(times))
-    print(json.dumps({"batch_s": s_batch, "iterations": [r.final_iter for r in res]}), file=sys.stderr, flush=True)
+    if notes:
+        print(json.dumps({"batch_s": s_batch, "iterations": [r.final_iter for r in res]}), file=sys.stderr,
+              flush=True)
     lib.batch_destroy_L(B)
-    if args.no_sequential:
+    if not sequential:
         lib.finalize()
-        print(json.dumps({"mode": "batch", "workload": BATCH_WORKLOAD, "batch_s": s_batch,
-                          "rhs_per_thread": batch_g[0], "batch_iterations": [r.final_iter for r in res]}))
-        return
+        return {"mode": "batch", "workload": BATCH_WORKLOAD, "batch_s": s_batch,
+                "rhs_per_thread": batch_g[0], "batch_iterations": [r.final_iter for r in res]}
 
     # the same systems one at a time (FP32 inner, FP64 reliable updates)
     seq = 0.0
@@ -965,7 +975,7 @@ def run_batch(args):
             trues.append(_true_rel_rsq(lib, L, xs[k], systems[k][2], BATCH_MASS, V))
         lib.destroy_L("D", L)
         lib.finalize()
-    print(json.dumps({
+    return {
         "mode": "batch", "workload": BATCH_WORKLOAD, "systems": len(systems), "lattices": len(lats),
         "field_generation_s": gen_s, "batch_s": s_batch, "batch_all_s": times,
         "rhs_per_thread": batch_g[0],
@@ -975,7 +985,13 @@ def run_batch(args):
         "true_rsq_rel_max": max(trues), "true_rsq_rel": trues,
         "timing": "batch: one C-ABI call from pinned host buffers (H2D of sources and guesses, D2H of "
                   "solutions inside); sequential: device time of each QPHIX_D3_asqtad_invert on resident vectors",
-    }))
+    }
+
+
+def run_batch(args):
+    """--mode batch: batch_workload on its 9 lattices (or --lattice alone);
+    prints one JSON line."""
+    print(json.dumps(batch_workload(args.lattice, args.steps, args.warmup, not args.no_sequential)))
 
 
 FORCE_DIMS = (16, 16, 16, 32)
@@ -1219,6 +1235,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="default run: skip the batched-solve workload (config 4) extra key")
     ap.add_argument("--no-target", action="store_true",
                     help="bench mode: skip the 32^3x64 solves reported beside the headline")
     ap.add_argument("--no-compress", action="store_true",
