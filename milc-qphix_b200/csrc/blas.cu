@@ -449,10 +449,10 @@ k_ms_update(VecBlock *xs, VecBlock *ps, VecView<S> r, int n, SolverState *st, in
 // The shifted directions and solutions are linear combinations of the base
 // residuals: p_k(t+1) = z_k r(t+1) + a_k p_k(t), x_k += b_k p_k(t).  Instead
 // of updating 2n vectors every iteration, an iteration stores its residual
-// (the vector the updates would read) and the scalars they would use; the
-// host expands the recurrences into coefficients and k_ms_flush applies them
-// once per segment in FP64, so a segment rounds p_k once instead of every
-// iteration.  The base direction is the Dslash input and is updated here,
+// (the vector the updates would read) and the scalars they would use;
+// k_ms_coef expands the recurrences into coefficients and k_ms_flush applies
+// them once per segment in FP64, so a segment rounds p_k once instead of
+// every iteration.  The base direction is the Dslash input and is updated here,
 // with the arithmetic of k_ms_update (its iterations are unchanged).
 __global__ void __launch_bounds__(kBlock)
 k_ms_defer(VecView<float> p_low, VecView<float> r, float2 *hist, MsHistEntry *hs, int n, SolverState *st, int gate)
