@@ -182,10 +182,11 @@ def max_over_ranks(pg, v):
     return float(t.item())
 
 
-def make_inputs(device=None):
+def make_inputs(device=None, dims=DIMS):
     # the eigendecompositions of the generator run on the host (torch CPU)
-    links = synthetic.asqtad_links(DIMS, seed=LINK_SEED)
-    src = synthetic.gaussian_source(DIMS, seed=SRC_SEED, parity="even")
+    # unless a device is given
+    links = synthetic.asqtad_links(dims, seed=LINK_SEED, device=device)
+    src = synthetic.gaussian_source(dims, seed=SRC_SEED, parity="even")
     return links, src
 
 
@@ -643,10 +644,16 @@ def run_profile_dslash(args):
 
 
 def run_profile_mixed(args):
-    """--mode mixed: only the timed mixed-precision solves (ncu launch list)."""
-    links, src = make_inputs()
+    """--mode mixed: only the timed mixed-precision solves (ncu launch list);
+    --lattice another lattice than the headline's (same link recipe, mass and
+    tolerance), with its kernel timings and the autotuner's per-variant
+    times."""
+    import torch
+
+    dims = tuple(int(v) for v in args.lattice.split("x")) if args.lattice else DIMS
+    links, src = make_inputs("cuda" if torch.cuda.is_available() and args.lattice else None, dims)
     lib = capi.QphixLib(LIB_PATH)
-    assert lib.init(DIMS) == 0, lib.last_error()
+    assert lib.init(dims) == 0, lib.last_error()
     lib.set_reliable_delta(RU_DELTA)
     lib.set_link_compression(args.compress)
     L = lib.create_L("D", links)
@@ -663,13 +670,22 @@ def run_profile_mixed(args):
         res_all.append({"ms": ms, "iterations": st.iterations, "reliable_updates": st.reliable_updates,
                         "true_rsq_rel": res.final_rsq})
         lib.destroy_V("D", x)
-    lib.destroy_V("D", b)
-    lib.destroy_L("D", L)
     name = {"single": "single-r12" if args.compress else "single"}.get(args.inner, args.inner)
     lib_tuning = (lib.tuning(name), lib.tuning(name, "mdagm"))
+    # K1 / K2 device time inside one more solve (not timed above)
+    lib.set_kernel_timing(True)
+    x = lib.create_V("D", np.zeros_like(src), "even")
+    lib.invert("D", L, x, b, MASS, parity="even", max_iter=MAX_ITER, nrestart=NRESTART, resid=RESID)
+    st = lib.last_stats()
+    lib.set_kernel_timing(False)
+    lib.destroy_V("D", x)
+    lib.destroy_V("D", b)
+    lib.destroy_L("D", L)
     lib.finalize()
-    print(json.dumps({"mode": "mixed", "inner": args.inner, "solves": res_all,
-                      "tuning_k1": lib_tuning[0], "tuning_k2": lib_tuning[1]}))
+    k1_us = st.dslash_ms / max(st.dslash_launches, 1) * 1e3
+    k2_us = st.mdagm_ms / max(st.mdagm_launches, 1) * 1e3
+    print(json.dumps({"mode": "mixed", "inner": args.inner, "lattice": "x".join(map(str, dims)), "solves": res_all,
+                      "k1_us": k1_us, "k2_us": k2_us, "tuning_k1": lib_tuning[0], "tuning_k2": lib_tuning[1]}))
 
 
 MS_DIMS = (32, 32, 32, 64)
