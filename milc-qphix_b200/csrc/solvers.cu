@@ -150,6 +150,8 @@ public:
     IterLoop &operator=(const IterLoop &) = delete;
     ~IterLoop() { release(); }
     void invalidate() { release(); }
+    // host time spent capturing and instantiating graphs so far
+    double build_seconds() const { return build_sec_; }
 
     template <typename Enq, typename Next>
     void run(Enq enqueue, Next next, TimedLaunches &tl, int cap, int first_chunk = 8)
@@ -162,7 +164,11 @@ public:
         S.counter = S.counter2 = 0;
         // NCCL calls are not captured: a solve over several GPUs runs in chunks
         if (graphs_enabled() && !tl.on && !(c.halo.on && c.halo.nranks > 1)) {
-            if (!exec_) build(enqueue);
+            if (!exec_) {
+                const double t0 = wall_seconds();
+                build(enqueue);
+                build_sec_ += wall_seconds() - t0;
+            }
             S.use_cond = 1;
             S.cond = handle_;
             S.iter_cap = S.iteration + (cap > 0 ? cap : 1);
@@ -237,6 +243,7 @@ private:
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
     cudaGraphConditionalHandle handle_ = 0;
+    double build_sec_ = 0;
 };
 
 }  // namespace
@@ -439,6 +446,10 @@ struct MixedResult {
     int iterations = 0;
     int reliable_updates = 0;
     int escalated = 0;
+    // wall-clock split (QPHIX_B200_VERBOSE >= 2 only): set-up and first
+    // true residual, inner CG loops, reliable updates, and the graph
+    // captures inside the inner loops
+    double t_setup = 0, t_loop = 0, t_ru = 0, t_graph = 0;
 };
 
 // `ls_up`: FP32 links to continue with when a 16-bit inner solve stops
@@ -460,6 +471,15 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
     const double m4 = 4.0 * mass * mass;
     const double delta2 = c.reliable_delta * c.reliable_delta;
     MixedResult out;
+    const bool split = c.verbose >= 2;
+    double t_mark = split ? wall_seconds() : 0.0;
+    auto lap = [&](double &acc) {
+        if (!split) return;
+        sync_check();
+        const double now = wall_seconds();
+        acc += now - t_mark;
+        t_mark = now;
+    };
 
     const double bnorm = norm2_sync(Prec::Double, b);
     require_finite("asqtad_invert", bnorm, "|source|^2");
@@ -508,6 +528,7 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
     int stalled = 0;
     dslash_prepare(ps, *ls_cur, L);
     IterLoop loop;
+    lap(out.t_setup);
     for (;;) {
         double size_prev = S.rsq;
         loop.run(
@@ -527,6 +548,7 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
             },
             tl, max_cg - S.iteration + 1);
         if (S.error) breakdown("asqtad_invert (mixed precision)", S.error, S.iteration);
+        lap(out.t_loop);
         out.iterations = S.iteration;
         const double oldrsq = S.oldrsq;
         const double sloppy_rsq = S.rsq;
@@ -579,7 +601,10 @@ MixedResult mixed_pass(Prec ps, const LinkSet &ls64, const LinkSet &lss, const L
         S.counter = S.counter2 = 0;
         upload_state();
         cg_axpy(ps, L, rs, pv, c.d_state, -1);  // p = r + beta p with the true residual
+        lap(out.t_ru);
     }
+    lap(out.t_ru);
+    out.t_graph = loop.build_seconds();
     return out;
 }
 
@@ -1144,6 +1169,10 @@ int multishift_mixed(Prec ps, const LinkSet &ls64, const LinkSet &lss, const Lin
                 const double now = wall_seconds();
                 std::fprintf(stderr, "qphix_b200 mixed multi-shift: shift %d refinement %d iterations, %d updates, "
                                      "%.2f ms\n", j, m.iterations, m.reliable_updates, 1e3 * (now - t_shift));
+                if (c.verbose >= 2)
+                    std::fprintf(stderr, "qphix_b200 mixed multi-shift: shift %d set-up %.2f ms, inner %.2f ms, "
+                                         "updates %.2f ms, escalated %d (graph builds %.2f ms of the inner)\n", j,
+                                 1e3 * m.t_setup, 1e3 * m.t_loop, 1e3 * m.t_ru, m.escalated, 1e3 * m.t_graph);
                 t_shift = now;
             }
             A.res[j]->final_rsq = m.true_rsq_rel;
