@@ -212,8 +212,9 @@ __device__ __forceinline__ void dslash_site(const DslashArgs<SV, SL> &a, int j, 
 // kernels keep one stage in flight in 80 registers at 3 blocks/SM.
 // 24^3x48 mixed solves: 12-real 100.7 ms (4 blocks: 107.8 ms); 18-real
 // 113.9 ms (1 block at 241 registers: 116.7 ms); 16-bit links 93.6 ms (1
-// block: 118.1 ms); 16-bit vectors and links 88.7 ms (4 blocks at 64
-// registers: 93.0 ms)
+// block: 118.1 ms; 4 blocks at 64 registers, no spills in K1: 93.0 against
+// 88.0 ms, K2 49.8 against 44.9 us); 16-bit vectors and links 88.7 ms (4
+// blocks at 64 registers: 93.0 ms)
 template <typename SV, typename SL> struct MinBlocks { static constexpr int value = 1; };
 template <> struct MinBlocks<float, float> { static constexpr int value = 3; };
 template <> struct MinBlocks<float, Recon12> { static constexpr int value = 3; };
